@@ -1,0 +1,149 @@
+/*
+ * warpmd_rmsd.h -- C ABI of the B200 (sm_100a) RMSD library libwarpmd_rmsd.so.
+ *
+ * Scope: the RMSD hot path of warp-md 0.4.30 -- per-frame optimal-superposition
+ * RMSD against a reference (RmsdPlan), the all-pairs frame x frame RMSD matrix
+ * (PairwiseRmsdPlan, metrics "rms" and "nofit"), the gradient dRMSD/dx, and a
+ * batched launch over many trajectories of uneven size.
+ *
+ * Conventions
+ *   - Every entry point returns an int status: WMD_OK (0) or a negative WMD_ERR_*
+ *     code; wmd_last_error(ctx) gives the message of the last failure on ctx.
+ *     This mirrors TrajResult<T> / TrajError (crates/traj-core/src/error.rs:3-34):
+ *     WMD_ERR_MISMATCH <-> TrajError::Mismatch, WMD_ERR_UNSUPPORTED and
+ *     WMD_ERR_CUDA <-> TrajError::Unsupported("cuda driver error: ...")
+ *     (crates/traj-gpu/src/cuda.rs:384-390).
+ *   - Coordinates are float32, frame-major: coords[frame][atom][stride] with
+ *     stride 3 (packed xyz) or 4 (xyzw, the reference's FrameChunk/Float4 layout,
+ *     crates/traj-core/src/frame.rs:10-20; w is ignored).
+ *   - Pointers may be host or device memory where a function says so; the
+ *     library detects which with cudaPointerGetAttributes.  Host inputs are
+ *     streamed to the device in chunks inside the call (copies overlap the
+ *     kernels), host outputs are written before the call returns.
+ *   - `stream` is a cudaStream_t (NULL = the legacy default stream).  Calls with
+ *     only device pointers are asynchronous on that stream; calls with any host
+ *     pointer synchronize before returning.
+ *   - A wmd_ctx owns its scratch memory and is not thread-safe: use one context
+ *     per host thread / stream.  The caller owns every input and output buffer.
+ */
+#ifndef WARPMD_RMSD_H
+#define WARPMD_RMSD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WMD_OK 0
+#define WMD_ERR_INVALID_ARG (-1) /* null pointer, bad stride/size/mode       */
+#define WMD_ERR_CUDA (-2)        /* CUDA runtime error (message has details) */
+#define WMD_ERR_OOM (-3)         /* device or pinned-host allocation failed  */
+#define WMD_ERR_MISMATCH (-4)    /* shapes disagree (TrajError::Mismatch)    */
+#define WMD_ERR_UNSUPPORTED (-5) /* mode/metric not provided on this build   */
+#define WMD_ERR_TIMEOUT (-6)     /* a bounded device-side wait ran out       */
+#define WMD_ERR_NO_DEVICE (-7)   /* no CUDA device / not an sm_100 device     */
+
+#define WMD_PAIR_RMS 0   /* optimal-superposition RMSD (metric "rms")  */
+#define WMD_PAIR_NOFIT 1 /* plain coordinate RMSD (metric "nofit")     */
+
+#define WMD_MODE_FP32 0  /* plain FP32 SIMT covariance tiles, FP64 QCP epilogue       */
+#define WMD_MODE_I8X3 1  /* tcgen05 int8 tensor cores, 3 limbs (24-bit fixed point), */
+                         /* exact int32 accumulation, FP64 QCP epilogue              */
+#define WMD_MODE_I8X2 2  /* as WMD_MODE_I8X3 with 2 limbs (16-bit fixed point)       */
+#define WMD_MODE_FP64 3  /* FP64 SIMT covariance tiles (accuracy reference on GPU)    */
+
+/* Per-frame statistics written by wmd_rmsd_forward and read by
+ * wmd_rmsd_backward: 16 doubles per frame
+ *   [0..2]  frame centroid        [3..11] H = sum (x - cx)(y - cy)^T (row-major)
+ *   [12]    lambda_max (QCP)      [13]    rmsd
+ *   [14]    n_sel                 [15]    G_x + G_y                            */
+#define WMD_FRAME_STATS 16
+
+typedef struct wmd_ctx wmd_ctx;
+typedef struct wmd_ref wmd_ref;
+
+/* Creates a context on CUDA device `device` (replaces GpuContext::new,
+ * crates/traj-gpu/src/cuda/runtime_core.rs:4-17; no runtime compilation). */
+int wmd_create(int device, wmd_ctx** out);
+int wmd_destroy(wmd_ctx* ctx);
+/* Message of the last failing call on ctx (never NULL; "" when none).  With
+ * ctx == NULL, the message of the last failing wmd_create on this thread. */
+const char* wmd_last_error(const wmd_ctx* ctx);
+/* Library version string, e.g. "0.4.30+b200.1". */
+const char* wmd_version(void);
+
+/* Uploads a reference structure of n_sel atoms (host or device pointer,
+ * stride 3 or 4) and precomputes, in FP64, its centroid, the centred
+ * coordinates and G_y.  Replaces GpuContext::reference
+ * (crates/traj-gpu/src/cuda/runtime_core.rs:127-137). */
+int wmd_reference_upload(wmd_ctx* ctx, const float* ref, int64_t n_sel, int stride, wmd_ref** out);
+int wmd_reference_free(wmd_ctx* ctx, wmd_ref* ref);
+
+/* Per-frame RMSD of n_frames frames against `ref` (RmsdPlan, plan.rs:323-404
+ * and rmsd_aligned_selected plan.rs:1161-1248 when align != 0; rmsd_raw_selected
+ * plan.rs:1093-1110 when align == 0).
+ *   coords : host or device, [n_frames][n_atoms][stride]
+ *   sel    : NULL for the dense selection 0..n_sel-1 (requires n_atoms == n_sel),
+ *            else n_sel uint32 atom indices < n_atoms (host or device)
+ *   out    : host or device, n_frames doubles
+ * FP64 accumulation of the frame statistics, QCP in FP64. */
+int wmd_rmsd_frames(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                    const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, int align, double* out,
+                    void* stream);
+
+/* Same as wmd_rmsd_frames (align = 1) but device pointers only, and also
+ * writes WMD_FRAME_STATS doubles per frame to `stats` (device) for
+ * wmd_rmsd_backward. */
+int wmd_rmsd_forward(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                     const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, double* out, double* stats,
+                     void* stream);
+
+/* Gradient of the aligned RMSD (no counterpart in the reference, which has no
+ * derivative): grad[f][sel[i]][:] = grad_rmsd[f] * (x_i - cx - R^T (y_i - cy))
+ * / (n_sel * rmsd_f), R re-derived from the QCP eigenvector of the H stored in
+ * `stats`.  Device pointers only.  grad_rmsd may be NULL (all ones).  grad is
+ * [n_frames][n_atoms][3] float32; rows of unselected atoms are not written. */
+int wmd_rmsd_backward(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                      const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, const double* stats,
+                      const float* grad_rmsd, float* grad, void* stream);
+
+/* Shape drop-in for GpuContext::rmsd_covariance
+ * (crates/traj-gpu/src/cuda/runtime_core.rs:375-472): per frame the 3x3
+ * covariance cov[f*9 + 3*a + b] = sum (x_a - cx_a)(y_b - cy_b) and the centred
+ * sums of squares sum_x2[f], sum_y2[f], as float32 (accumulated in FP64).
+ * Host or device outputs. */
+int wmd_rmsd_covariance(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                        const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, float* cov, float* sum_x2,
+                        float* sum_y2, void* stream);
+
+/* All-pairs RMSD matrix (PairwiseRmsdPlan::finalize, plan.rs:593-674): out is
+ * row-major n_frames x n_frames float32, symmetric, zero diagonal, all zeros
+ * when n_sel < 2.  coords/sel/out host or device.  metric WMD_PAIR_*,
+ * mode WMD_MODE_*. */
+int wmd_pairwise_rmsd(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                      const uint32_t* sel, int64_t n_sel, int metric, int mode, float* out, void* stream);
+
+/* One trajectory of a batched launch.  All pointers are device pointers. */
+typedef struct wmd_batch_desc {
+  const float* coords; /* [n_frames][n_atoms][3] packed xyz             */
+  const float* ref;    /* [n_atoms][3] reference structure               */
+  int64_t n_atoms;
+  int64_t n_frames;
+  double* rmsd;        /* [n_frames] output                              */
+  float* grad;         /* [n_frames][n_atoms][3] output, or NULL         */
+} wmd_batch_desc;
+
+/* Per-frame RMSD (+ gradients when with_grad != 0 and grad != NULL) of n_traj
+ * independent trajectories of uneven size in one persistent launch.  Performs
+ * no allocation and no host synchronization once the context's workspace is
+ * large enough (see wmd_batched_prepare), so it can be captured in a CUDA graph.
+ * No counterpart in the reference, which runs one plan per trajectory. */
+int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, int n_traj, int with_grad);
+int wmd_batched_rmsd(wmd_ctx* ctx, const wmd_batch_desc* descs, int n_traj, int with_grad, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WARPMD_RMSD_H */

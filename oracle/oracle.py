@@ -1,0 +1,132 @@
+"""ctypes wrapper over the CPU FP64 oracle (``oracle/rmsd_oracle.c``).
+
+TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()``
+and the CPU-baseline / ``--impl reference`` legs of ``bench.py``, always as the
+checker.  The product (``warp-md_b200/warp_md``) never imports it.
+
+The C file restates warp-md's RMSD plans (see its header for the file:line
+citations into crates/traj-engine/src/plans/rmsd/plan.rs).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Optional, Tuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "librmsd_oracle.so")
+_lib = None
+
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_i64 = ctypes.c_int64
+_int = ctypes.c_int
+_vp = ctypes.c_void_p
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (gcc + OpenMP)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.wmdo_rmsd_frames.argtypes = [_vp, _i64, _i64, _int, _vp, _i64, _vp, _int, _int, _vp, _vp, _int]
+        L.wmdo_rmsd_frames.restype = None
+        L.wmdo_rmsd_grad.argtypes = [_vp, _i64, _i64, _int, _vp, _i64, _vp, _int, _vp, _vp, _int]
+        L.wmdo_rmsd_grad.restype = None
+        L.wmdo_pairwise_block.argtypes = [_vp, _i64, _i64, _int, _int, _i64, _i64, _i64, _i64, _vp, _vp, _i64, _int]
+        L.wmdo_pairwise_block.restype = None
+        L.wmdo_qcp_rmsd.argtypes = [_vp, _vp, _i64, _int, _int]
+        L.wmdo_qcp_rmsd.restype = ctypes.c_double
+        L.wmdo_svd3.argtypes = [_f64p, _f64p, _f64p, _f64p]
+        L.wmdo_svd3.restype = _int
+        L.wmdo_kabsch_rotation.argtypes = [_f64p, _f64p, ctypes.POINTER(ctypes.c_double)]
+        L.wmdo_kabsch_rotation.restype = None
+        _lib = L
+    return _lib
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _coords(coords) -> Tuple[np.ndarray, int]:
+    c = np.ascontiguousarray(coords, dtype=np.float32)
+    if c.ndim == 2:
+        c = c[None]
+    if c.ndim != 3 or c.shape[2] not in (3, 4):
+        raise ValueError("coords must be (frames, atoms, 3|4)")
+    return c, c.shape[2]
+
+
+def rmsd_frames(coords, reference, selection=None, align: bool = True, threads: int = 0):
+    """RmsdPlan semantics: reference holds the selected atoms (n_sel, 3|4).
+    Returns (f32 array as the reference returns it, f64 array before rounding)."""
+    c, stride = _coords(coords)
+    ref = np.ascontiguousarray(reference, dtype=np.float32)
+    n_sel = ref.shape[0]
+    sel = None if selection is None else np.ascontiguousarray(selection, dtype=np.uint32)
+    if sel is not None and sel.shape[0] != n_sel:
+        raise ValueError("selection and reference lengths differ")
+    out32 = np.empty(c.shape[0], np.float32)
+    out64 = np.empty(c.shape[0], np.float64)
+    lib().wmdo_rmsd_frames(_ptr(c), c.shape[0], c.shape[1], stride, _ptr(sel), n_sel, _ptr(ref),
+                           ref.shape[1], int(bool(align)), _ptr(out32), _ptr(out64), int(threads))
+    return out32, out64
+
+
+def rmsd_grad(coords, reference, selection=None, threads: int = 0):
+    """Analytic FP64 gradient dRMSD/dx, shape (frames, atoms, 3); rows of
+    unselected atoms are zero.  Returns (rmsd f64, grad f64)."""
+    c, stride = _coords(coords)
+    ref = np.ascontiguousarray(reference, dtype=np.float32)
+    sel = None if selection is None else np.ascontiguousarray(selection, dtype=np.uint32)
+    rm = np.empty(c.shape[0], np.float64)
+    g = np.zeros((c.shape[0], c.shape[1], 3), np.float64)
+    lib().wmdo_rmsd_grad(_ptr(c), c.shape[0], c.shape[1], stride, _ptr(sel), ref.shape[0], _ptr(ref),
+                         ref.shape[1], _ptr(rm), _ptr(g), int(threads))
+    return rm, g
+
+
+def pairwise(frames, metric: str = "rms", block=None, threads: int = 0):
+    """PairwiseRmsdPlan::finalize semantics over already-selected frames.
+    block = (i0, i1, j0, j1) restricts to a sub-block.  Returns (f32, f64)."""
+    c, stride = _coords(frames)
+    n = c.shape[0]
+    i0, i1, j0, j1 = block if block is not None else (0, n, 0, n)
+    m = {"rms": 0, "nofit": 1}[metric]
+    out32 = np.empty((i1 - i0, j1 - j0), np.float32)
+    out64 = np.empty((i1 - i0, j1 - j0), np.float64)
+    lib().wmdo_pairwise_block(_ptr(c), n, c.shape[1], stride, m, i0, i1, j0, j1, _ptr(out32), _ptr(out64),
+                              j1 - j0, int(threads))
+    return out32, out64
+
+
+def qcp_rmsd(x, y, high_precision: bool = False) -> float:
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    return float(lib().wmdo_qcp_rmsd(_ptr(x), _ptr(y), x.shape[0], x.shape[1], int(high_precision)))
+
+
+def svd3(a):
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(9)
+    u = np.empty(9); s = np.empty(3); vt = np.empty(9)
+    lib().wmdo_svd3(a, u, s, vt)
+    return u.reshape(3, 3), s, vt.reshape(3, 3)
+
+
+def kabsch_rotation(h):
+    h = np.ascontiguousarray(h, dtype=np.float64).reshape(9)
+    r = np.empty(9)
+    ss = ctypes.c_double()
+    lib().wmdo_kabsch_rotation(h, r, ctypes.byref(ss))
+    return r.reshape(3, 3), ss.value

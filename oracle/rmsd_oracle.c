@@ -1,0 +1,400 @@
+/*
+ * rmsd_oracle.c -- CPU FP64 restatement of warp-md's RMSD plans.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA library in
+ * warp-md_b200/: only tests/, __graft_entry__.smoke() and the cpu_baseline /
+ * --impl reference legs of bench.py load it.  Nothing in the product links it.
+ *
+ * What it restates (reference = warp-md 0.4.30, Rust):
+ *   - rmsd_aligned_selected   crates/traj-engine/src/plans/rmsd/plan.rs:1161-1248
+ *       two-pass FP64 centroid + covariance H = sum (x-cx)(y-cy)^T, 3x3 SVD,
+ *       R = V U^T with the reflection fix (negate the last row of V^T when
+ *       det R < 0), explicit residual pass, result rounded to f32.
+ *   - rmsd_raw_selected       plan.rs:1093-1110   (align = false)
+ *   - rmsd_aligned            plan.rs:1112-1159   (pairwise metric "rms")
+ *   - rmsd_raw                plan.rs:1081-1091   (pairwise metric "nofit")
+ *   - PairwiseRmsdPlan::finalize  plan.rs:593-674 (symmetric fill, zero
+ *       diagonal, n_sel < 2 -> all zeros)
+ *
+ * The SVD in the reference is nalgebra 0.32.6 (Cargo.lock:792-793), which is
+ * not vendored.  Here it is a one-sided Jacobi SVD (Hestenes 1958; Demmel &
+ * Veselic 1992) with singular values sorted in descending order, which is the
+ * ordering the reference's reflection fix relies on.  Any correct SVD yields
+ * the same minimum RMSD.
+ *
+ * Also here, for cross-checks: the QCP characteristic-polynomial route
+ * (Theobald 2005, Acta Cryst A61:478; Liu, Agrafiotis & Theobald 2010) and the
+ * analytic gradient dRMSD/dx_k = (x_k - cx - R^T (y_k - cy)) / (n RMSD).
+ * The reference has no gradient; this one is checked by central differences.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define WMDO_API __attribute__((visibility("default")))
+
+/* ------------------------------------------------------------------ */
+/* 3x3 helpers (row-major)                                             */
+/* ------------------------------------------------------------------ */
+static double det3(const double m[9]) {
+  return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+         m[2] * (m[3] * m[7] - m[4] * m[6]);
+}
+
+/* One-sided Jacobi SVD of a 3x3 matrix A = U diag(s) V^T, s sorted
+ * descending, U and V orthogonal (U completed by cross products when A is
+ * rank deficient).  Returns 0. */
+WMDO_API int wmdo_svd3(const double a_in[9], double u[9], double s[3], double vt[9]) {
+  double a[9], v[9];
+  memcpy(a, a_in, sizeof(a));
+  for (int i = 0; i < 9; ++i) v[i] = (i % 4 == 0) ? 1.0 : 0.0;
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    int rotated = 0;
+    for (int p = 0; p < 2; ++p) {
+      for (int q = p + 1; q < 3; ++q) {
+        double alpha = 0, beta = 0, gamma = 0;
+        for (int k = 0; k < 3; ++k) {
+          alpha += a[k * 3 + p] * a[k * 3 + p];
+          beta += a[k * 3 + q] * a[k * 3 + q];
+          gamma += a[k * 3 + p] * a[k * 3 + q];
+        }
+        if (gamma == 0.0 || fabs(gamma) <= 1e-17 * sqrt(alpha * beta)) continue;
+        rotated = 1;
+        double zeta = (beta - alpha) / (2.0 * gamma);
+        double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        double c = 1.0 / sqrt(1.0 + t * t), sn = c * t;
+        for (int k = 0; k < 3; ++k) {
+          double ap = a[k * 3 + p], aq = a[k * 3 + q];
+          a[k * 3 + p] = c * ap - sn * aq;
+          a[k * 3 + q] = sn * ap + c * aq;
+          double vp = v[k * 3 + p], vq = v[k * 3 + q];
+          v[k * 3 + p] = c * vp - sn * vq;
+          v[k * 3 + q] = sn * vp + c * vq;
+        }
+      }
+    }
+    if (!rotated) break;
+  }
+  double sv[3];
+  int order[3] = {0, 1, 2};
+  for (int j = 0; j < 3; ++j)
+    sv[j] = sqrt(a[0 * 3 + j] * a[0 * 3 + j] + a[1 * 3 + j] * a[1 * 3 + j] + a[2 * 3 + j] * a[2 * 3 + j]);
+  for (int i = 0; i < 3; ++i)
+    for (int j = i + 1; j < 3; ++j)
+      if (sv[order[j]] > sv[order[i]]) { int t = order[i]; order[i] = order[j]; order[j] = t; }
+  double uu[9];
+  double smax = sv[order[0]];
+  int have[3] = {0, 0, 0};
+  for (int jj = 0; jj < 3; ++jj) {
+    int j = order[jj];
+    s[jj] = sv[j];
+    for (int k = 0; k < 3; ++k) vt[jj * 3 + k] = v[k * 3 + j];
+    if (sv[j] > 1e-300 && sv[j] > smax * 1e-15) {
+      for (int k = 0; k < 3; ++k) uu[k * 3 + jj] = a[k * 3 + j] / sv[j];
+      have[jj] = 1;
+    }
+  }
+  /* complete U for rank-deficient inputs */
+  if (!have[0]) { uu[0] = 1; uu[3] = 0; uu[6] = 0; have[0] = 1; }
+  if (!have[1]) {
+    /* any unit vector orthogonal to u0 */
+    double x = uu[0], y = uu[3], z = uu[6];
+    double px, py, pz;
+    if (fabs(x) < 0.9) { px = 0; py = -z; pz = y; } else { px = -y; py = x; pz = 0; }
+    double nn = sqrt(px * px + py * py + pz * pz);
+    uu[1] = px / nn; uu[4] = py / nn; uu[7] = pz / nn;
+    have[1] = 1;
+  }
+  if (!have[2]) {
+    uu[2] = uu[3] * uu[7] - uu[6] * uu[4];
+    uu[5] = uu[6] * uu[1] - uu[0] * uu[7];
+    uu[8] = uu[0] * uu[4] - uu[3] * uu[1];
+  }
+  memcpy(u, uu, sizeof(uu));
+  return 0;
+}
+
+/* R = V U^T with the reference's reflection fix. */
+static void kabsch_rotation(const double h[9], double r[9], double* sigma_sum) {
+  double u[9], s[3], vt[9];
+  wmdo_svd3(h, u, s, vt);
+  /* r = vt^T * u^T  -> r[i][j] = sum_k vt[k][i] * u[j][k] */
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double acc = 0;
+      for (int k = 0; k < 3; ++k) acc += vt[k * 3 + i] * u[j * 3 + k];
+      r[i * 3 + j] = acc;
+    }
+  double ss = s[0] + s[1] + s[2];
+  if (det3(r) < 0.0) {
+    for (int k = 0; k < 3; ++k) vt[2 * 3 + k] = -vt[2 * 3 + k];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        double acc = 0;
+        for (int k = 0; k < 3; ++k) acc += vt[k * 3 + i] * u[j * 3 + k];
+        r[i * 3 + j] = acc;
+      }
+    ss -= 2.0 * s[2];
+  }
+  if (sigma_sum) *sigma_sum = ss;
+}
+
+/* ------------------------------------------------------------------ */
+/* Per-frame plans                                                     */
+/* ------------------------------------------------------------------ */
+
+/* plan.rs:1093-1110 */
+static double raw_selected(const float* frame, int64_t frame_atoms, int stride, const float* ref,
+                           int ref_stride, const uint32_t* sel, int64_t n) {
+  if (n == 0) return 0.0;
+  double sum = 0.0;
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t idx = sel ? (int64_t)sel[i] : i;
+    if (idx >= frame_atoms) break;
+    const float* p = frame + idx * stride;
+    const float* q = ref + i * ref_stride;
+    double dx = (double)p[0] - (double)q[0];
+    double dy = (double)p[1] - (double)q[1];
+    double dz = (double)p[2] - (double)q[2];
+    sum += dx * dx + dy * dy + dz * dz;
+  }
+  return sqrt(sum / (double)n);
+}
+
+/* plan.rs:1161-1248.  Returns RMSD in FP64 (the reference rounds it to f32);
+ * optionally returns the rotation, centroids (for the gradient). */
+static double aligned_selected(const float* frame, int64_t frame_atoms, int stride, const float* ref,
+                               int ref_stride, const uint32_t* sel, int64_t n, double r_out[9],
+                               double cx_out[3], double cy_out[3]) {
+  if (n == 0) return 0.0;
+  double cx[3] = {0, 0, 0}, cy[3] = {0, 0, 0};
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t idx = sel ? (int64_t)sel[i] : i;
+    if (idx >= frame_atoms) return 0.0;
+    const float* p = frame + idx * stride;
+    const float* q = ref + i * ref_stride;
+    cx[0] += p[0]; cx[1] += p[1]; cx[2] += p[2];
+    cy[0] += q[0]; cy[1] += q[1]; cy[2] += q[2];
+  }
+  double inv_n = 1.0 / (double)n;
+  for (int k = 0; k < 3; ++k) { cx[k] *= inv_n; cy[k] *= inv_n; }
+  double h[9] = {0};
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t idx = sel ? (int64_t)sel[i] : i;
+    const float* p = frame + idx * stride;
+    const float* q = ref + i * ref_stride;
+    double px = p[0] - cx[0], py = p[1] - cx[1], pz = p[2] - cx[2];
+    double qx = q[0] - cy[0], qy = q[1] - cy[1], qz = q[2] - cy[2];
+    h[0] += px * qx; h[1] += px * qy; h[2] += px * qz;
+    h[3] += py * qx; h[4] += py * qy; h[5] += py * qz;
+    h[6] += pz * qx; h[7] += pz * qy; h[8] += pz * qz;
+  }
+  double r[9];
+  kabsch_rotation(h, r, NULL);
+  double sum = 0.0;
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t idx = sel ? (int64_t)sel[i] : i;
+    const float* p = frame + idx * stride;
+    const float* q = ref + i * ref_stride;
+    double px = p[0] - cx[0], py = p[1] - cx[1], pz = p[2] - cx[2];
+    double qx = q[0] - cy[0], qy = q[1] - cy[1], qz = q[2] - cy[2];
+    double ax = r[0] * px + r[1] * py + r[2] * pz;
+    double ay = r[3] * px + r[4] * py + r[5] * pz;
+    double az = r[6] * px + r[7] * py + r[8] * pz;
+    double dx = ax - qx, dy = ay - qy, dz = az - qz;
+    sum += dx * dx + dy * dy + dz * dz;
+  }
+  if (r_out) memcpy(r_out, r, sizeof(r));
+  if (cx_out) memcpy(cx_out, cx, sizeof(cx));
+  if (cy_out) memcpy(cy_out, cy, sizeof(cy));
+  return sqrt(sum * inv_n);
+}
+
+/* RmsdPlan over a frame-major trajectory: coords [n_frames][n_atoms][stride],
+ * reference [n_sel][ref_stride] (already the selected atoms, as the plan
+ * stores it), sel = NULL means the dense selection 0..n_sel-1.
+ * out32 receives the reference's f32 result, out64 (nullable) the FP64 value
+ * before rounding.  n_threads <= 0 means all OpenMP threads. */
+WMDO_API void wmdo_rmsd_frames(const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                               const uint32_t* sel, int64_t n_sel, const float* ref, int ref_stride,
+                               int align, float* out32, double* out64, int n_threads) {
+#ifdef _OPENMP
+  int nt = n_threads > 0 ? n_threads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
+#endif
+  for (int64_t f = 0; f < n_frames; ++f) {
+    const float* frame = coords + f * n_atoms * stride;
+    double v = align ? aligned_selected(frame, n_atoms, stride, ref, ref_stride, sel, n_sel, NULL, NULL, NULL)
+                     : raw_selected(frame, n_atoms, stride, ref, ref_stride, sel, n_sel);
+    if (out32) out32[f] = (float)v;
+    if (out64) out64[f] = v;
+  }
+  (void)n_threads;
+}
+
+/* Analytic FP64 gradient of the aligned RMSD w.r.t. the frame coordinates:
+ * grad[f][i][:] = (x_i - cx - R^T (y_i - cy)) / (n * rmsd), zero when rmsd == 0.
+ * Writes only the selected atoms' rows (grad has the layout of coords with
+ * stride 3; unselected atoms are left untouched). */
+WMDO_API void wmdo_rmsd_grad(const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                             const uint32_t* sel, int64_t n_sel, const float* ref, int ref_stride,
+                             double* rmsd_out, double* grad, int n_threads) {
+#ifdef _OPENMP
+  int nt = n_threads > 0 ? n_threads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
+#endif
+  for (int64_t f = 0; f < n_frames; ++f) {
+    const float* frame = coords + f * n_atoms * stride;
+    double r[9], cx[3], cy[3];
+    double v = aligned_selected(frame, n_atoms, stride, ref, ref_stride, sel, n_sel, r, cx, cy);
+    if (rmsd_out) rmsd_out[f] = v;
+    double scale = (v > 0.0 && n_sel > 0) ? 1.0 / ((double)n_sel * v) : 0.0;
+    for (int64_t i = 0; i < n_sel; ++i) {
+      int64_t idx = sel ? (int64_t)sel[i] : i;
+      const float* p = frame + idx * stride;
+      const float* q = ref + i * ref_stride;
+      double qx = q[0] - cy[0], qy = q[1] - cy[1], qz = q[2] - cy[2];
+      /* R^T q */
+      double tx = r[0] * qx + r[3] * qy + r[6] * qz;
+      double ty = r[1] * qx + r[4] * qy + r[7] * qz;
+      double tz = r[2] * qx + r[5] * qy + r[8] * qz;
+      double* g = grad + (f * n_atoms + idx) * 3;
+      g[0] = (p[0] - cx[0] - tx) * scale;
+      g[1] = (p[1] - cx[1] - ty) * scale;
+      g[2] = (p[2] - cx[2] - tz) * scale;
+    }
+  }
+  (void)n_threads;
+}
+
+/* ------------------------------------------------------------------ */
+/* Pairwise plan (plan.rs:593-674 with rmsd_aligned / rmsd_raw)        */
+/* ------------------------------------------------------------------ */
+
+/* plan.rs:1112-1159: frame = frames[i], reference = frames[j] */
+static double pair_aligned(const float* a, const float* b, int64_t n, int stride) {
+  return aligned_selected(a, n, stride, b, stride, NULL, n, NULL, NULL, NULL);
+}
+
+/* plan.rs:1081-1091 */
+static double pair_raw(const float* a, const float* b, int64_t n, int stride) {
+  return raw_selected(a, n, stride, b, stride, NULL, n);
+}
+
+/* Fills rows [i0,i1) x cols [j0,j1) of the pairwise matrix of the frames in
+ * `frames` ([n_frames][n_sel][stride], already selected).  metric 0 = rms,
+ * 1 = nofit.  out32 (and optional out64) are row-major with leading dimension
+ * ld.  The diagonal is 0; n_sel < 2 gives zeros (plan.rs:604-610). */
+WMDO_API void wmdo_pairwise_block(const float* frames, int64_t n_frames, int64_t n_sel, int stride,
+                                  int metric, int64_t i0, int64_t i1, int64_t j0, int64_t j1,
+                                  float* out32, double* out64, int64_t ld, int n_threads) {
+  (void)n_frames;
+#ifdef _OPENMP
+  int nt = n_threads > 0 ? n_threads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+#endif
+  for (int64_t i = i0; i < i1; ++i) {
+    for (int64_t j = j0; j < j1; ++j) {
+      double v = 0.0;
+      if (i != j && n_sel >= 2) {
+        /* the reference computes pair (min, max) and mirrors it */
+        int64_t a = i < j ? i : j, b = i < j ? j : i;
+        const float* fa = frames + a * n_sel * stride;
+        const float* fb = frames + b * n_sel * stride;
+        v = metric == 0 ? pair_aligned(fa, fb, n_sel, stride) : pair_raw(fa, fb, n_sel, stride);
+      }
+      if (out32) out32[(i - i0) * ld + (j - j0)] = (float)v;
+      if (out64) out64[(i - i0) * ld + (j - j0)] = v;
+    }
+  }
+  (void)n_threads;
+}
+
+/* ------------------------------------------------------------------ */
+/* QCP cross-check (Theobald 2005)                                     */
+/* ------------------------------------------------------------------ */
+
+static double det4(const double k[16]) {
+  double s0 = k[0] * k[5] - k[1] * k[4];
+  double s1 = k[0] * k[6] - k[2] * k[4];
+  double s2 = k[0] * k[7] - k[3] * k[4];
+  double s3 = k[1] * k[6] - k[2] * k[5];
+  double s4 = k[1] * k[7] - k[3] * k[5];
+  double s5 = k[2] * k[7] - k[3] * k[6];
+  double c5 = k[10] * k[15] - k[11] * k[14];
+  double c4 = k[9] * k[15] - k[11] * k[13];
+  double c3 = k[9] * k[14] - k[10] * k[13];
+  double c2 = k[8] * k[15] - k[11] * k[12];
+  double c1 = k[8] * k[14] - k[10] * k[12];
+  double c0 = k[8] * k[13] - k[9] * k[12];
+  return s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
+}
+
+/* RMSD of one frame against one reference by QCP in FP64 (centroids and
+ * G terms computed two-pass in FP64).  Long-double Newton when hp != 0. */
+WMDO_API double wmdo_qcp_rmsd(const float* x, const float* y, int64_t n, int stride, int hp) {
+  if (n == 0) return 0.0;
+  double cx[3] = {0, 0, 0}, cy[3] = {0, 0, 0};
+  for (int64_t i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) { cx[k] += x[i * stride + k]; cy[k] += y[i * stride + k]; }
+  for (int k = 0; k < 3; ++k) { cx[k] /= (double)n; cy[k] /= (double)n; }
+  double h[9] = {0}, gx = 0, gy = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    double p[3], q[3];
+    for (int k = 0; k < 3; ++k) { p[k] = x[i * stride + k] - cx[k]; q[k] = y[i * stride + k] - cy[k]; }
+    for (int a = 0; a < 3; ++a) {
+      gx += p[a] * p[a];
+      gy += q[a] * q[a];
+      for (int b = 0; b < 3; ++b) h[a * 3 + b] += p[a] * q[b];
+    }
+  }
+  double sxx = h[0], sxy = h[1], sxz = h[2], syx = h[3], syy = h[4], syz = h[5], szx = h[6], szy = h[7], szz = h[8];
+  double K[16] = {sxx + syy + szz, syz - szy, szx - sxz, sxy - syx,
+                  syz - szy, sxx - syy - szz, sxy + syx, szx + sxz,
+                  szx - sxz, sxy + syx, -sxx + syy - szz, syz + szy,
+                  sxy - syx, szx + sxz, syz + szy, -sxx - syy + szz};
+  double c2 = 0;
+  for (int i = 0; i < 9; ++i) c2 += h[i] * h[i];
+  c2 *= -2.0;
+  double c1 = -8.0 * det3(h);
+  double c0 = det4(K);
+  double e0 = 0.5 * (gx + gy);
+  double lambda;
+  if (hp) {
+    long double l = e0;
+    for (int it = 0; it < 200; ++it) {
+      long double l2 = l * l;
+      long double p = l2 * l2 + c2 * l2 + c1 * l + c0;
+      long double dp = 4 * l2 * l + 2 * c2 * l + c1;
+      if (dp == 0) break;
+      long double nl = l - p / dp;
+      if (fabsl(nl - l) <= 1e-19L * fabsl(nl)) { l = nl; break; }
+      l = nl;
+    }
+    lambda = (double)l;
+  } else {
+    double l = e0;
+    for (int it = 0; it < 200; ++it) {
+      double l2 = l * l;
+      double p = l2 * l2 + c2 * l2 + c1 * l + c0;
+      double dp = 4 * l2 * l + 2 * c2 * l + c1;
+      if (dp == 0) break;
+      double nl = l - p / dp;
+      if (fabs(nl - l) <= 1e-15 * fabs(nl)) { l = nl; break; }
+      l = nl;
+    }
+    lambda = l;
+  }
+  double msd = (gx + gy - 2.0 * lambda) / (double)n;
+  return msd > 0 ? sqrt(msd) : 0.0;
+}
+
+/* Kabsch rotation for an arbitrary covariance (exposed for tests of the
+ * rotation convention): r maps frame coordinates onto the reference. */
+WMDO_API void wmdo_kabsch_rotation(const double h[9], double r[9], double* sigma_sum) {
+  kabsch_rotation(h, r, sigma_sum);
+}

@@ -1,0 +1,122 @@
+"""All-pairs RMSD matrix on the GPU against the oracle's restatement of
+PairwiseRmsdPlan::finalize (plan.rs:593-674).
+
+Tolerances (max abs error vs the FP64 oracle, float32 outputs):
+  fp64 : 1e-5 A   (FP64 covariance tiles, exact up to the float32 output)
+  i8x3 : 1e-4 A   (24-bit fixed point, exact int32 accumulation)
+  i8x2 : 5e-4 A   (16-bit fixed point)
+  fp32 : 2e-2 A   (plain FP32 accumulation; measured error is reported by bench.py)
+"""
+import numpy as np
+import pytest
+
+import oracle
+import warp_md
+from warp_md import _native as N
+from warp_md import synth
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-5, "i8x3": 1e-4, "i8x2": 5e-4, "fp32": 2e-2}
+MODES = ["fp64", "fp32", "i8x3", "i8x2"]
+
+
+def gpu_pairwise(ctx, frames, metric="rms", mode="fp64", sel=None, device_io=False):
+    from warp_md.plans import _PAIR_MODES
+
+    fr = np.ascontiguousarray(frames, np.float32)
+    F, n_atoms = fr.shape[0], fr.shape[1]
+    n_sel = n_atoms if sel is None else len(sel)
+    m = N.PAIR_RMS if metric == "rms" else N.PAIR_NOFIT
+    if device_io:
+        d = torch.from_numpy(fr).cuda()
+        out = torch.empty(F, F, dtype=torch.float32, device="cuda")
+        ds = None if sel is None else torch.from_numpy(np.asarray(sel, np.int32)).cuda()
+        ctx.check(ctx.lib.wmd_pairwise_rmsd(ctx.handle, d.data_ptr(), F, n_atoms, 3,
+                                            None if ds is None else ds.data_ptr(), n_sel, m, _PAIR_MODES[mode],
+                                            out.data_ptr(), None))
+        torch.cuda.synchronize()
+        return out.cpu().numpy()
+    out = np.empty((F, F), np.float32)
+    s = None if sel is None else np.ascontiguousarray(sel, np.uint32)
+    ctx.check(ctx.lib.wmd_pairwise_rmsd(ctx.handle, fr.ctypes.data, F, n_atoms, 3, N.ptr(s), n_sel, m,
+                                        _PAIR_MODES[mode], out.ctypes.data, None))
+    return out
+
+
+def _supported(ctx, mode):
+    fr = np.zeros((2, 3, 3), np.float32)
+    out = np.empty((2, 2), np.float32)
+    from warp_md.plans import _PAIR_MODES
+
+    rc = ctx.lib.wmd_pairwise_rmsd(ctx.handle, fr.ctypes.data, 2, 3, 3, None, 3, 0, _PAIR_MODES[mode],
+                                   out.ctypes.data, None)
+    return rc != N.WMD_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_golden_pairwise(gpu_ctx, golden, mode):
+    if not _supported(gpu_ctx, mode):
+        pytest.skip(f"{mode} not built")
+    for name in sorted(k[7:] for k in golden.files if k.startswith("frames_")):
+        if "expect_pair_aligned_" + name not in golden.files:
+            continue
+        fr = golden["frames_" + name]
+        got = gpu_pairwise(gpu_ctx, fr, "rms", mode)
+        np.testing.assert_allclose(got, golden["expect_pair_aligned_" + name], rtol=0, atol=TOL[mode], err_msg=name)
+        got = gpu_pairwise(gpu_ctx, fr, "nofit", mode)
+        np.testing.assert_allclose(got, golden["expect_pair_raw_" + name], rtol=0, atol=TOL[mode], err_msg=name)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("F,n", [(2, 2), (3, 5), (33, 17), (129, 100), (300, 257)])
+def test_drift_shapes(gpu_ctx, mode, F, n):
+    if not _supported(gpu_ctx, mode):
+        pytest.skip(f"{mode} not built")
+    fr = synth.make_drift_trajectory(n, F, 0.1, seed=F + n)
+    got = gpu_pairwise(gpu_ctx, fr, "rms", mode, device_io=True)
+    _, exp = oracle.pairwise(fr, "rms")
+    assert np.all(np.diag(got) == 0)
+    np.testing.assert_array_equal(got, got.T)
+    np.testing.assert_allclose(got, exp, rtol=0, atol=TOL[mode])
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_allpairs_subblock(gpu_ctx, mode):
+    """All-pairs workload recipe (slow drift + random rigid motions), 1,000
+    atoms; errors on a 512 x 512 block against the FP64 oracle."""
+    if not _supported(gpu_ctx, mode):
+        pytest.skip(f"{mode} not built")
+    fr = synth.make_drift_trajectory(1000, 640, 0.1, seed=3)
+    got = gpu_pairwise(gpu_ctx, fr, "rms", mode, device_io=True)
+    _, exp = oracle.pairwise(fr, "rms", block=(0, 512, 128, 640))
+    err = np.abs(got[0:512, 128:640] - exp)
+    assert err.max() <= TOL[mode], (mode, err.max(), np.sqrt((err ** 2).mean()))
+
+
+def test_selection_and_small_selections(gpu_ctx):
+    fr = synth.make_drift_trajectory(300, 40, 0.1, seed=8)
+    sel = np.arange(1, 300, 2)
+    got = gpu_pairwise(gpu_ctx, fr, "rms", "fp64", sel=sel)
+    _, exp = oracle.pairwise(fr[:, sel], "rms")
+    np.testing.assert_allclose(got, exp, rtol=0, atol=1e-5)
+    one = gpu_pairwise(gpu_ctx, fr, "rms", "fp64", sel=[7])
+    assert np.all(one == 0)  # n_sel < 2 -> zeros (plan.rs:604-610)
+
+
+def test_plan_api_known_answers():
+    coords = np.array([[[0, 0, 0], [1, 0, 0]], [[0, 0, 0], [2, 0, 0]], [[0, 0, 0], [3, 0, 0]]], np.float32)
+    system = warp_md.System.from_arrays({"name": ["DA", "AC"], "resid": [1, 2]}, positions0=coords[0])
+    traj = warp_md.Trajectory.from_numpy(coords)
+    sel = system.select("resid 1:2")
+    m = warp_md.PairwiseRmsdPlan(sel, metric="nofit").run(traj, system, frame_indices=[0, 1])
+    assert abs(m[0, 1] - np.sqrt(0.5)) < 1e-6 and abs(m[1, 0] - np.sqrt(0.5)) < 1e-6
+    m = warp_md.PairwiseRmsdPlan(sel, metric="nofit").run(traj, system, frame_indices=[0, 2])
+    np.testing.assert_allclose(m[0, 1], np.sqrt(2.0), atol=1e-6)
+    from warp_md.analysis.rmsd import pairwise_rmsd
+
+    m = pairwise_rmsd(warp_md.Trajectory.from_numpy(coords[:2]), system, mask="all", metric="srmsd")
+    np.testing.assert_allclose(m[0, 1], 0.5, rtol=1e-6)
+    half = pairwise_rmsd(traj, system, mask="all", metric="nofit", mat_type="half")
+    assert half.shape == (3,)

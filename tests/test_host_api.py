@@ -1,0 +1,99 @@
+"""Host-side behaviour of the warp_md drop-in that needs no GPU: the
+System/Selection/Trajectory constructors, the selection grammar, device and
+enum parsing, frame subsets, and the errors the reference raises."""
+import numpy as np
+import pytest
+
+import warp_md
+from warp_md import plans
+
+
+def _system(n=6, positions0=None):
+    table = {"name": ["CA", "CB", "N", "CA", "C", "O"][:n], "resname": ["ALA"] * n,
+             "resid": [1, 1, 1, 2, 2, 3][:n], "element": ["C", "C", "N", "C", "C", "O"][:n]}
+    return warp_md.System.from_arrays(table, positions0=positions0)
+
+
+def test_selection_grammar():
+    s = _system()
+    assert s.select("all").indices == [0, 1, 2, 3, 4, 5]
+    assert s.select("").indices == [0, 1, 2, 3, 4, 5]
+    assert s.select("name CA").indices == [0, 3]
+    assert s.select("name CA CB").indices == [0, 1, 3]
+    assert s.select("resid 1:2").indices == [0, 1, 2, 3, 4]
+    assert s.select("resid 2-3").indices == [3, 4, 5]
+    assert s.select("resid 1 3").indices == [0, 1, 2, 5]
+    assert s.select("name CA and resid 2").indices == [3]
+    assert s.select("not element C").indices == [2, 5]
+    assert s.select("(name N or name O) and not resid 3").indices == [2]
+    for bad in ("bogus", "name", "resid x", "(name CA", "resid 1 :"):
+        with pytest.raises(RuntimeError):
+            s.select(bad)
+    assert s.select_indices([5, 1]).indices == [5, 1]
+
+
+def test_from_arrays_validation():
+    with pytest.raises(RuntimeError):
+        warp_md.System.from_arrays({"name": ["A", "B"], "resid": [1]})
+    with pytest.raises(RuntimeError):
+        warp_md.System.from_arrays({"resid": [1]})
+    s = warp_md.System.from_arrays({"name": ["A", "B"]}, positions0=np.zeros((2, 3)))
+    assert s.n_atoms() == 2 and s.positions0.dtype == np.float32
+
+
+def test_trajectory_from_numpy():
+    t = warp_md.Trajectory.from_numpy(np.zeros((4, 3), np.float64))
+    assert t.coords.shape == (1, 4, 3) and t.coords.dtype == np.float32
+    with pytest.raises(RuntimeError):
+        warp_md.Trajectory.from_numpy(np.zeros((2, 4, 2), np.float32))
+    with pytest.raises(RuntimeError):
+        warp_md.Trajectory.from_numpy(np.zeros((2, 4, 3), np.int32))
+
+
+def test_parsers():
+    assert plans.parse_device("auto") == 0
+    assert plans.parse_device("cuda") == 0
+    assert plans.parse_device("CUDA:3") == 3
+    for bad in ("cuda:", "cuda:x", "cuda:1:2", "tpu"):
+        with pytest.raises(RuntimeError):
+            plans.parse_device(bad)
+    with pytest.raises(warp_md.WarpMdError):
+        plans.parse_device("cpu")
+    with pytest.raises(RuntimeError, match="reference must be"):
+        warp_md.RmsdPlan(_system().select("all"), reference="first")
+    with pytest.raises(RuntimeError, match="metric must be"):
+        warp_md.PairwiseRmsdPlan(_system().select("all"), metric="bogus")
+    with pytest.raises(RuntimeError, match="pbc must be"):
+        warp_md.PairwiseRmsdPlan(_system().select("all"), pbc="triclinic")
+
+
+def test_frame_subset_semantics():
+    assert plans.frame_subset(5, None) is None
+    assert plans.frame_subset(5, [0, 2]).tolist() == [0, 2]
+    assert plans.frame_subset(5, [4, 0, 9]).tolist() == [4, 0]
+    assert plans.frame_subset(5, [-1, 0, -6]).tolist() == [4, 0]
+
+
+def test_plan_input_errors_before_device_work():
+    s = _system(positions0=None)
+    t = warp_md.Trajectory.from_numpy(np.zeros((2, 5, 3), np.float32))
+    with pytest.raises(RuntimeError, match="atom count"):
+        warp_md.RmsdPlan(s.select("all")).run(t, s)
+    t6 = warp_md.Trajectory.from_numpy(np.zeros((2, 6, 3), np.float32))
+    with pytest.raises(RuntimeError, match="no topology reference"):
+        warp_md.RmsdPlan(s.select("all"), reference="topology").run(t6, s)
+    with pytest.raises(warp_md.WarpMdError):
+        warp_md.RmsdPlan(s.select("all"), reference="frame0").run(t6, s, device="cpu")
+    with pytest.raises(warp_md.WarpMdError, match="dme"):
+        warp_md.PairwiseRmsdPlan(s.select("all"), metric="dme").run(t6, s)
+
+
+def test_synth_shapes_and_seeding():
+    fr, ref = warp_md.synth.make_trajectory(50, 4, (0.05, 3.0), seed=3)
+    fr2, ref2 = warp_md.synth.make_trajectory(50, 4, (0.05, 3.0), seed=3)
+    assert fr.shape == (4, 50, 3) and fr.dtype == np.float32
+    np.testing.assert_array_equal(fr, fr2)
+    steps = np.linalg.norm(np.diff(ref.astype(np.float64), axis=0), axis=1)
+    np.testing.assert_allclose(steps, 3.8, rtol=1e-5)
+    d = warp_md.synth.make_drift_trajectory(20, 3, 0.1, seed=1)
+    assert d.shape == (3, 20, 3)

@@ -1,0 +1,291 @@
+// qcp.cuh -- FP64 optimal-superposition math shared by every kernel.
+//
+// Given the 3x3 cross-covariance H = sum_k (x_k - cx)(y_k - cy)^T of a frame x
+// against a reference y, the minimum over rotations R of sum |R(x_k-cx) - (y_k-cy)|^2
+// is G_x + G_y - 2 lambda_max, where lambda_max = s1 + s2 + sign(det H) s3 (s_i the
+// singular values of H) is the largest eigenvalue of the 4x4 quaternion key
+// matrix K(H) (Horn 1987).  The reference (warp-md plan.rs:1161-1248,
+// math.rs:7-38) gets the same number from an nalgebra SVD with the
+// reflection fix; this file uses QCP: Newton iteration on the characteristic
+// polynomial of K (Theobald 2005, Acta Cryst A61:478-480; Liu, Agrafiotis &
+// Theobald 2010, J Comput Chem 31:1561), in FP64, starting from the upper
+// bound (G_x + G_y)/2.  When the largest root is (nearly) double -- collinear or
+// planar structures -- the polynomial route loses accuracy, so lambda is then
+// taken from a one-sided Jacobi SVD (Hestenes 1958) instead.
+//
+// The rotation (needed by the gradient) is re-derived from the eigenvector of
+// K for lambda_max, read off the adjugate of (K - lambda I), and converted to
+// the rotation matrix that maps frame coordinates onto the reference
+// (the same R = V U^T the reference builds).
+#pragma once
+
+#include <math.h>
+
+#if defined(__CUDACC__)
+#define WMD_HD __host__ __device__ __forceinline__
+#else
+#define WMD_HD inline
+#endif
+
+namespace wmd {
+
+WMD_HD double det3(const double m[9]) {
+  return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+         m[2] * (m[3] * m[7] - m[4] * m[6]);
+}
+
+// Key matrix K (row-major 4x4, symmetric) of H (row-major, H[a][b] = sum x_a y_b).
+WMD_HD void key_matrix(const double h[9], double k[16]) {
+  const double sxx = h[0], sxy = h[1], sxz = h[2];
+  const double syx = h[3], syy = h[4], syz = h[5];
+  const double szx = h[6], szy = h[7], szz = h[8];
+  k[0] = sxx + syy + szz; k[1] = syz - szy;        k[2] = szx - sxz;         k[3] = sxy - syx;
+  k[4] = k[1];            k[5] = sxx - syy - szz;  k[6] = sxy + syx;         k[7] = szx + sxz;
+  k[8] = k[2];            k[9] = k[6];             k[10] = -sxx + syy - szz; k[11] = syz + szy;
+  k[12] = k[3];           k[13] = k[7];            k[14] = k[11];            k[15] = -sxx - syy + szz;
+}
+
+// Determinant of a 4x4 matrix by 2x2 minors of the first two and last two rows.
+WMD_HD double det4(const double k[16]) {
+  const double s0 = k[0] * k[5] - k[1] * k[4];
+  const double s1 = k[0] * k[6] - k[2] * k[4];
+  const double s2 = k[0] * k[7] - k[3] * k[4];
+  const double s3 = k[1] * k[6] - k[2] * k[5];
+  const double s4 = k[1] * k[7] - k[3] * k[5];
+  const double s5 = k[2] * k[7] - k[3] * k[6];
+  const double c5 = k[10] * k[15] - k[11] * k[14];
+  const double c4 = k[9] * k[15] - k[11] * k[13];
+  const double c3 = k[9] * k[14] - k[10] * k[13];
+  const double c2 = k[8] * k[15] - k[11] * k[12];
+  const double c1 = k[8] * k[14] - k[10] * k[12];
+  const double c0 = k[8] * k[13] - k[9] * k[12];
+  return s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
+}
+
+// One-sided Jacobi SVD (Hestenes): returns singular values s (unsorted, >= 0)
+// and, when u/v are non-null, the matching left/right singular vectors as
+// columns (u column j = A v_j / s_j, left zero when s_j == 0).
+WMD_HD void svd3_jacobi(const double a_in[9], double s[3], double* u, double* v) {
+  double a[9];
+  double vv[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  for (int i = 0; i < 9; ++i) a[i] = a_in[i];
+  for (int sweep = 0; sweep < 40; ++sweep) {
+    bool rotated = false;
+    for (int pq = 0; pq < 3; ++pq) {
+      const int p = pq == 2 ? 1 : 0;
+      const int q = pq == 0 ? 1 : 2;
+      double alpha = 0, beta = 0, gamma = 0;
+      for (int r = 0; r < 3; ++r) {
+        alpha += a[r * 3 + p] * a[r * 3 + p];
+        beta += a[r * 3 + q] * a[r * 3 + q];
+        gamma += a[r * 3 + p] * a[r * 3 + q];
+      }
+      if (gamma == 0.0 || fabs(gamma) <= 1e-17 * sqrt(alpha * beta)) continue;
+      rotated = true;
+      const double zeta = (beta - alpha) / (2.0 * gamma);
+      const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+      const double c = 1.0 / sqrt(1.0 + t * t), sn = c * t;
+      for (int r = 0; r < 3; ++r) {
+        const double ap = a[r * 3 + p], aq = a[r * 3 + q];
+        a[r * 3 + p] = c * ap - sn * aq;
+        a[r * 3 + q] = sn * ap + c * aq;
+        const double vp = vv[r * 3 + p], vq = vv[r * 3 + q];
+        vv[r * 3 + p] = c * vp - sn * vq;
+        vv[r * 3 + q] = sn * vp + c * vq;
+      }
+    }
+    if (!rotated) break;
+  }
+  for (int j = 0; j < 3; ++j) {
+    s[j] = sqrt(a[j] * a[j] + a[3 + j] * a[3 + j] + a[6 + j] * a[6 + j]);
+    if (u) {
+      const double inv = s[j] > 0 ? 1.0 / s[j] : 0.0;
+      for (int r = 0; r < 3; ++r) u[r * 3 + j] = a[r * 3 + j] * inv;
+    }
+  }
+  if (v)
+    for (int i = 0; i < 9; ++i) v[i] = vv[i];
+}
+
+// lambda_max from the SVD: s1 + s2 + sign(det H) * s_min.
+WMD_HD double lambda_from_svd(const double h[9]) {
+  double s[3];
+  svd3_jacobi(h, s, nullptr, nullptr);
+  double smin = s[0];
+  if (s[1] < smin) smin = s[1];
+  if (s[2] < smin) smin = s[2];
+  const double sum = s[0] + s[1] + s[2];
+  return det3(h) < 0.0 ? sum - 2.0 * smin : sum;
+}
+
+struct QcpOut {
+  double lambda;
+  int iters;     // Newton iterations used
+  int fallback;  // 1 when lambda came from the SVD
+};
+
+// Largest eigenvalue of K(H); e0 = (G_x + G_y) / 2 >= lambda_max.
+WMD_HD QcpOut qcp_lambda(const double h[9], double e0) {
+  QcpOut o{0.0, 0, 0};
+  if (!(e0 > 0.0)) return o;
+  double k[16];
+  key_matrix(h, k);
+  double c2 = 0.0;
+  for (int i = 0; i < 9; ++i) c2 += h[i] * h[i];
+  c2 *= -2.0;
+  const double c1 = -8.0 * det3(h);
+  const double c0 = det4(k);
+  double l = e0;
+  bool converged = false;
+  int it = 0;
+  for (; it < 60; ++it) {
+    const double l2 = l * l;
+    const double b = (l2 + c2) * l;
+    const double a = b + c1;
+    const double p = a * l + c0;               // P(l)  = l^4 + c2 l^2 + c1 l + c0
+    const double dp = 2.0 * l2 * l + b + a;    // P'(l) = 4 l^3 + 2 c2 l + c1
+    if (!(dp != 0.0)) break;
+    const double delta = p / dp;
+    l -= delta;
+    if (fabs(delta) <= 1e-15 * fabs(l)) {
+      converged = true;
+      ++it;
+      break;
+    }
+  }
+  o.iters = it;
+  // simple-root check: |P'(lambda)| = prod_{i>1} (lambda - lambda_i) is O(lambda^3)
+  // unless another eigenvalue is within ~1e-6 relative of lambda_max.
+  const double l3 = l * l * l;
+  const double dp = 4.0 * l3 + 2.0 * c2 * l + c1;
+  if (!converged || !(fabs(dp) > 1e-6 * 4.0 * fabs(l3)) || !(l == l)) {
+    o.lambda = lambda_from_svd(h);
+    o.fallback = 1;
+  } else {
+    o.lambda = l;
+  }
+  return o;
+}
+
+// Mean-square deviation from the QCP eigenvalue, clamped at zero as the
+// reference does (math.rs:34-37).
+WMD_HD double msd_from(double gx, double gy, double lambda, double n) {
+  const double msd = (gx + gy - 2.0 * lambda) / n;
+  return msd > 0.0 ? msd : 0.0;
+}
+
+// Rotation mapping frame coordinates onto the reference: R = V U^T with the
+// reflection fix, from the SVD.  Used when the eigenvector is ill-defined.
+WMD_HD void rotation_from_svd(const double h[9], double r[9]) {
+  double s[3], u[9], v[9];
+  svd3_jacobi(h, s, u, v);
+  // order columns by singular value, descending
+  int o0 = 0, o1 = 1, o2 = 2, t;
+  if (s[o1] > s[o0]) { t = o0; o0 = o1; o1 = t; }
+  if (s[o2] > s[o1]) { t = o1; o1 = o2; o2 = t; }
+  if (s[o1] > s[o0]) { t = o0; o0 = o1; o1 = t; }
+  const int ord[3] = {o0, o1, o2};
+  double uu[9], vs[9];
+  for (int j = 0; j < 3; ++j)
+    for (int rr = 0; rr < 3; ++rr) {
+      uu[rr * 3 + j] = u[rr * 3 + ord[j]];
+      vs[rr * 3 + j] = v[rr * 3 + ord[j]];
+    }
+  // complete U where singular values vanish
+  const double smax = s[o0];
+  const bool have1 = s[o1] > 1e-15 * smax && s[o1] > 0;
+  const bool have2 = s[o2] > 1e-15 * smax && s[o2] > 0;
+  if (!(smax > 0)) {
+    for (int i = 0; i < 9; ++i) r[i] = (i % 4 == 0) ? 1.0 : 0.0;
+    return;
+  }
+  if (!have1) {
+    const double x = uu[0], y = uu[3], z = uu[6];
+    double px, py, pz;
+    if (fabs(x) < 0.9) { px = 0; py = -z; pz = y; } else { px = -y; py = x; pz = 0; }
+    const double nn = sqrt(px * px + py * py + pz * pz);
+    uu[1] = px / nn; uu[4] = py / nn; uu[7] = pz / nn;
+  }
+  if (!have2 || !have1) {
+    uu[2] = uu[3] * uu[7] - uu[6] * uu[4];
+    uu[5] = uu[6] * uu[1] - uu[0] * uu[7];
+    uu[8] = uu[0] * uu[4] - uu[3] * uu[1];
+  }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double acc = 0;
+      for (int kk = 0; kk < 3; ++kk) acc += vs[i * 3 + kk] * uu[j * 3 + kk];
+      r[i * 3 + j] = acc;
+    }
+  if (det3(r) < 0.0) {
+    for (int i = 0; i < 3; ++i) vs[i * 3 + 2] = -vs[i * 3 + 2];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        double acc = 0;
+        for (int kk = 0; kk < 3; ++kk) acc += vs[i * 3 + kk] * uu[j * 3 + kk];
+        r[i * 3 + j] = acc;
+      }
+  }
+}
+
+// Rotation from the QCP eigenvector of K(H) for eigenvalue lambda: the
+// eigenvector is a column of adj(K - lambda I); the column with the largest
+// diagonal entry is the best conditioned.  Falls back to the SVD rotation when
+// the adjugate vanishes (degenerate lambda_max).
+WMD_HD void rotation_from_qcp(const double h[9], double lambda, double r[9]) {
+  double k[16];
+  key_matrix(h, k);
+  for (int i = 0; i < 4; ++i) k[i * 5] -= lambda;
+  // cofactor C_ij = (-1)^(i+j) det(minor_ij)
+  double best = -1.0;
+  int m = 0;
+  double diag[4];
+  for (int i = 0; i < 4; ++i) {
+    int r0 = i == 0 ? 1 : 0, r1 = i <= 1 ? 2 : 1, r2 = i <= 2 ? 3 : 2;
+    const double mm[9] = {k[r0 * 4 + r0], k[r0 * 4 + r1], k[r0 * 4 + r2],
+                          k[r1 * 4 + r0], k[r1 * 4 + r1], k[r1 * 4 + r2],
+                          k[r2 * 4 + r0], k[r2 * 4 + r1], k[r2 * 4 + r2]};
+    diag[i] = det3(mm);
+    if (fabs(diag[i]) > best) { best = fabs(diag[i]); m = i; }
+  }
+  double q[4];
+  double norm2 = 0.0;
+  for (int j = 0; j < 4; ++j) {
+    if (j == m) {
+      q[j] = diag[m];
+    } else {
+      // cofactor C_mj: delete row m and column j
+      int rows[3], cols[3], nr = 0, nc = 0;
+      for (int t = 0; t < 4; ++t) {
+        if (t != m) rows[nr++] = t;
+        if (t != j) cols[nc++] = t;
+      }
+      double mm[9];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) mm[a * 3 + b] = k[rows[a] * 4 + cols[b]];
+      const double sgn = ((m + j) & 1) ? -1.0 : 1.0;
+      q[j] = sgn * det3(mm);
+    }
+    norm2 += q[j] * q[j];
+  }
+  // scale-free degeneracy test: |adj column|^2 vs (|K|_F^3)^2
+  double kf = 0.0;
+  for (int i = 0; i < 16; ++i) kf += k[i] * k[i];
+  if (!(norm2 > 1e-24 * kf * kf * kf)) {
+    rotation_from_svd(h, r);
+    return;
+  }
+  const double inv = 1.0 / sqrt(norm2);
+  const double w = q[0] * inv, x = q[1] * inv, y = q[2] * inv, z = q[3] * inv;
+  r[0] = w * w + x * x - y * y - z * z;
+  r[1] = 2.0 * (x * y - w * z);
+  r[2] = 2.0 * (x * z + w * y);
+  r[3] = 2.0 * (x * y + w * z);
+  r[4] = w * w - x * x + y * y - z * z;
+  r[5] = 2.0 * (y * z - w * x);
+  r[6] = 2.0 * (x * z - w * y);
+  r[7] = 2.0 * (y * z + w * x);
+  r[8] = w * w - x * x - y * y + z * z;
+}
+
+}  // namespace wmd

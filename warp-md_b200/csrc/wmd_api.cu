@@ -1,0 +1,669 @@
+// wmd_api.cu -- host side of libwarpmd_rmsd.so: the C ABI declared in
+// include/warpmd_rmsd.h.
+//
+// Plays the role of the reference's GpuContext (crates/traj-gpu/src/cuda.rs,
+// crates/traj-gpu/src/cuda/runtime_core.rs:375-535) without runtime
+// compilation: kernels are built ahead of time for sm_100a.  Differences by
+// design:
+//   * host inputs are streamed in chunks through two device buffers, with the
+//     host->device copy of chunk k+1 (copy stream) overlapping the kernel of
+//     chunk k (caller's stream), instead of one synchronous clone_htod per
+//     chunk followed by three synchronous downloads;
+//   * the reference is centred once, in FP64, at upload time;
+//   * the per-frame QCP runs on the device in the same launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/warpmd_rmsd.h"
+#include "pairwise.h"
+#include "wmd_internal.h"
+
+#define WMD_EXPORT extern "C" __attribute__((visibility("default")))
+
+namespace {
+
+constexpr const char* kVersion = "0.4.30+b200.1";
+// Host-input chunk size for the streaming pipeline.
+constexpr size_t kChunkBytes = size_t(256) << 20;
+// Scratch bound for one forward launch's tile partials.
+constexpr size_t kPartialBytesMax = size_t(512) << 20;
+
+thread_local std::string g_create_error;
+
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+struct HostBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct wmd_ref {
+  double* yc = nullptr;
+  wmd::RefInfo info;
+};
+
+struct wmd_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t h2d_done[2] = {nullptr, nullptr};
+  cudaEvent_t kern_done[2] = {nullptr, nullptr};
+  int* status_host = nullptr;  // mapped pinned word the kernels report into
+  int* status_dev = nullptr;
+  DevBuf partial, counter, rot, chunk[2], out_tmp, sel_buf, aux;
+  HostBuf stage[2];
+  std::string err;
+  wmd::PairwiseWorkspace pw;
+};
+
+namespace {
+
+int set_err(wmd_ctx* ctx, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (ctx) ctx->err = buf;
+  else g_create_error = buf;
+  return code;
+}
+
+int cuda_err(wmd_ctx* ctx, cudaError_t e, const char* what) {
+  // same wording as the reference's map_driver_err (crates/traj-gpu/src/cuda.rs:384-386)
+  return set_err(ctx, e == cudaErrorMemoryAllocation ? WMD_ERR_OOM : WMD_ERR_CUDA, "cuda driver error: %s: %s",
+                 what, cudaGetErrorString(e));
+}
+
+#define CU(call, what)                                  \
+  do {                                                  \
+    cudaError_t _e = (call);                            \
+    if (_e != cudaSuccess) return cuda_err(ctx, _e, what); \
+  } while (0)
+
+// Keeps the caller's current device across a call.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+enum class Mem { Null, Device, PinnedHost, PageableHost };
+
+Mem classify(const void* p) {
+  if (!p) return Mem::Null;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return Mem::PageableHost;
+  }
+  switch (a.type) {
+    case cudaMemoryTypeDevice:
+    case cudaMemoryTypeManaged:
+      return Mem::Device;
+    case cudaMemoryTypeHost:
+      return Mem::PinnedHost;
+    default:
+      return Mem::PageableHost;
+  }
+}
+
+bool is_host(Mem m) { return m == Mem::PinnedHost || m == Mem::PageableHost; }
+
+int ensure(wmd_ctx* ctx, DevBuf& b, size_t bytes, bool zero = false) {
+  if (b.bytes >= bytes && b.ptr) return WMD_OK;
+  if (b.ptr) {
+    cudaFree(b.ptr);  // synchronizes the device: no launch still uses it
+    b.ptr = nullptr;
+    b.bytes = 0;
+  }
+  size_t want = std::max<size_t>(bytes, 256);
+  cudaError_t e = cudaMalloc(&b.ptr, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    b.ptr = nullptr;
+    return set_err(ctx, WMD_ERR_OOM, "cuda driver error: device allocation of %zu bytes failed: %s", want,
+                   cudaGetErrorString(e));
+  }
+  b.bytes = want;
+  if (zero) {
+    e = cudaMemset(b.ptr, 0, want);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "cudaMemset");
+  }
+  return WMD_OK;
+}
+
+int ensure_host(wmd_ctx* ctx, HostBuf& b, size_t bytes) {
+  if (b.bytes >= bytes && b.ptr) return WMD_OK;
+  if (b.ptr) {
+    cudaFreeHost(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+  }
+  cudaError_t e = cudaHostAlloc(&b.ptr, bytes, cudaHostAllocPortable);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    b.ptr = nullptr;
+    return set_err(ctx, WMD_ERR_OOM, "pinned host allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+  }
+  b.bytes = bytes;
+  return WMD_OK;
+}
+
+// Reports timeouts / bad indices recorded by earlier kernels.
+int check_status(wmd_ctx* ctx) {
+  const int st = __atomic_exchange_n(ctx->status_host, 0, __ATOMIC_ACQ_REL);
+  if (st == 0) return WMD_OK;
+  // a kernel gave up mid-way: its frame counters may be dirty
+  if (ctx->counter.ptr) cudaMemset(ctx->counter.ptr, 0, ctx->counter.bytes);
+  if (st & 16) return set_err(ctx, WMD_ERR_INVALID_ARG, "selection index out of range (status 0x%x)", st);
+  return set_err(ctx, WMD_ERR_TIMEOUT, "a device-side wait exceeded its limit (status 0x%x)", st);
+}
+
+int check_common(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                 const uint32_t* sel, int64_t n_sel, const wmd_ref* ref) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  if (!ref) return set_err(ctx, WMD_ERR_INVALID_ARG, "reference is null");
+  if (stride != 3 && stride != 4) return set_err(ctx, WMD_ERR_INVALID_ARG, "stride must be 3 or 4 (got %d)", stride);
+  if (n_frames < 0 || n_atoms < 0 || n_sel < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "negative size");
+  if (n_frames > 0 && !coords) return set_err(ctx, WMD_ERR_INVALID_ARG, "coords is null");
+  if (n_sel != ref->info.n_sel)
+    return set_err(ctx, WMD_ERR_MISMATCH, "reference has %lld atoms but the selection has %lld",
+                   (long long)ref->info.n_sel, (long long)n_sel);
+  if (!sel && n_sel > n_atoms)
+    return set_err(ctx, WMD_ERR_MISMATCH, "selection of %lld atoms exceeds the frame's %lld atoms", (long long)n_sel,
+                   (long long)n_atoms);
+  return WMD_OK;
+}
+
+// Resolves the selection to a device pointer, validating host indices.
+int resolve_sel(wmd_ctx* ctx, const uint32_t* sel, int64_t n_sel, int64_t n_atoms, const uint32_t** dsel,
+                cudaStream_t s) {
+  *dsel = nullptr;
+  if (!sel) return WMD_OK;
+  const Mem m = classify(sel);
+  if (m == Mem::Device) {
+    *dsel = sel;
+    return WMD_OK;
+  }
+  for (int64_t i = 0; i < n_sel; ++i)
+    if ((int64_t)sel[i] >= n_atoms)
+      return set_err(ctx, WMD_ERR_INVALID_ARG, "selection index %u out of range for %lld atoms", sel[i],
+                     (long long)n_atoms);
+  int rc = ensure(ctx, ctx->sel_buf, (size_t)n_sel * 4);
+  if (rc) return rc;
+  CU(cudaMemcpyAsync(ctx->sel_buf.ptr, sel, (size_t)n_sel * 4, cudaMemcpyHostToDevice, s), "upload selection");
+  *dsel = static_cast<const uint32_t*>(ctx->sel_buf.ptr);
+  return WMD_OK;
+}
+
+wmd::FrameLaunch base_launch(wmd_ctx* ctx, const wmd_ref* ref, int64_t n_atoms, int stride, const uint32_t* dsel) {
+  wmd::FrameLaunch L;
+  L.n_atoms = n_atoms;
+  L.stride = stride;
+  L.sel = dsel;
+  L.ref = ref->info;
+  L.ref.yc = ref->yc;
+  L.status = ctx->status_dev;
+  L.tile_atoms = wmd::kConsumerThreads * 4;
+  return L;
+}
+
+// Runs the forward over device-resident frames, splitting into frame batches
+// so the tile-partial scratch stays bounded.  `o` points at frame 0 outputs.
+int forward_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames, int64_t n_atoms, int stride,
+                   const uint32_t* dsel, const wmd_ref* ref, int align, wmd::FrameOutputs o, cudaStream_t s) {
+  if (n_frames == 0) return WMD_OK;
+  wmd::FrameLaunch L = base_launch(ctx, ref, n_atoms, stride, dsel);
+  L.align = align;
+  L.gather = dsel != nullptr || (reinterpret_cast<uintptr_t>(dcoords) & 15u) != 0;
+  const int tiles = wmd::frame_tiles(L);
+  const size_t per_frame = (size_t)tiles * wmd::kStatDoubles * sizeof(double);
+  int64_t batch = n_frames;
+  if (tiles > 1) {
+    batch = std::max<int64_t>(1, (int64_t)(kPartialBytesMax / per_frame));
+    batch = std::min(batch, n_frames);
+    int rc = ensure(ctx, ctx->partial, per_frame * (size_t)batch);
+    if (rc) return rc;
+    rc = ensure(ctx, ctx->counter, (size_t)batch * sizeof(unsigned), true);
+    if (rc) return rc;
+  }
+  for (int64_t f0 = 0; f0 < n_frames; f0 += batch) {
+    const int64_t nf = std::min(batch, n_frames - f0);
+    wmd::FrameLaunch B = L;
+    B.coords = dcoords + (size_t)f0 * n_atoms * stride;
+    B.n_frames = nf;
+    B.out.rmsd = o.rmsd ? o.rmsd + f0 : nullptr;
+    B.out.stats = o.stats ? o.stats + f0 * wmd::kStatDoubles : nullptr;
+    B.out.cov = o.cov ? o.cov + f0 * 9 : nullptr;
+    B.out.sum_x2 = o.sum_x2 ? o.sum_x2 + f0 : nullptr;
+    B.out.sum_y2 = o.sum_y2 ? o.sum_y2 + f0 : nullptr;
+    B.partial = static_cast<double*>(ctx->partial.ptr);
+    B.counter = static_cast<unsigned*>(ctx->counter.ptr);
+    B.grid = wmd::frame_grid(B, ctx->sm_count, false);
+    CU(wmd::launch_rmsd_forward(B, s), "rmsd forward launch");
+  }
+  return WMD_OK;
+}
+
+// Host-resident frames: chunked double-buffered H2D overlapping the kernels.
+int forward_host(wmd_ctx* ctx, const float* hcoords, Mem kind, int64_t n_frames, int64_t n_atoms, int stride,
+                 const uint32_t* dsel, const wmd_ref* ref, int align, wmd::FrameOutputs o, cudaStream_t s) {
+  const size_t frame_bytes = (size_t)n_atoms * stride * sizeof(float);
+  if (frame_bytes == 0) return forward_device(ctx, nullptr, 0, n_atoms, stride, dsel, ref, align, o, s);
+  const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(n_frames, (int64_t)(kChunkBytes / frame_bytes)));
+  const size_t chunk_bytes = (size_t)chunk * frame_bytes;
+  for (int b = 0; b < 2; ++b) {
+    int rc = ensure(ctx, ctx->chunk[b], chunk_bytes);
+    if (rc) return rc;
+    if (kind == Mem::PageableHost) {
+      rc = ensure_host(ctx, ctx->stage[b], chunk_bytes);
+      if (rc) return rc;
+    }
+  }
+  // the buffers may have been used by earlier work on other streams
+  CU(cudaEventRecord(ctx->kern_done[0], s), "event");
+  CU(cudaEventRecord(ctx->kern_done[1], s), "event");
+  CU(cudaEventRecord(ctx->h2d_done[0], ctx->copy_stream), "event");
+  CU(cudaEventRecord(ctx->h2d_done[1], ctx->copy_stream), "event");
+  int64_t k = 0;
+  for (int64_t f0 = 0; f0 < n_frames; f0 += chunk, ++k) {
+    const int b = (int)(k & 1);
+    const int64_t nf = std::min(chunk, n_frames - f0);
+    const size_t bytes = (size_t)nf * frame_bytes;
+    const char* src = reinterpret_cast<const char*>(hcoords) + (size_t)f0 * frame_bytes;
+    if (kind == Mem::PageableHost) {
+      CU(cudaEventSynchronize(ctx->h2d_done[b]), "staging wait");
+      std::memcpy(ctx->stage[b].ptr, src, bytes);
+      src = static_cast<const char*>(ctx->stage[b].ptr);
+    }
+    CU(cudaStreamWaitEvent(ctx->copy_stream, ctx->kern_done[b], 0), "stream wait");
+    CU(cudaMemcpyAsync(ctx->chunk[b].ptr, src, bytes, cudaMemcpyHostToDevice, ctx->copy_stream), "H2D");
+    CU(cudaEventRecord(ctx->h2d_done[b], ctx->copy_stream), "event");
+    CU(cudaStreamWaitEvent(s, ctx->h2d_done[b], 0), "stream wait");
+    wmd::FrameOutputs oc;
+    oc.rmsd = o.rmsd ? o.rmsd + f0 : nullptr;
+    oc.stats = o.stats ? o.stats + f0 * wmd::kStatDoubles : nullptr;
+    oc.cov = o.cov ? o.cov + f0 * 9 : nullptr;
+    oc.sum_x2 = o.sum_x2 ? o.sum_x2 + f0 : nullptr;
+    oc.sum_y2 = o.sum_y2 ? o.sum_y2 + f0 : nullptr;
+    int rc = forward_device(ctx, static_cast<const float*>(ctx->chunk[b].ptr), nf, n_atoms, stride, dsel, ref, align,
+                            oc, s);
+    if (rc) return rc;
+    CU(cudaEventRecord(ctx->kern_done[b], s), "event");
+  }
+  return WMD_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+WMD_EXPORT const char* wmd_version(void) { return kVersion; }
+
+WMD_EXPORT const char* wmd_last_error(const wmd_ctx* ctx) {
+  return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}
+
+WMD_EXPORT int wmd_create(int device, wmd_ctx** out) {
+  if (!out) return set_err(nullptr, WMD_ERR_INVALID_ARG, "out is null");
+  *out = nullptr;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return set_err(nullptr, WMD_ERR_NO_DEVICE, "no CUDA device available (%s)",
+                   e == cudaSuccess ? "device count is 0" : cudaGetErrorString(e));
+  }
+  if (device < 0 || device >= n)
+    return set_err(nullptr, WMD_ERR_INVALID_ARG, "invalid cuda device index %d (have %d)", device, n);
+  cudaDeviceProp prop;
+  if ((e = cudaGetDeviceProperties(&prop, device)) != cudaSuccess)
+    return set_err(nullptr, WMD_ERR_CUDA, "cuda driver error: %s", cudaGetErrorString(e));
+  if (prop.major != 10)
+    return set_err(nullptr, WMD_ERR_NO_DEVICE, "device %d is sm_%d%d; this library is built for sm_100a (B200)", device,
+                   prop.major, prop.minor);
+  DeviceGuard g(device);
+  wmd_ctx* ctx = new wmd_ctx();
+  ctx->device = device;
+  ctx->sm_count = prop.multiProcessorCount;
+  auto fail = [&](cudaError_t ee, const char* what) {
+    std::string msg = std::string("cuda driver error: ") + what + ": " + cudaGetErrorString(ee);
+    wmd_destroy(ctx);
+    return set_err(nullptr, WMD_ERR_CUDA, "%s", msg.c_str());
+  };
+  if ((e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return fail(e, "stream");
+  for (int b = 0; b < 2; ++b) {
+    if ((e = cudaEventCreateWithFlags(&ctx->h2d_done[b], cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+    if ((e = cudaEventCreateWithFlags(&ctx->kern_done[b], cudaEventDisableTiming)) != cudaSuccess)
+      return fail(e, "event");
+  }
+  if ((e = cudaHostAlloc(&ctx->status_host, sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable)) != cudaSuccess)
+    return fail(e, "status word");
+  *ctx->status_host = 0;
+  if ((e = cudaHostGetDevicePointer(&ctx->status_dev, ctx->status_host, 0)) != cudaSuccess) return fail(e, "status word");
+  *out = ctx;
+  return WMD_OK;
+}
+
+WMD_EXPORT int wmd_destroy(wmd_ctx* ctx) {
+  if (!ctx) return WMD_OK;
+  DeviceGuard g(ctx->device);
+  cudaDeviceSynchronize();
+  for (DevBuf* b : {&ctx->partial, &ctx->counter, &ctx->rot, &ctx->chunk[0], &ctx->chunk[1], &ctx->out_tmp,
+                    &ctx->sel_buf, &ctx->aux})
+    if (b->ptr) cudaFree(b->ptr);
+  for (HostBuf* b : {&ctx->stage[0], &ctx->stage[1]})
+    if (b->ptr) cudaFreeHost(b->ptr);
+  wmd::pairwise_workspace_free(ctx->pw);
+  for (int b = 0; b < 2; ++b) {
+    if (ctx->h2d_done[b]) cudaEventDestroy(ctx->h2d_done[b]);
+    if (ctx->kern_done[b]) cudaEventDestroy(ctx->kern_done[b]);
+  }
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  if (ctx->status_host) cudaFreeHost(ctx->status_host);
+  delete ctx;
+  return WMD_OK;
+}
+
+WMD_EXPORT int wmd_reference_upload(wmd_ctx* ctx, const float* ref, int64_t n_sel, int stride, wmd_ref** out) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  if (!out) return set_err(ctx, WMD_ERR_INVALID_ARG, "out is null");
+  *out = nullptr;
+  if (stride != 3 && stride != 4) return set_err(ctx, WMD_ERR_INVALID_ARG, "stride must be 3 or 4 (got %d)", stride);
+  if (n_sel < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "negative size");
+  if (n_sel > 0 && !ref) return set_err(ctx, WMD_ERR_INVALID_ARG, "reference is null");
+  DeviceGuard g(ctx->device);
+  std::vector<float> host;
+  const float* h = ref;
+  if (n_sel > 0 && classify(ref) == Mem::Device) {
+    host.resize((size_t)n_sel * stride);
+    CU(cudaMemcpy(host.data(), ref, host.size() * sizeof(float), cudaMemcpyDeviceToHost), "download reference");
+    h = host.data();
+  }
+  wmd_ref* r = new wmd_ref();
+  wmd::RefInfo& I = r->info;
+  I.n_sel = n_sel;
+  std::vector<double> yc((size_t)std::max<int64_t>(n_sel, 1) * 3, 0.0);
+  if (n_sel > 0) {
+    // FP64 two-pass centring, as rmsd_aligned_selected does (plan.rs:1172-1190)
+    double m[3] = {0, 0, 0};
+    for (int64_t i = 0; i < n_sel; ++i)
+      for (int c = 0; c < 3; ++c) m[c] += (double)h[i * stride + c];
+    for (int c = 0; c < 3; ++c) I.mean[c] = m[c] / (double)n_sel;
+    double sumsq = 0;
+    for (int64_t i = 0; i < n_sel; ++i)
+      for (int c = 0; c < 3; ++c) {
+        const double y = (double)h[i * stride + c];
+        yc[i * 3 + c] = y - I.mean[c];
+        I.sum_c[c] += yc[i * 3 + c];
+        sumsq += y * y;
+      }
+    I.sumsq = sumsq;
+    double gy = 0;
+    for (int64_t i = 0; i < n_sel; ++i)
+      for (int c = 0; c < 3; ++c) {
+        const double d = yc[i * 3 + c] - I.sum_c[c] / (double)n_sel;
+        gy += d * d;
+      }
+    I.gy = gy;
+  }
+  cudaError_t e = cudaMalloc(&r->yc, yc.size() * sizeof(double));
+  if (e != cudaSuccess) {
+    delete r;
+    cudaGetLastError();
+    return set_err(ctx, WMD_ERR_OOM, "cuda driver error: reference allocation failed: %s", cudaGetErrorString(e));
+  }
+  e = cudaMemcpy(r->yc, yc.data(), yc.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(r->yc);
+    delete r;
+    return cuda_err(ctx, e, "upload reference");
+  }
+  I.yc = r->yc;
+  *out = r;
+  return WMD_OK;
+}
+
+WMD_EXPORT int wmd_reference_free(wmd_ctx* ctx, wmd_ref* ref) {
+  if (!ref) return WMD_OK;
+  if (ctx) {
+    DeviceGuard g(ctx->device);
+    cudaFree(ref->yc);
+  } else {
+    cudaFree(ref->yc);
+  }
+  delete ref;
+  return WMD_OK;
+}
+
+static int frames_common(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                         const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, int align, wmd::FrameOutputs o_user,
+                         bool outputs_host, cudaStream_t s) {
+  const Mem cm = classify(coords);
+  const uint32_t* dsel = nullptr;
+  int rc = resolve_sel(ctx, sel, n_sel, n_atoms, &dsel, s);
+  if (rc) return rc;
+  if (n_sel == 0) {
+    // the reference returns 0.0 for every frame (plan.rs:1166-1168)
+    if (o_user.rmsd) {
+      if (outputs_host) std::fill(o_user.rmsd, o_user.rmsd + n_frames, 0.0);
+      else CU(cudaMemsetAsync(o_user.rmsd, 0, (size_t)n_frames * sizeof(double), s), "memset");
+    }
+    return WMD_OK;
+  }
+  // outputs staged through device memory when the caller's are host memory
+  wmd::FrameOutputs o = o_user;
+  size_t off_rmsd = 0, off_cov = 0, off_x2 = 0, off_y2 = 0, total = 0;
+  if (outputs_host) {
+    auto take = [&](size_t bytes) { size_t at = total; total += (bytes + 255) & ~size_t(255); return at; };
+    if (o_user.rmsd) off_rmsd = take((size_t)n_frames * sizeof(double));
+    if (o_user.cov) off_cov = take((size_t)n_frames * 9 * sizeof(float));
+    if (o_user.sum_x2) off_x2 = take((size_t)n_frames * sizeof(float));
+    if (o_user.sum_y2) off_y2 = take((size_t)n_frames * sizeof(float));
+    rc = ensure(ctx, ctx->out_tmp, total);
+    if (rc) return rc;
+    char* base = static_cast<char*>(ctx->out_tmp.ptr);
+    o.rmsd = o_user.rmsd ? reinterpret_cast<double*>(base + off_rmsd) : nullptr;
+    o.cov = o_user.cov ? reinterpret_cast<float*>(base + off_cov) : nullptr;
+    o.sum_x2 = o_user.sum_x2 ? reinterpret_cast<float*>(base + off_x2) : nullptr;
+    o.sum_y2 = o_user.sum_y2 ? reinterpret_cast<float*>(base + off_y2) : nullptr;
+  }
+  if (is_host(cm)) rc = forward_host(ctx, coords, cm, n_frames, n_atoms, stride, dsel, ref, align, o, s);
+  else rc = forward_device(ctx, coords, n_frames, n_atoms, stride, dsel, ref, align, o, s);
+  if (rc) return rc;
+  if (outputs_host) {
+    if (o.rmsd) CU(cudaMemcpyAsync(o_user.rmsd, o.rmsd, (size_t)n_frames * 8, cudaMemcpyDeviceToHost, s), "D2H");
+    if (o.cov) CU(cudaMemcpyAsync(o_user.cov, o.cov, (size_t)n_frames * 36, cudaMemcpyDeviceToHost, s), "D2H");
+    if (o.sum_x2) CU(cudaMemcpyAsync(o_user.sum_x2, o.sum_x2, (size_t)n_frames * 4, cudaMemcpyDeviceToHost, s), "D2H");
+    if (o.sum_y2) CU(cudaMemcpyAsync(o_user.sum_y2, o.sum_y2, (size_t)n_frames * 4, cudaMemcpyDeviceToHost, s), "D2H");
+  }
+  if (outputs_host || is_host(cm) || (sel && classify(sel) != Mem::Device)) {
+    CU(cudaStreamSynchronize(s), "synchronize");
+    return check_status(ctx);
+  }
+  return WMD_OK;
+}
+
+WMD_EXPORT int wmd_rmsd_frames(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                               const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, int align, double* out,
+                               void* stream) {
+  int rc = check_common(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, ref);
+  if (rc) return rc;
+  if (n_frames > 0 && !out) return set_err(ctx, WMD_ERR_INVALID_ARG, "out is null");
+  DeviceGuard g(ctx->device);
+  if ((rc = check_status(ctx))) return rc;
+  if (n_frames == 0) return WMD_OK;
+  wmd::FrameOutputs o;
+  o.rmsd = out;
+  return frames_common(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, ref, align, o, is_host(classify(out)),
+                       static_cast<cudaStream_t>(stream));
+}
+
+WMD_EXPORT int wmd_rmsd_covariance(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                                   const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, float* cov, float* sum_x2,
+                                   float* sum_y2, void* stream) {
+  int rc = check_common(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, ref);
+  if (rc) return rc;
+  if (n_frames > 0 && (!cov || !sum_x2 || !sum_y2)) return set_err(ctx, WMD_ERR_INVALID_ARG, "output is null");
+  DeviceGuard g(ctx->device);
+  if ((rc = check_status(ctx))) return rc;
+  if (n_frames == 0) return WMD_OK;
+  const bool oh = is_host(classify(cov));
+  if (oh != is_host(classify(sum_x2)) || oh != is_host(classify(sum_y2)))
+    return set_err(ctx, WMD_ERR_INVALID_ARG, "cov, sum_x2 and sum_y2 must all be host or all be device memory");
+  if (n_sel == 0) {
+    // covariance of an empty selection is zero
+    if (oh) {
+      std::fill(cov, cov + n_frames * 9, 0.f);
+      std::fill(sum_x2, sum_x2 + n_frames, 0.f);
+      std::fill(sum_y2, sum_y2 + n_frames, 0.f);
+      return WMD_OK;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    CU(cudaMemsetAsync(cov, 0, (size_t)n_frames * 36, s), "memset");
+    CU(cudaMemsetAsync(sum_x2, 0, (size_t)n_frames * 4, s), "memset");
+    CU(cudaMemsetAsync(sum_y2, 0, (size_t)n_frames * 4, s), "memset");
+    return WMD_OK;
+  }
+  wmd::FrameOutputs o;
+  o.cov = cov;
+  o.sum_x2 = sum_x2;
+  o.sum_y2 = sum_y2;
+  return frames_common(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, ref, 1, o, oh,
+                       static_cast<cudaStream_t>(stream));
+}
+
+static int require_device(wmd_ctx* ctx, const void* p, const char* name) {
+  if (p && classify(p) != Mem::Device)
+    return set_err(ctx, WMD_ERR_INVALID_ARG, "%s must be device memory for this entry point", name);
+  return WMD_OK;
+}
+
+WMD_EXPORT int wmd_rmsd_forward(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                                const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, double* out, double* stats,
+                                void* stream) {
+  int rc = check_common(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, ref);
+  if (rc) return rc;
+  DeviceGuard g(ctx->device);
+  if ((rc = check_status(ctx))) return rc;
+  if (n_frames == 0) return WMD_OK;
+  if ((rc = require_device(ctx, coords, "coords")) || (rc = require_device(ctx, sel, "sel")) ||
+      (rc = require_device(ctx, out, "out")) || (rc = require_device(ctx, stats, "stats")))
+    return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (n_sel == 0) {
+    if (out) CU(cudaMemsetAsync(out, 0, (size_t)n_frames * 8, s), "memset");
+    if (stats) CU(cudaMemsetAsync(stats, 0, (size_t)n_frames * wmd::kStatDoubles * 8, s), "memset");
+    return WMD_OK;
+  }
+  wmd::FrameOutputs o;
+  o.rmsd = out;
+  o.stats = stats;
+  return forward_device(ctx, coords, n_frames, n_atoms, stride, sel, ref, 1, o, s);
+}
+
+WMD_EXPORT int wmd_rmsd_backward(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                                 const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, const double* stats,
+                                 const float* grad_rmsd, float* grad, void* stream) {
+  int rc = check_common(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, ref);
+  if (rc) return rc;
+  DeviceGuard g(ctx->device);
+  if ((rc = check_status(ctx))) return rc;
+  if (n_frames == 0 || n_sel == 0) return WMD_OK;
+  if (!stats || !grad) return set_err(ctx, WMD_ERR_INVALID_ARG, "stats and grad are required");
+  if ((rc = require_device(ctx, coords, "coords")) || (rc = require_device(ctx, sel, "sel")) ||
+      (rc = require_device(ctx, stats, "stats")) || (rc = require_device(ctx, grad_rmsd, "grad_rmsd")) ||
+      (rc = require_device(ctx, grad, "grad")))
+    return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  rc = ensure(ctx, ctx->rot, (size_t)n_frames * wmd::kStatDoubles * sizeof(double));
+  if (rc) return rc;
+  wmd::FrameLaunch L = base_launch(ctx, ref, n_atoms, stride, sel);
+  L.coords = coords;
+  L.n_frames = n_frames;
+  L.gather = sel != nullptr || (reinterpret_cast<uintptr_t>(coords) & 15u) != 0;
+  L.grad = grad;
+  L.grid = wmd::frame_grid(L, ctx->sm_count, true);
+  CU(wmd::launch_rmsd_backward(L, stats, grad_rmsd, static_cast<double*>(ctx->rot.ptr), s), "rmsd backward launch");
+  return WMD_OK;
+}
+
+WMD_EXPORT int wmd_pairwise_rmsd(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                                 const uint32_t* sel, int64_t n_sel, int metric, int mode, float* out, void* stream) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  if (stride != 3 && stride != 4) return set_err(ctx, WMD_ERR_INVALID_ARG, "stride must be 3 or 4 (got %d)", stride);
+  if (n_frames < 0 || n_atoms < 0 || n_sel < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "negative size");
+  if (metric != WMD_PAIR_RMS && metric != WMD_PAIR_NOFIT)
+    return set_err(ctx, WMD_ERR_UNSUPPORTED, "pairwise metric %d is not provided (rms=0, nofit=1)", metric);
+  if (mode < WMD_MODE_FP32 || mode > WMD_MODE_FP64)
+    return set_err(ctx, WMD_ERR_INVALID_ARG, "unknown pairwise mode %d", mode);
+  if (n_frames > 0 && (!coords || !out)) return set_err(ctx, WMD_ERR_INVALID_ARG, "coords/out is null");
+  if (!sel && n_sel > n_atoms)
+    return set_err(ctx, WMD_ERR_MISMATCH, "selection of %lld atoms exceeds the frame's %lld atoms", (long long)n_sel,
+                   (long long)n_atoms);
+  DeviceGuard g(ctx->device);
+  int rc = check_status(ctx);
+  if (rc) return rc;
+  if (n_frames == 0) return WMD_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const Mem cm = classify(coords), om = classify(out);
+  const uint32_t* dsel = nullptr;
+  if ((rc = resolve_sel(ctx, sel, n_sel, n_atoms, &dsel, s))) return rc;
+  const float* dcoords = coords;
+  if (is_host(cm)) {
+    const size_t bytes = (size_t)n_frames * n_atoms * stride * sizeof(float);
+    if ((rc = ensure(ctx, ctx->aux, bytes))) return rc;
+    CU(cudaMemcpyAsync(ctx->aux.ptr, coords, bytes, cudaMemcpyHostToDevice, s), "H2D");
+    dcoords = static_cast<const float*>(ctx->aux.ptr);
+  }
+  float* dout = out;
+  const size_t out_bytes = (size_t)n_frames * n_frames * sizeof(float);
+  if (is_host(om)) {
+    if ((rc = ensure(ctx, ctx->out_tmp, out_bytes))) return rc;
+    dout = static_cast<float*>(ctx->out_tmp.ptr);
+  }
+  std::string msg;
+  const int prc = wmd::pairwise_run(ctx->pw, ctx->sm_count, dcoords, n_frames, n_atoms, stride, dsel, n_sel, metric,
+                                    mode, dout, ctx->status_dev, s, &msg);
+  if (prc) return set_err(ctx, prc, "%s", msg.c_str());
+  if (is_host(om)) CU(cudaMemcpyAsync(out, dout, out_bytes, cudaMemcpyDeviceToHost, s), "D2H");
+  if (is_host(om) || is_host(cm) || (sel && classify(sel) != Mem::Device)) {
+    CU(cudaStreamSynchronize(s), "synchronize");
+    return check_status(ctx);
+  }
+  return WMD_OK;
+}
+
+WMD_EXPORT int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, int n_traj, int with_grad) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  (void)descs; (void)n_traj; (void)with_grad;
+  return set_err(ctx, WMD_ERR_UNSUPPORTED, "batched launch not built yet");
+}
+
+WMD_EXPORT int wmd_batched_rmsd(wmd_ctx* ctx, const wmd_batch_desc* descs, int n_traj, int with_grad, void* stream) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  (void)descs; (void)n_traj; (void)with_grad; (void)stream;
+  return set_err(ctx, WMD_ERR_UNSUPPORTED, "batched launch not built yet");
+}

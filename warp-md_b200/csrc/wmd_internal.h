@@ -1,0 +1,65 @@
+// wmd_internal.h -- launch parameters shared between the host API
+// (wmd_api.cu) and the kernel files.  Not part of the public C ABI.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace wmd {
+
+// Per-frame kernel geometry: 8 consumer warps + 1 producer warp per CTA; each
+// consumer thread owns kAtomsPerThread atoms of an atom tile, whose reference
+// coordinates it keeps in registers (FP64, centred) while frames stream past.
+constexpr int kConsumerWarps = 8;
+constexpr int kConsumerThreads = kConsumerWarps * 32;
+constexpr int kThreads = kConsumerThreads + 32;
+constexpr int kStatDoubles = 16;  // per-frame / per-tile partial record
+
+// Which outputs a per-frame forward launch writes.
+struct FrameOutputs {
+  double* rmsd = nullptr;   // [n_frames]
+  double* stats = nullptr;  // [n_frames][16]
+  float* cov = nullptr;     // [n_frames][9]
+  float* sum_x2 = nullptr;  // [n_frames]
+  float* sum_y2 = nullptr;  // [n_frames]
+};
+
+struct RefInfo {
+  const double* yc = nullptr;  // device [n_sel][3]: y - mean(y) in FP64
+  int64_t n_sel = 0;
+  double sum_c[3] = {0, 0, 0};  // sum of yc (round-off residue of the centring)
+  double gy = 0;                // sum |yc - mean(yc)|^2
+  double mean[3] = {0, 0, 0};   // mean(y), for the no-fit RMSD
+  double sumsq = 0;             // sum |y|^2, for the no-fit RMSD
+};
+
+struct FrameLaunch {
+  const float* coords = nullptr;  // device, frames of this launch
+  int64_t n_frames = 0;
+  int64_t n_atoms = 0;            // frame stride in atoms
+  int stride = 3;                 // floats per atom (3 or 4)
+  const uint32_t* sel = nullptr;  // device indices, or null (dense 0..n_sel-1)
+  bool gather = false;            // plain loads (selection or unaligned base)
+  int tile_atoms = 2048;          // atoms per tile (kConsumerThreads * atoms/thread)
+  int align = 1;
+  RefInfo ref;
+  FrameOutputs out;
+  // backward
+  const double* rot = nullptr;  // [n_frames][16] from the backward prologue
+  float* grad = nullptr;        // [n_frames][n_atoms][3]
+  // scratch
+  double* partial = nullptr;    // [n_frames][n_tiles][16]
+  unsigned* counter = nullptr;  // [n_frames], zero between launches
+  int* status = nullptr;        // device-visible status word (mapped host)
+  int grid = 0;                 // CTAs (persistent)
+};
+
+int frame_tiles(const FrameLaunch& L);
+size_t frame_smem_bytes(int stride, int tile_atoms);
+cudaError_t launch_rmsd_forward(const FrameLaunch& L, cudaStream_t s);
+cudaError_t launch_rmsd_backward(const FrameLaunch& L, const double* stats, const float* grad_rmsd,
+                                 double* rot_scratch, cudaStream_t s);
+// occupancy-derived persistent grid for a launch
+int frame_grid(const FrameLaunch& L, int sm_count, bool backward);
+
+}  // namespace wmd

@@ -1,0 +1,53 @@
+"""``pairwise_rmsd`` wrapper with the reference's arguments
+(python/warp_md/analysis/rmsd.py:244-283): metric aliases ("srmsd" -> "rms"),
+``mat_type`` "full" (N x N) or "half" (upper triangle, k=1, as float32)."""
+from __future__ import annotations
+
+from typing import Optional, Sequence
+
+import numpy as np
+
+from ..core import System, Trajectory
+from ..plans import PairwiseRmsdPlan
+
+
+def pairwise_rmsd(
+    traj: Trajectory,
+    system: System,
+    mask: str = "",
+    metric: str = "rms",
+    mat_type: str = "full",
+    pbc: str = "none",
+    length_scale: float = 1.0,
+    frame_indices: Optional[Sequence[int]] = None,
+    chunk_frames: Optional[int] = None,
+    device: str = "auto",
+    mode: str = "fp64",
+) -> np.ndarray:
+    """Compute pairwise RMSD matrix (rms, nofit, srmsd)."""
+    metric = metric.lower()
+    if metric == "srmsd":
+        metric = "rms"
+    if metric not in ("rms", "nofit", "dme"):
+        raise ValueError("metric must be 'rms', 'nofit', 'dme', or 'srmsd'")
+    mat_type = mat_type.lower()
+    if mat_type not in ("full", "half"):
+        raise ValueError("mat_type must be 'full' or 'half'")
+    pbc = pbc.lower()
+    if pbc not in ("none", "orthorhombic"):
+        raise ValueError("pbc must be 'none' or 'orthorhombic'")
+    sel = system.select(mask if mask else "all")
+    t = traj
+    if length_scale != 1.0:
+        t = Trajectory.from_numpy(traj.coords * np.float32(length_scale))
+    values = PairwiseRmsdPlan(sel, metric=metric, pbc=pbc, mode=mode).run(
+        t, system, chunk_frames=chunk_frames, device=device, frame_indices=frame_indices)
+    if mat_type == "full":
+        return values
+    if values.size == 0:
+        return np.empty((0,), dtype=np.float32)
+    tri = np.triu_indices(values.shape[0], k=1)
+    return np.asarray(values[tri], dtype=np.float32)
+
+
+__all__ = ["pairwise_rmsd"]

@@ -1,0 +1,171 @@
+"""RmsdPlan and PairwiseRmsdPlan with the reference's constructor and run()
+signatures (crates/traj-py/src/io.rs:2617-2659 and 2759-2802).
+
+The reference streams FrameChunks of ``chunk_frames`` frames through
+``Plan::process_chunk_selected`` (crates/traj-engine/src/executor.rs:471-512)
+and, for RmsdPlan, runs rmsd_aligned_selected per frame
+(crates/traj-engine/src/plans/rmsd/plan.rs:1161-1248).  Here the whole call is
+one C-ABI call: the library streams host frames to the device in chunks and
+runs the fused per-frame kernel.  Results are float32 like the reference
+(``dtype=np.float64`` gives the unrounded values).
+"""
+from __future__ import annotations
+
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _native as N
+from .core import Selection, System, Trajectory
+
+_PAIR_MODES = {"fp32": N.MODE_FP32, "i8x3": N.MODE_I8X3, "i8x2": N.MODE_I8X2, "fp64": N.MODE_FP64}
+
+
+def parse_device(device: str) -> int:
+    """Device::from_spec (crates/traj-engine/src/executor.rs:21-52) restricted
+    to CUDA: "auto" and "cuda" mean device 0, "cuda:N" device N."""
+    spec = (device or "").strip().lower()
+    if spec == "cpu":
+        raise N.WarpMdError(N.WMD_ERR_UNSUPPORTED,
+                            "unsupported: this warp_md build runs the RMSD plans on CUDA (sm_100a) only")
+    if spec in ("auto", "cuda"):
+        return 0
+    if spec.startswith("cuda"):
+        head, _, tail = spec.partition(":")
+        if head != "cuda" or not tail or ":" in tail:
+            raise RuntimeError(f"parse error: invalid cuda device spec '{device}'")
+        try:
+            return int(tail)
+        except ValueError:
+            raise RuntimeError(f"parse error: invalid cuda device spec '{device}'") from None
+    raise RuntimeError(f"unsupported: unknown device spec '{device}'")
+
+
+def parse_reference(value: str) -> str:
+    """crates/traj-py/src/pack.rs:2627-2634"""
+    if value not in ("topology", "frame0"):
+        raise RuntimeError("reference must be 'topology' or 'frame0'")
+    return value
+
+
+def parse_pairwise_metric(value: str) -> str:
+    """crates/traj-py/src/pack.rs:2675-2684"""
+    if value not in ("rms", "nofit", "dme"):
+        raise RuntimeError("metric must be 'rms', 'nofit', or 'dme'")
+    return value
+
+
+def parse_pbc(value: str) -> str:
+    if value not in ("none", "orthorhombic"):
+        raise RuntimeError("pbc must be 'none' or 'orthorhombic'")
+    return value
+
+
+def frame_subset(n_frames: int, frame_indices: Optional[Sequence[int]]) -> Optional[np.ndarray]:
+    """run_plan_with_frame_subset (crates/traj-py/src/pack.rs:1259-1330): when any
+    index is negative all are normalised against n_frames
+    (executor.rs:210-222), dropping those out of range; otherwise negative-free
+    indices are used as given and indices past the end are dropped."""
+    if frame_indices is None:
+        return None
+    raw = [int(i) for i in frame_indices]
+    if any(i < 0 for i in raw):
+        out = [i + n_frames if i < 0 else i for i in raw]
+    else:
+        out = raw
+    return np.asarray([i for i in out if 0 <= i < n_frames], dtype=np.int64)
+
+
+def _check_inputs(traj: Trajectory, system: System, selection: Selection) -> np.ndarray:
+    if traj.n_atoms() != system.n_atoms():
+        raise RuntimeError("mismatch: trajectory atom count does not match system")
+    sel = selection.as_array()
+    if sel.size and int(sel.max()) >= traj.n_atoms():
+        raise RuntimeError("invalid selection: selection index out of range")
+    return sel
+
+
+def _dense_prefix(sel: np.ndarray) -> bool:
+    return sel.size == 0 or bool(np.array_equal(sel, np.arange(sel.size, dtype=sel.dtype)))
+
+
+class RmsdPlan:
+    """Per-frame RMSD against a reference (warp_md.RmsdPlan)."""
+
+    def __init__(self, selection: Selection, reference: str = "topology", align: bool = True):
+        self.selection = selection
+        self.reference_mode = parse_reference(reference)
+        self.align = bool(align)
+
+    def run(self, traj: Trajectory, system: System, chunk_frames: Optional[int] = None, device: str = "auto",
+            frame_indices: Optional[Sequence[int]] = None, dtype=np.float32) -> np.ndarray:
+        dev = parse_device(device)
+        sel = _check_inputs(traj, system, self.selection)
+        coords = traj.coords
+        sub = frame_subset(coords.shape[0], frame_indices)
+        if sub is not None:
+            coords = np.ascontiguousarray(coords[sub])
+        n_frames = coords.shape[0]
+        # reference structure: topology positions0 (plan.rs:188-199) or the
+        # first processed frame (plan.rs:336-342)
+        if self.reference_mode == "topology":
+            if system.positions0 is None:
+                raise RuntimeError("mismatch: no topology reference coords")
+            ref = system.positions0[sel]
+        else:
+            if n_frames == 0:
+                return np.empty(0, dtype=dtype)
+            ref = coords[0][sel]
+        if n_frames == 0:
+            return np.empty(0, dtype=dtype)
+        ctx = N.context(dev)
+        r = N.Reference.from_numpy(ctx, ref)
+        try:
+            out = np.empty(n_frames, np.float64)
+            dense = _dense_prefix(sel)
+            sel_arr = None if dense else np.ascontiguousarray(sel, dtype=np.uint32)
+            ctx.check(ctx.lib.wmd_rmsd_frames(ctx.handle, coords.ctypes.data, n_frames, coords.shape[1], 3,
+                                              N.ptr(sel_arr), int(sel.size), r.handle, int(self.align),
+                                              out.ctypes.data, None))
+        finally:
+            r.close()
+        return out.astype(dtype, copy=False)
+
+
+class PairwiseRmsdPlan:
+    """All-pairs frame x frame RMSD matrix (warp_md.PairwiseRmsdPlan).
+
+    ``mode`` picks the covariance arithmetic: "i8x3" (tensor cores on
+    24-bit fixed-point coordinates split into three int8 limbs, exact integer
+    accumulation), "i8x2" (16-bit fixed point), "fp32" (plain FP32 CUDA-core
+    tiles) or "fp64" (default; FP64 CUDA-core tiles).  All use an FP64 QCP epilogue."""
+
+    def __init__(self, selection: Selection, metric: str = "rms", pbc: str = "none", mode: str = "fp64"):
+        self.selection = selection
+        self.metric = parse_pairwise_metric(metric)
+        self.pbc = parse_pbc(pbc)
+        if mode not in _PAIR_MODES:
+            raise RuntimeError(f"mode must be one of {sorted(_PAIR_MODES)}")
+        self.mode = mode
+
+    def run(self, traj: Trajectory, system: System, chunk_frames: Optional[int] = None, device: str = "auto",
+            frame_indices: Optional[Sequence[int]] = None) -> np.ndarray:
+        dev = parse_device(device)
+        if self.metric == "dme":
+            raise N.WarpMdError(N.WMD_ERR_UNSUPPORTED, "unsupported: pairwise metric 'dme' is not provided by this build")
+        sel = _check_inputs(traj, system, self.selection)
+        coords = traj.coords
+        sub = frame_subset(coords.shape[0], frame_indices)
+        if sub is not None:
+            coords = np.ascontiguousarray(coords[sub])
+        n = coords.shape[0]
+        out = np.zeros((n, n), np.float32)
+        if n == 0:
+            return np.zeros((0, 0), np.float32)
+        ctx = N.context(dev)
+        dense = _dense_prefix(sel)
+        sel_arr = None if dense else np.ascontiguousarray(sel, dtype=np.uint32)
+        metric = N.PAIR_RMS if self.metric == "rms" else N.PAIR_NOFIT
+        ctx.check(ctx.lib.wmd_pairwise_rmsd(ctx.handle, coords.ctypes.data, n, coords.shape[1], 3, N.ptr(sel_arr),
+                                            int(sel.size), metric, _PAIR_MODES[self.mode], out.ctypes.data, None))
+        return out

@@ -1,0 +1,101 @@
+"""Differentiable RMSD for PyTorch (CUDA tensors only).
+
+``rmsd(coords, reference)`` returns per-frame RMSD (float64) of
+``coords[F, N, 3]`` against ``reference[N_sel, 3]`` after optimal
+superposition, through a ``torch.autograd.Function`` whose backward is the
+library's hand-written kernel: dRMSD/dx_k = (x_k - x_bar - R^T (y_k - y_bar)) /
+(n RMSD), with R re-derived from the QCP eigenvector of the covariance saved by
+the forward (16 doubles per frame) rather than stored.  The reference plan has
+no gradient; this is an addition.  Calls are issued on torch's current stream.
+"""
+from __future__ import annotations
+
+from typing import Optional
+
+import torch
+
+from . import _native as N
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+class _RefCache:
+    """Keeps uploaded references alive per (device, data_ptr, version)."""
+
+    def __init__(self):
+        self._key = None
+        self._ref = None
+
+    def get(self, ctx: N.Context, ref: torch.Tensor) -> N.Reference:
+        key = (ctx.device, ref.data_ptr(), ref._version, tuple(ref.shape))
+        if key != self._key:
+            r = ref.detach().to(torch.float32).contiguous()
+            self._ref = N.Reference(ctx, r.data_ptr(), r.shape[0], r.shape[1], keepalive=r)
+            self._key = key
+        return self._ref
+
+
+_cache = _RefCache()
+
+
+class RmsdFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx_, coords: torch.Tensor, reference: torch.Tensor, selection: Optional[torch.Tensor]):
+        if not coords.is_cuda:
+            raise N.WarpMdError(N.WMD_ERR_INVALID_ARG, "coords must be a CUDA tensor")
+        if coords.dtype != torch.float32 or coords.dim() != 3 or coords.shape[2] != 3:
+            raise N.WarpMdError(N.WMD_ERR_INVALID_ARG, "coords must be float32 with shape (frames, atoms, 3)")
+        x = coords.contiguous()
+        dev = x.device.index or 0
+        ctx = N.context(dev)
+        ref = _cache.get(ctx, reference.to(x.device))
+        F, n_atoms = x.shape[0], x.shape[1]
+        sel = None
+        n_sel = ref.n_sel
+        if selection is not None:
+            sel = selection.to(device=x.device, dtype=torch.int32).contiguous()
+            if sel.numel() != n_sel:
+                raise N.WarpMdError(N.WMD_ERR_MISMATCH, "selection and reference lengths differ")
+        out = torch.empty(F, dtype=torch.float64, device=x.device)
+        stats = torch.empty(F, N.FRAME_STATS, dtype=torch.float64, device=x.device)
+        ctx.check(ctx.lib.wmd_rmsd_forward(ctx.handle, x.data_ptr(), F, n_atoms, 3,
+                                           None if sel is None else sel.data_ptr(), n_sel, ref.handle,
+                                           out.data_ptr(), stats.data_ptr(), _stream()))
+        ctx_.save_for_backward(x, stats, sel if sel is not None else torch.empty(0, device=x.device))
+        ctx_.ref = ref
+        ctx_.has_sel = sel is not None
+        return out
+
+    @staticmethod
+    def backward(ctx_, grad_out: torch.Tensor):
+        x, stats, sel = ctx_.saved_tensors
+        ref = ctx_.ref
+        ctx = N.context(x.device.index or 0)
+        F, n_atoms = x.shape[0], x.shape[1]
+        g = grad_out.to(torch.float32).contiguous()
+        grad = torch.zeros_like(x)
+        ctx.check(ctx.lib.wmd_rmsd_backward(ctx.handle, x.data_ptr(), F, n_atoms, 3,
+                                            sel.data_ptr() if ctx_.has_sel else None, ref.n_sel, ref.handle,
+                                            stats.data_ptr(), g.data_ptr(), grad.data_ptr(), _stream()))
+        return grad, None, None
+
+
+def rmsd(coords: torch.Tensor, reference: torch.Tensor, selection: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """Per-frame aligned RMSD (float64), differentiable w.r.t. ``coords``."""
+    return RmsdFunction.apply(coords, reference, selection)
+
+
+def pairwise(coords: torch.Tensor, metric: str = "rms", mode: str = "i8x3") -> torch.Tensor:
+    """All-pairs RMSD matrix of CUDA float32 frames (F, N, 3) -> (F, F) float32."""
+    from .plans import _PAIR_MODES
+
+    x = coords.contiguous()
+    ctx = N.context(x.device.index or 0)
+    F = x.shape[0]
+    out = torch.empty(F, F, dtype=torch.float32, device=x.device)
+    m = N.PAIR_RMS if metric == "rms" else N.PAIR_NOFIT
+    ctx.check(ctx.lib.wmd_pairwise_rmsd(ctx.handle, x.data_ptr(), F, x.shape[1], 3, None, x.shape[1], m,
+                                        _PAIR_MODES[mode], out.data_ptr(), _stream()))
+    return out
