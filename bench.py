@@ -119,21 +119,22 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(threads: int, n_frames: int, seed: int = 7):
-    """Times the oracle (C FP64 restatement of the reference CPU path) on a
-    bounded sample of the streaming workload."""
+def cpu_baseline(threads: int, n_frames: int, seed: int = 7, frames=None, ref=None):
+    """Times the oracle (C FP64 restatement of the reference CPU path,
+    rmsd_aligned_selected) on a bounded sample of the streaming workload:
+    the given host frames, or freshly generated ones."""
     sys.path.insert(0, os.path.join(HERE, "oracle"))
-    import numpy as np
-
     import oracle
     from warp_md import synth
 
-    fr, ref = synth.make_trajectory(N_ATOMS, n_frames, SIGMA, seed=seed)
+    if frames is None:
+        frames, ref = synth.make_trajectory(N_ATOMS, n_frames, SIGMA, seed=seed)
+    fr = frames[:n_frames]
     oracle.rmsd_frames(fr[:2], ref, threads=threads)  # warm
     t0 = time.perf_counter()
-    oracle.rmsd_frames(fr, ref, threads=threads)
+    _, vals = oracle.rmsd_frames(fr, ref, threads=threads)
     dt = time.perf_counter() - t0
-    return (N_ATOMS * n_frames) / dt, dt
+    return (N_ATOMS * fr.shape[0]) / dt, dt, vals
 
 
 def run_reference(args):
@@ -144,7 +145,7 @@ def run_reference(args):
     frames = args.ref_frames
     vals = []
     for i in range(args.warmup + args.steps):
-        v, _ = cpu_baseline(threads, frames, seed=100 + i)
+        v, _, _ = cpu_baseline(threads, frames, seed=100 + i)
         if i >= args.warmup:
             vals.append(v)
     value = statistics.median(vals)
@@ -180,12 +181,13 @@ def run_ours(args):
 
     ctx = N.context(local)
     stream = torch.cuda.current_stream()
-    coords, ref = synth.make_trajectory_torch(N_ATOMS, N_FRAMES, SIGMA, seed=1 + rank, device="cuda")
+    n_frames = args.n_frames
+    coords, ref = synth.make_trajectory_torch(N_ATOMS, n_frames, SIGMA, seed=1 + rank, device="cuda")
     r = N.Reference(ctx, ref.data_ptr(), N_ATOMS, 3, keepalive=ref)
-    out = torch.empty(N_FRAMES, dtype=torch.float64, device="cuda")
+    out = torch.empty(n_frames, dtype=torch.float64, device="cuda")
 
     def step():
-        ctx.check(ctx.lib.wmd_rmsd_frames(ctx.handle, coords.data_ptr(), N_FRAMES, N_ATOMS, 3, None, N_ATOMS,
+        ctx.check(ctx.lib.wmd_rmsd_frames(ctx.handle, coords.data_ptr(), n_frames, N_ATOMS, 3, None, N_ATOMS,
                                           r.handle, 1, out.data_ptr(), stream.cuda_stream))
 
     for _ in range(args.warmup):
@@ -210,10 +212,10 @@ def run_ours(args):
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         total_ms = float(t.item())
         pg.barrier()
-    units = float(N_ATOMS) * N_FRAMES * ws * args.steps
+    units = float(N_ATOMS) * n_frames * ws * args.steps
     value = units / (total_ms / 1e3)
     kern_ms = statistics.median(per_launch_ms)
-    alg_bytes = N_ATOMS * N_FRAMES * BYTES_PER_UNIT + N_FRAMES * BYTES_PER_FRAME_OUT
+    alg_bytes = N_ATOMS * n_frames * BYTES_PER_UNIT + n_frames * BYTES_PER_FRAME_OUT
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9
     peak, peak_kind = _measured_peaks()
     traffic = None
@@ -222,7 +224,7 @@ def run_ours(args):
         with open(tfile) as fh:
             tj = json.load(fh)
         if "rmsd_frames_bytes_per_atom_frame" in tj:
-            traffic = tj["rmsd_frames_bytes_per_atom_frame"] * N_ATOMS * N_FRAMES
+            traffic = tj["rmsd_frames_bytes_per_atom_frame"] * N_ATOMS * n_frames
 
     # sanity: results finite, a sample against nothing but physics (rmsd within noise range)
     vals = out.cpu().numpy()
@@ -230,8 +232,9 @@ def run_ours(args):
 
     # ---- end to end through the C ABI with pinned host buffers ----
     e2e = None
+    host = None
     if not args.skip_e2e:
-        e2e_frames = N_FRAMES
+        e2e_frames = n_frames
         try:
             host = torch.empty((e2e_frames, N_ATOMS, 3), dtype=torch.float32, pin_memory=True)
             host.copy_(coords[:e2e_frames])
@@ -261,25 +264,36 @@ def run_ours(args):
                    "h2d_bytes_per_step": int(e2e_frames * N_ATOMS * 12), "d2h_bytes_per_step": int(e2e_frames * 8),
                    "frames": e2e_frames, "host_buffer": "pinned"}
             np.testing.assert_allclose(hout, vals[:e2e_frames], rtol=0, atol=0)
-            del host
         except RuntimeError as exc:  # e.g. pinned allocation refused on the host
             e2e = {"value": None, "unit": UNIT, "error": str(exc)[:200]}
 
     cpu = None
     if rank == 0 and not args.skip_cpu:
         threads = os.cpu_count() or 1
-        v_all, dt_all = cpu_baseline(threads, args.cpu_frames)
-        v_one, dt_one = cpu_baseline(1, max(2, args.cpu_frames // 8))
+        if host is not None:
+            hframes, href = host.numpy(), ref.cpu().numpy()
+        else:
+            hframes, href = None, None
+        all_frames = min(args.cpu_frames, n_frames) if hframes is not None else args.cpu_frames
+        v_all, dt_all, cvals = cpu_baseline(threads, all_frames, frames=hframes, ref=href)
+        one_frames = max(2, min(args.cpu_frames_single, all_frames))
+        v_one, dt_one, _ = cpu_baseline(1, one_frames, frames=hframes, ref=href)
+        err = None
+        if hframes is not None:
+            err = float(np.abs(cvals - vals[:all_frames]).max())
         cpu = {"value": v_all, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"{args.cpu_frames} frames x {N_ATOMS} atoms ({dt_all:.1f} s) with {threads} threads",
-               "single_thread": {"value": v_one, "frames": max(2, args.cpu_frames // 8), "seconds": dt_one}}
+               "sample": (f"first {all_frames} frames x {N_ATOMS} atoms of the workload "
+                          f"({dt_all:.1f} s with {threads} threads)"),
+               "single_thread": {"value": v_one, "frames": one_frames, "seconds": dt_one},
+               "max_abs_err_gpu_vs_cpu_A": err}
+    del host
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_atoms": N_ATOMS, "n_frames_per_gpu": N_FRAMES,
+            "config": {"workload": WORKLOAD, "n_atoms": N_ATOMS, "n_frames_per_gpu": n_frames,
                        "input_layout": "float32 xyz, frame-major", "l2": "inputs larger than L2 (12 GB per GPU)",
                        "parallelism": f"frames sharded, {ws} independent ranks"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -306,7 +320,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--cpu-frames", type=int, default=96)
+    ap.add_argument("--cpu-frames", type=int, default=10_000)
+    ap.add_argument("--cpu-frames-single", type=int, default=1_000)
+    ap.add_argument("--n-frames", type=int, default=N_FRAMES, help="frames per GPU (profiling runs only)")
     ap.add_argument("--ref-frames", type=int, default=48)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--skip-e2e", action="store_true")

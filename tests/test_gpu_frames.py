@@ -127,7 +127,13 @@ def test_bitwise_deterministic(gpu_ctx):
 def test_identical_and_empty(gpu_ctx):
     fr, ref = synth.make_trajectory(100, 3, 0.0, seed=1)
     same = np.stack([ref, ref, ref])
-    assert np.all(gpu_rmsd(gpu_ctx, same, ref) < TOL)
+    assert np.all(gpu_rmsd(gpu_ctx, same, ref) < 1e-9)  # explicit residual pass near zero
+    big, bref = synth.make_trajectory(20000, 4, 0.5, seed=2)
+    big[2] = bref  # one frame equal to the reference, among ordinary frames
+    got = gpu_rmsd(gpu_ctx, big, bref)
+    _, exp = oracle.rmsd_frames(big, bref)
+    np.testing.assert_allclose(got, exp, rtol=0, atol=TOL)
+    assert got[2] < 1e-9
     out = gpu_rmsd(gpu_ctx, fr, np.zeros((0, 3), np.float32), sel=np.zeros(0, np.uint32))
     assert np.all(out == 0)
 

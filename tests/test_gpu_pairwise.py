@@ -1,7 +1,9 @@
 """All-pairs RMSD matrix on the GPU against the oracle's restatement of
 PairwiseRmsdPlan::finalize (plan.rs:593-674).
 
-Tolerances (max abs error vs the FP64 oracle, float32 outputs):
+Tolerances (max abs error vs the FP64 oracle; outputs are float32 like the
+reference's, so a relative 1e-7 for the float32 rounding of large values is
+added to each):
   fp64 : 1e-5 A   (FP64 covariance tiles, exact up to the float32 output)
   i8x3 : 1e-4 A   (24-bit fixed point, exact int32 accumulation)
   i8x2 : 5e-4 A   (16-bit fixed point)
@@ -64,9 +66,9 @@ def test_golden_pairwise(gpu_ctx, golden, mode):
             continue
         fr = golden["frames_" + name]
         got = gpu_pairwise(gpu_ctx, fr, "rms", mode)
-        np.testing.assert_allclose(got, golden["expect_pair_aligned_" + name], rtol=0, atol=TOL[mode], err_msg=name)
+        np.testing.assert_allclose(got, golden["expect_pair_aligned_" + name], rtol=1e-7, atol=TOL[mode], err_msg=name)
         got = gpu_pairwise(gpu_ctx, fr, "nofit", mode)
-        np.testing.assert_allclose(got, golden["expect_pair_raw_" + name], rtol=0, atol=TOL[mode], err_msg=name)
+        np.testing.assert_allclose(got, golden["expect_pair_raw_" + name], rtol=1e-7, atol=TOL[mode], err_msg=name)
 
 
 @pytest.mark.parametrize("mode", MODES)
@@ -79,7 +81,7 @@ def test_drift_shapes(gpu_ctx, mode, F, n):
     _, exp = oracle.pairwise(fr, "rms")
     assert np.all(np.diag(got) == 0)
     np.testing.assert_array_equal(got, got.T)
-    np.testing.assert_allclose(got, exp, rtol=0, atol=TOL[mode])
+    np.testing.assert_allclose(got, exp, rtol=1e-7, atol=TOL[mode])
 
 
 @pytest.mark.parametrize("mode", MODES)
@@ -100,7 +102,7 @@ def test_selection_and_small_selections(gpu_ctx):
     sel = np.arange(1, 300, 2)
     got = gpu_pairwise(gpu_ctx, fr, "rms", "fp64", sel=sel)
     _, exp = oracle.pairwise(fr[:, sel], "rms")
-    np.testing.assert_allclose(got, exp, rtol=0, atol=1e-5)
+    np.testing.assert_allclose(got, exp, rtol=1e-7, atol=1e-5)
     one = gpu_pairwise(gpu_ctx, fr, "rms", "fp64", sel=[7])
     assert np.all(one == 0)  # n_sel < 2 -> zeros (plan.rs:604-610)
 

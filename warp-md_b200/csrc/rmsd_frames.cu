@@ -19,10 +19,10 @@
 //     P = sum x y_c^T (9) -- all statistics the QCP needs in one pass.  Frames
 //     are not pre-centred: with y_c centred, H = P - x_bar (sum y_c)^T exactly.
 //   * The 15 sums are reduced across the CTA with a butterfly reduce-scatter
-//     (16 shuffles) and a 2 KB shared buffer.  Frames spanning several tiles
-//     leave a 16-double partial in scratch; the CTA that completes a frame
-//     (atomic counter) adds the partials in tile order -- so results are
-//     bitwise reproducible -- runs QCP in FP64 and resets the counter.
+//     (16 shuffles) and a 2 KB shared buffer, and stored as a 16-double
+//     partial per (frame, tile).  A finalize kernel adds each frame's partials
+//     in tile order -- so results are bitwise reproducible -- and runs QCP in
+//     FP64; the streaming loop itself never fences or waits on other CTAs.
 //   * Bounded waits everywhere: a wait that exceeds kWaitLimitNs records a
 //     status bit in the context's status word and the CTA exits after letting
 //     its copies in flight land.
@@ -47,11 +47,11 @@ template <int STRIDE, int APT>
 struct Geo {
   static constexpr int kTile = kConsumerThreads * APT;
   static constexpr int kStageBytes = ((kTile * STRIDE * 4 + 32) + 127) / 128 * 128;
-  static constexpr int kStagesRaw = 98304 / kStageBytes;
-  static constexpr int kStages = kStagesRaw < 2 ? 2 : (kStagesRaw > 8 ? 8 : kStagesRaw);
+  static constexpr int kStagesRaw = 51200 / kStageBytes;
+  static constexpr int kStages = kStagesRaw < 3 ? 3 : (kStagesRaw > 8 ? 8 : kStagesRaw);
   static constexpr int kRedBytes = 2 * kConsumerWarps * 16 * 8;
   static constexpr int kBarOffset = kStages * kStageBytes;
-  static constexpr int kRedOffset = kBarOffset + 2 * kStages * 8;
+  static constexpr int kRedOffset = kBarOffset + kStages * 8;
   static constexpr int kAbortOffset = kRedOffset + kRedBytes;
   static constexpr int kSmemBytes = kAbortOffset + 16;
 };
@@ -82,6 +82,16 @@ __device__ __noinline__ void finish_frame(const FrameLaunch& L, int64_t f, doubl
   const QcpOut q = qcp_lambda(h, 0.5 * (gx + gy));
   const double rmsd = sqrt(msd_from(gx, gy, q.lambda, n));
   if (L.out.rmsd) L.out.rmsd[f] = rmsd;
+  if (L.refine && (L.out.rmsd || L.out.stats) && rmsd < kRefineScale * (gx + gy) * inv_n) {
+    // near-zero RMSD: queue the frame for the explicit residual pass
+    const unsigned slot = atomicAdd(L.refine_count, 1u);
+    double* rec = L.refine + (size_t)slot * kStatDoubles;
+    rec[0] = (double)f;
+    rec[1] = sx[0] * inv_n; rec[2] = sx[1] * inv_n; rec[3] = sx[2] * inv_n;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) rec[4 + e] = h[e];
+    rec[13] = q.lambda;
+  }
   if (L.out.stats) {
     double* st = L.out.stats + f * kStatDoubles;
     st[0] = sx[0] * inv_n; st[1] = sx[1] * inv_n; st[2] = sx[2] * inv_n;
@@ -97,122 +107,119 @@ __device__ __noinline__ void finish_frame(const FrameLaunch& L, int64_t f, doubl
   if (L.out.sum_y2) L.out.sum_y2[f] = (float)gy;
 }
 
-// Leader warp of an item: total over the 8 consumer warps, then either finish
-// the frame or deposit a tile partial and let the last tile finish it.
+// Leader warp of an item: total over the 8 consumer warps, stored as the
+// item's 16-double partial.  No fence and no atomic here: frames are finished
+// by rmsd_finalize_kernel after the streaming kernel has ended.
 __device__ __forceinline__ void item_epilogue(const FrameLaunch& L, const double* red, int n_tiles, int t,
-                                              int64_t f, int mode) {
+                                              int64_t f) {
   const int lane = threadIdx.x & 31;
-  double v = 0.0;
   if (lane < 16) {
+    double v = 0.0;
 #pragma unroll
     for (int w = 0; w < kConsumerWarps; ++w) v += red[w * 16 + lane];
+    L.partial[((size_t)f * n_tiles + t) * kStatDoubles + lane] = v;
   }
-  if (n_tiles == 1) {
-    finish_frame(L, f, v, mode);
-    return;
-  }
-  double* part = L.partial + (size_t)f * n_tiles * kStatDoubles;
-  if (lane < 16) part[(size_t)t * kStatDoubles + lane] = v;
-  __threadfence();
-  __syncwarp();
-  unsigned prev = 0;
-  if (lane == 0) prev = atomicAdd(L.counter + f, 1u);
-  prev = __shfl_sync(0xffffffffu, prev, 0);
-  if (prev != (unsigned)(n_tiles - 1)) return;
-  __threadfence();
-  double s = 0.0;
-  if (lane < 16)
-    for (int tt = 0; tt < n_tiles; ++tt) s += __ldcg(part + (size_t)tt * kStatDoubles + lane);
-  if (lane == 0) L.counter[f] = 0u;
-  finish_frame(L, f, s, mode);
 }
 
+// One warp per frame: adds the frame's tile partials in tile order (so results
+// are bitwise reproducible), then QCP / outputs in finish_frame.
+template <int MODE>
+__global__ void __launch_bounds__(256) rmsd_finalize_kernel(const FrameLaunch L, int n_tiles) {
+  const int64_t f = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (f >= L.n_frames) return;
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  if (lane < 16) {
+    const double* part = L.partial + (size_t)f * n_tiles * kStatDoubles + lane;
+    for (int tt = 0; tt < n_tiles; ++tt) s += part[(size_t)tt * kStatDoubles];
+  }
+  finish_frame(L, f, s, MODE);
+}
+
+// Byte range of item (t, f) and its bulk copy into a stage.  The 16-byte
+// aligned hull [c0, c1) is copied; a range that runs into the unaligned tail
+// of the array gets its last floats by plain loads.  Called by one thread.
+template <int STRIDE, int T>
+__device__ __forceinline__ void issue_item(const FrameLaunch& L, int t, int64_t f, unsigned char* dst, uint64_t* bar,
+                                           uint64_t total_al) {
+  const int64_t a0 = (int64_t)t * T;
+  const int64_t a1 = min(L.ref.n_sel, a0 + T);
+  const unsigned char* base = reinterpret_cast<const unsigned char*>(L.coords);
+  const uint64_t b0 = (uint64_t)(f * L.n_atoms + a0) * STRIDE * 4ull;
+  const uint64_t b1 = (uint64_t)(f * L.n_atoms + a1) * STRIDE * 4ull;
+  const uint64_t c0 = b0 & ~15ull;
+  uint64_t c1 = (b1 + 15ull) & ~15ull;
+  if (c1 > total_al) {
+    const uint64_t tail0 = total_al > c0 ? total_al : c0;
+    for (uint64_t bb = tail0; bb < b1; bb += 4)
+      *reinterpret_cast<float*>(dst + (bb - c0)) = __ldg(reinterpret_cast<const float*>(base + bb));
+    c1 = tail0;
+  }
+  const uint32_t core = (uint32_t)(c1 - c0);
+  // order this CTA's earlier generic-proxy reads of the stage before the
+  // async-proxy write into it
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  mbar_arrive_expect_tx(bar, core);
+  if (core) bulk_copy_g2s(dst, base + c0, core, bar);
+}
+
+// Streaming kernel.  Items (tile t, frame f) are enumerated tile-major; each
+// CTA owns the contiguous run [w0, w1) and walks it with incremental (t, f).
+// Thread 0 doubles as the producer: at the top of item i it refills the stage
+// that item i-1 used (all consumers passed item i-1's named barrier, so its
+// reads are done) with item i + kStages - 1.
 template <int STRIDE, int APT, int MODE, bool GATHER>
-__global__ void __maxnreg__(112) rmsd_frames_kernel(const FrameLaunch L) {
+__global__ void __launch_bounds__(kThreads, 3) rmsd_frames_kernel(const FrameLaunch L) {
   using G = Geo<STRIDE, APT>;
   constexpr int T = G::kTile;
+  constexpr int S = G::kStages;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + G::kBarOffset);
-  uint64_t* empty = full + G::kStages;
   double* red = reinterpret_cast<double*>(smem + G::kRedOffset);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + G::kAbortOffset);
 
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t n_sel = L.ref.n_sel;
+  const int64_t F = L.n_frames;
   const int n_tiles = (int)((n_sel + T - 1) / T);
-  const int64_t W = (int64_t)n_tiles * L.n_frames;
+  const int64_t W = (int64_t)n_tiles * F;
   const int64_t w0 = W * blockIdx.x / gridDim.x, w1 = W * (blockIdx.x + 1) / gridDim.x;
+  const int64_t n_items = w1 - w0;
+  const uint64_t total_al = ((uint64_t)F * (uint64_t)L.n_atoms * STRIDE * 4ull) & ~15ull;
 
-  if (!GATHER) {
-    if (threadIdx.x == 0) {
-      for (int s = 0; s < G::kStages; ++s) {
-        mbar_init(&full[s], 1);
-        mbar_init(&empty[s], kConsumerWarps);
-      }
-      *abort_flag = 0;
-      fence_barrier_init();
-    }
-  } else if (threadIdx.x == 0) {
+  if (tid == 0) {
+    if (!GATHER)
+      for (int st = 0; st < S; ++st) mbar_init(&full[st], 1);
     *abort_flag = 0;
+    fence_barrier_init();
   }
   __syncthreads();
 
-  if (warp == kConsumerWarps) {
-    // ---------------- producer warp ----------------
-    if (GATHER || lane != 0) return;
-    const uint64_t total = (uint64_t)L.n_frames * (uint64_t)L.n_atoms * STRIDE * 4ull;
-    const uint64_t total_al = total & ~15ull;
-    const unsigned char* base = reinterpret_cast<const unsigned char*>(L.coords);
-    int64_t i = 0;
-    for (int64_t w = w0; w < w1; ++w, ++i) {
-      const int s = (int)(i % G::kStages);
-      const uint32_t ph = (uint32_t)((i / G::kStages) & 1);
-      if (!mbar_wait(&empty[s], ph ^ 1u, L.status, kStatusTimeoutEmpty, abort_flag)) break;
-      const int t = (int)(w / L.n_frames);
-      const int64_t f = w - (int64_t)t * L.n_frames;
-      const int64_t a0 = (int64_t)t * T;
-      const int64_t a1 = min(n_sel, a0 + T);
-      const uint64_t b0 = (uint64_t)(f * L.n_atoms + a0) * STRIDE * 4ull;
-      const uint64_t b1 = (uint64_t)(f * L.n_atoms + a1) * STRIDE * 4ull;
-      const uint64_t c0 = b0 & ~15ull;
-      uint64_t c1 = (b1 + 15ull) & ~15ull;
-      unsigned char* dst = smem + s * G::kStageBytes;
-      if (c1 > total_al) {
-        const uint64_t tail0 = total_al > c0 ? total_al : c0;
-        for (uint64_t bb = tail0; bb < b1; bb += 4)
-          *reinterpret_cast<float*>(dst + (bb - c0)) = __ldg(reinterpret_cast<const float*>(base + bb));
-        c1 = tail0;
-      }
-      const uint32_t core = (uint32_t)(c1 - c0);
-      mbar_arrive_expect_tx(&full[s], core);
-      if (core) bulk_copy_g2s(dst, base + c0, core, &full[s]);
+  // producer cursor (thread 0 only)
+  int tp = (int)(w0 / F);
+  int64_t fp = w0 - (int64_t)tp * F;
+  int64_t issued = 0;
+  if (!GATHER && tid == 0) {
+    for (; issued < S - 1 && issued < n_items; ++issued) {
+      issue_item<STRIDE, T>(L, tp, fp, smem + (issued % S) * G::kStageBytes, &full[issued % S], total_al);
+      if (++fp == F) { fp = 0; ++tp; }
     }
-    // let every copy this CTA issued land before the CTA may exit
-    const int64_t n_issued = i;
-    const int64_t first = n_issued > G::kStages ? n_issued - G::kStages : 0;
-    for (int64_t j = first; j < n_issued; ++j) {
-      const int s = (int)(j % G::kStages);
-      const uint32_t ph = (uint32_t)((j / G::kStages) & 1);
-      const uint64_t t0 = global_timer_ns();
-      while (!mbar_try_wait(&full[s], ph)) {
-        if (global_timer_ns() - t0 > kWaitLimitNs) {
-          atomicOr(L.status, kStatusTimeoutDrain);
-          break;
-        }
-      }
-    }
-    return;
   }
 
-  // ---------------- consumer warps ----------------
-  const int tid = threadIdx.x;  // 0 .. kConsumerThreads-1
   double yr[APT][3];
   uint32_t gidx[GATHER ? APT : 1];
+  int t = (int)(w0 / F);
+  int64_t f = w0 - (int64_t)t * F;
   int cur_tile = -1;
-  int64_t i = 0;
-  for (int64_t w = w0; w < w1; ++w, ++i) {
-    const int t = (int)(w / L.n_frames);
-    const int64_t f = w - (int64_t)t * L.n_frames;
+  int s = 0;
+  uint32_t phase = 0;
+  for (int64_t i = 0; i < n_items; ++i) {
+    if (!GATHER && tid == 0 && issued < n_items) {
+      const int sp = (int)(issued % S);
+      issue_item<STRIDE, T>(L, tp, fp, smem + sp * G::kStageBytes, &full[sp], total_al);
+      ++issued;
+      if (++fp == F) { fp = 0; ++tp; }
+    }
     const int64_t a0 = (int64_t)t * T;
     const int len = (int)(min(n_sel, a0 + T) - a0);
     if (t != cur_tile) {
@@ -238,16 +245,9 @@ __global__ void __maxnreg__(112) rmsd_frames_kernel(const FrameLaunch L) {
       }
     }
     const float* xs = nullptr;
-    int s = 0;
     bool ok = true;
     if (!GATHER) {
-      s = (int)(i % G::kStages);
-      const uint32_t ph = (uint32_t)((i / G::kStages) & 1);
-      ok = mbar_wait(&full[s], ph, L.status, kStatusTimeoutFull, abort_flag);
-      // The backward has no CTA barrier, so a failed wait can leave at once.  The
-      // forward still joins this item's named barrier (with zero sums) and all
-      // consumer warps then leave together on the shared abort flag.
-      if (MODE == kBwd && !ok) break;
+      ok = mbar_wait(&full[s], phase, L.status, kStatusTimeoutFull, abort_flag);
       xs = reinterpret_cast<const float*>(smem + s * G::kStageBytes) +
            (int)(((uint64_t)(f * L.n_atoms + a0) * STRIDE) & 3ull);
     }
@@ -287,78 +287,90 @@ __global__ void __maxnreg__(112) rmsd_frames_kernel(const FrameLaunch L) {
     };
 
     if (MODE == kBwd) {
-      const double* rt = L.rot + f * kStatDoubles;
-      double R[9], c[3];
+      if (ok) {
+        const double* rt = L.rot + f * kStatDoubles;
+        double R[9], c[3];
 #pragma unroll
-      for (int e = 0; e < 9; ++e) R[e] = __ldg(rt + e);
-      c[0] = __ldg(rt + 9); c[1] = __ldg(rt + 10); c[2] = __ldg(rt + 11);
-      const double scale = __ldg(rt + 12);
-      float* gframe = L.grad + (size_t)f * L.n_atoms * 3;
+        for (int e = 0; e < 9; ++e) R[e] = __ldg(rt + e);
+        c[0] = __ldg(rt + 9); c[1] = __ldg(rt + 10); c[2] = __ldg(rt + 11);
+        const double scale = __ldg(rt + 12);
+        float* gframe = L.grad + (size_t)f * L.n_atoms * 3;
 #pragma unroll
-      for (int j = 0; j < APT; ++j) {
-        const int k = tid + j * kConsumerThreads;
-        float x0, x1, x2;
-        load_x(j, x0, x1, x2);
-        if (k < len) {
-          const double ty0 = R[0] * yr[j][0] + R[3] * yr[j][1] + R[6] * yr[j][2];
-          const double ty1 = R[1] * yr[j][0] + R[4] * yr[j][1] + R[7] * yr[j][2];
-          const double ty2 = R[2] * yr[j][0] + R[5] * yr[j][1] + R[8] * yr[j][2];
-          const size_t atom = GATHER ? (size_t)gidx[GATHER ? j : 0] : (size_t)(a0 + k);
-          float* g = gframe + atom * 3;
-          g[0] = (float)(scale * (((double)x0 - c[0]) - ty0));
-          g[1] = (float)(scale * (((double)x1 - c[1]) - ty1));
-          g[2] = (float)(scale * (((double)x2 - c[2]) - ty2));
+        for (int j = 0; j < APT; ++j) {
+          const int k = tid + j * kConsumerThreads;
+          float x0, x1, x2;
+          load_x(j, x0, x1, x2);
+          if (k < len) {
+            const double ty0 = R[0] * yr[j][0] + R[3] * yr[j][1] + R[6] * yr[j][2];
+            const double ty1 = R[1] * yr[j][0] + R[4] * yr[j][1] + R[7] * yr[j][2];
+            const double ty2 = R[2] * yr[j][0] + R[5] * yr[j][1] + R[8] * yr[j][2];
+            const size_t atom = GATHER ? (size_t)gidx[GATHER ? j : 0] : (size_t)(a0 + k);
+            float* g = gframe + atom * 3;
+            g[0] = (float)(scale * (((double)x0 - c[0]) - ty0));
+            g[1] = (float)(scale * (((double)x1 - c[1]) - ty1));
+            g[2] = (float)(scale * (((double)x2 - c[2]) - ty2));
+          }
         }
       }
-      if (!GATHER) {
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[s]);
-      }
-      continue;
-    }
-
-    double acc[16];
-#pragma unroll
-    for (int e = 0; e < 16; ++e) acc[e] = 0.0;
-    if (MODE == kFwdRaw) {
-#pragma unroll
-      for (int j = 0; j < APT; ++j) {
-        float x0, x1, x2;
-        load_x(j, x0, x1, x2);
-        // y = y_c + mean, rebuilt in FP64; x - y in FP64
-        const double d0 = (double)x0 - (yr[j][0] + L.ref.mean[0]);
-        const double d1 = (double)x1 - (yr[j][1] + L.ref.mean[1]);
-        const double d2 = (double)x2 - (yr[j][2] + L.ref.mean[2]);
-        const bool in = tid + j * kConsumerThreads < len;
-        acc[0] = fma(d0, in ? d0 : 0.0, acc[0]);
-        acc[1] = fma(d1, in ? d1 : 0.0, acc[1]);
-        acc[2] = fma(d2, in ? d2 : 0.0, acc[2]);
-      }
-      acc[0] += acc[1] + acc[2];
-      acc[1] = acc[2] = 0.0;
+      named_barrier_sync(1, kConsumerThreads);  // stage s free for the producer
     } else {
+      double acc[16];
 #pragma unroll
-      for (int j = 0; j < APT; ++j) {
-        float f0, f1, f2;
-        load_x(j, f0, f1, f2);
-        const double x0 = f0, x1 = f1, x2 = f2;
-        acc[0] += x0; acc[1] += x1; acc[2] += x2;
-        acc[3] = fma(x0, x0, acc[3]); acc[4] = fma(x1, x1, acc[4]); acc[5] = fma(x2, x2, acc[5]);
-        acc[6] = fma(x0, yr[j][0], acc[6]);  acc[7] = fma(x0, yr[j][1], acc[7]);  acc[8] = fma(x0, yr[j][2], acc[8]);
-        acc[9] = fma(x1, yr[j][0], acc[9]);  acc[10] = fma(x1, yr[j][1], acc[10]); acc[11] = fma(x1, yr[j][2], acc[11]);
-        acc[12] = fma(x2, yr[j][0], acc[12]); acc[13] = fma(x2, yr[j][1], acc[13]); acc[14] = fma(x2, yr[j][2], acc[14]);
+      for (int e = 0; e < 16; ++e) acc[e] = 0.0;
+      if (MODE == kFwdRaw) {
+#pragma unroll
+        for (int j = 0; j < APT; ++j) {
+          float x0, x1, x2;
+          load_x(j, x0, x1, x2);
+          // y = y_c + mean, rebuilt in FP64; x - y in FP64
+          const double d0 = (double)x0 - (yr[j][0] + L.ref.mean[0]);
+          const double d1 = (double)x1 - (yr[j][1] + L.ref.mean[1]);
+          const double d2 = (double)x2 - (yr[j][2] + L.ref.mean[2]);
+          const bool in = ok && tid + j * kConsumerThreads < len;
+          acc[0] = fma(d0, in ? d0 : 0.0, acc[0]);
+          acc[1] = fma(d1, in ? d1 : 0.0, acc[1]);
+          acc[2] = fma(d2, in ? d2 : 0.0, acc[2]);
+        }
+        acc[0] += acc[1] + acc[2];
+        acc[1] = acc[2] = 0.0;
+      } else {
+#pragma unroll
+        for (int j = 0; j < APT; ++j) {
+          float f0, f1, f2;
+          load_x(j, f0, f1, f2);
+          const double x0 = f0, x1 = f1, x2 = f2;
+          acc[0] += x0; acc[1] += x1; acc[2] += x2;
+          acc[3] = fma(x0, x0, acc[3]); acc[4] = fma(x1, x1, acc[4]); acc[5] = fma(x2, x2, acc[5]);
+          acc[6] = fma(x0, yr[j][0], acc[6]);  acc[7] = fma(x0, yr[j][1], acc[7]);  acc[8] = fma(x0, yr[j][2], acc[8]);
+          acc[9] = fma(x1, yr[j][0], acc[9]);  acc[10] = fma(x1, yr[j][1], acc[10]); acc[11] = fma(x1, yr[j][2], acc[11]);
+          acc[12] = fma(x2, yr[j][0], acc[12]); acc[13] = fma(x2, yr[j][1], acc[13]); acc[14] = fma(x2, yr[j][2], acc[14]);
+        }
+      }
+      const double v = warp_reduce_scatter16(acc);
+      double* rb = red + (i & 1) * (kConsumerWarps * 16);
+      if ((lane & 1) == 0) rb[warp * 16 + (lane >> 1)] = v;
+      named_barrier_sync(1, kConsumerThreads);  // also frees stage s for the producer
+      if (warp == (int)(i & (kConsumerWarps - 1))) item_epilogue(L, rb, n_tiles, t, f);
+    }
+    if (*abort_flag) break;
+    if (++s == S) { s = 0; phase ^= 1u; }
+    if (++f == F) { f = 0; ++t; }
+  }
+
+  // every copy this CTA issued must land before the CTA may exit
+  if (!GATHER && tid == 0) {
+    const int64_t first = issued > S ? issued - S : 0;
+    for (int64_t j = first; j < issued; ++j) {
+      const int st = (int)(j % S);
+      const uint32_t ph = (uint32_t)((j / S) & 1);
+      const uint64_t t0 = global_timer_ns();
+      while (!mbar_try_wait(&full[st], ph)) {
+        if (global_timer_ns() - t0 > kWaitLimitNs) {
+          atomicOr(L.status, kStatusTimeoutDrain);
+          break;
+        }
       }
     }
-    if (!GATHER && ok) {
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[s]);
-    }
-    const double v = warp_reduce_scatter16(acc);
-    double* rb = red + (i & 1) * (kConsumerWarps * 16);
-    if ((lane & 1) == 0) rb[warp * 16 + (lane >> 1)] = v;
-    named_barrier_sync(1, kConsumerThreads);
-    if (*abort_flag) break;
-    if (warp == (int)(i % kConsumerWarps)) item_epilogue(L, rb, n_tiles, t, f, MODE);
   }
 }
 
@@ -379,6 +391,59 @@ __global__ void rmsd_bwd_prologue(const double* __restrict__ stats, const float*
   for (int e = 0; e < 9; ++e) o[e] = r[e];
   o[9] = st[0]; o[10] = st[1]; o[11] = st[2];
   o[12] = scale; o[13] = 0; o[14] = 0; o[15] = 0;
+}
+
+// Residual pass for flagged frames (near-zero RMSD): the RMSD from explicit
+// residuals sum |R (x_k - x_bar) - (y_k - y_bar)|^2 in FP64, as the reference's
+// rmsd_aligned_selected computes every frame (plan.rs:1223-1247), with R from
+// the QCP eigenvector.  One CTA per flagged frame (grid-stride).
+template <int STRIDE>
+__global__ void __launch_bounds__(256) rmsd_refine_kernel(const FrameLaunch L) {
+  __shared__ double sh_r[12];
+  __shared__ double red[8];
+  const unsigned count = *L.refine_count;
+  const int64_t n_sel = L.ref.n_sel;
+  const double inv_n = 1.0 / (double)n_sel;
+  for (unsigned rix = blockIdx.x; rix < count; rix += gridDim.x) {
+    const double* rec = L.refine + (size_t)rix * kStatDoubles;
+    if (threadIdx.x == 0) {
+      double h[9], r[9];
+      for (int e = 0; e < 9; ++e) h[e] = rec[4 + e];
+      rotation_from_qcp(h, rec[13], r);
+      for (int e = 0; e < 9; ++e) sh_r[e] = r[e];
+      sh_r[9] = rec[1]; sh_r[10] = rec[2]; sh_r[11] = rec[3];
+    }
+    __syncthreads();
+    const int64_t f = (int64_t)rec[0];
+    double R[9], c[3];
+    for (int e = 0; e < 9; ++e) R[e] = sh_r[e];
+    c[0] = sh_r[9]; c[1] = sh_r[10]; c[2] = sh_r[11];
+    const double my0 = L.ref.sum_c[0] * inv_n, my1 = L.ref.sum_c[1] * inv_n, my2 = L.ref.sum_c[2] * inv_n;
+    const float* frame = L.coords + (size_t)f * L.n_atoms * STRIDE;
+    double acc = 0.0;
+    for (int64_t k = threadIdx.x; k < n_sel; k += blockDim.x) {
+      int64_t atom = L.sel ? (int64_t)L.sel[k] : k;
+      if (atom >= L.n_atoms) atom = 0;  // reported by the forward kernel
+      const float* p = frame + atom * STRIDE;
+      const double d0 = (double)p[0] - c[0], d1 = (double)p[1] - c[1], d2 = (double)p[2] - c[2];
+      const double* y = L.ref.yc + k * 3;
+      const double r0 = R[0] * d0 + R[1] * d1 + R[2] * d2 - (y[0] - my0);
+      const double r1 = R[3] * d0 + R[4] * d1 + R[5] * d2 - (y[1] - my1);
+      const double r2 = R[6] * d0 + R[7] * d1 + R[8] * d2 - (y[2] - my2);
+      acc += r0 * r0 + r1 * r1 + r2 * r2;
+    }
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < 8; ++w) t += red[w];
+      const double rmsd = sqrt(t * inv_n);
+      if (L.out.rmsd) L.out.rmsd[f] = rmsd;
+      if (L.out.stats) L.out.stats[f * kStatDoubles + 13] = rmsd;
+    }
+    __syncthreads();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -414,9 +479,9 @@ static int occupancy_one() {
   return blocks < 1 ? 1 : blocks;
 }
 
-// Tile shape: 4 atoms per consumer thread (1024-atom tiles) keeps the kernel
-// within 112 registers, i.e. two CTAs (18 warps) per SM.
-constexpr int kApt = 4;
+// Tile shape: 8 atoms per thread x 128 threads = 1024-atom tiles; the
+// reference atoms of a tile live in registers (48 per thread).
+constexpr int kApt = 8;
 
 template <int MODE>
 static cudaError_t dispatch(const FrameLaunch& L, cudaStream_t s) {
@@ -450,7 +515,24 @@ int frame_grid(const FrameLaunch& L, int sm_count, bool backward) {
 
 cudaError_t launch_rmsd_forward(const FrameLaunch& L, cudaStream_t s) {
   if (L.n_frames == 0) return cudaSuccess;
-  return L.align ? dispatch<kFwdFit>(L, s) : dispatch<kFwdRaw>(L, s);
+  if (!L.align) {
+    cudaError_t e = dispatch<kFwdRaw>(L, s);
+    if (e != cudaSuccess) return e;
+    rmsd_finalize_kernel<kFwdRaw><<<(unsigned)((L.n_frames + 7) / 8), 256, 0, s>>>(L, frame_tiles(L));
+    return cudaGetLastError();
+  }
+  if (L.refine) {
+    cudaError_t e = cudaMemsetAsync(L.refine_count, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+  }
+  cudaError_t e = dispatch<kFwdFit>(L, s);
+  if (e != cudaSuccess) return e;
+  rmsd_finalize_kernel<kFwdFit><<<(unsigned)((L.n_frames + 7) / 8), 256, 0, s>>>(L, frame_tiles(L));
+  if ((e = cudaGetLastError()) != cudaSuccess || !L.refine) return e;
+  const int blocks = (int)std::min<int64_t>(L.n_frames, 148);
+  if (L.stride == 4) rmsd_refine_kernel<4><<<blocks, 256, 0, s>>>(L);
+  else rmsd_refine_kernel<3><<<blocks, 256, 0, s>>>(L);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_rmsd_backward(const FrameLaunch& L, const double* stats, const float* grad_rmsd,

@@ -37,6 +37,19 @@ constexpr size_t kPartialBytesMax = size_t(512) << 20;
 
 thread_local std::string g_create_error;
 
+// Compensated summation (Neumaier 1974): error bounded by ~2 eps |sum| plus
+// O(n eps^2) sum |x_i|, independent of the order of magnitudes.
+struct NeumaierSum {
+  double s = 0.0, c = 0.0;
+  void add(double x) {
+    const double t = s + x;
+    if (std::fabs(s) >= std::fabs(x)) c += (s - t) + x;
+    else c += (x - t) + s;
+    s = t;
+  }
+  double value() const { return s + c; }
+};
+
 struct DevBuf {
   void* ptr = nullptr;
   size_t bytes = 0;
@@ -62,7 +75,7 @@ struct wmd_ctx {
   cudaEvent_t kern_done[2] = {nullptr, nullptr};
   int* status_host = nullptr;  // mapped pinned word the kernels report into
   int* status_dev = nullptr;
-  DevBuf partial, counter, rot, chunk[2], out_tmp, sel_buf, aux;
+  DevBuf partial, refine, refine_count, rot, chunk[2], out_tmp, sel_buf, aux;
   HostBuf stage[2];
   std::string err;
   wmd::PairwiseWorkspace pw;
@@ -172,8 +185,6 @@ int ensure_host(wmd_ctx* ctx, HostBuf& b, size_t bytes) {
 int check_status(wmd_ctx* ctx) {
   const int st = __atomic_exchange_n(ctx->status_host, 0, __ATOMIC_ACQ_REL);
   if (st == 0) return WMD_OK;
-  // a kernel gave up mid-way: its frame counters may be dirty
-  if (ctx->counter.ptr) cudaMemset(ctx->counter.ptr, 0, ctx->counter.bytes);
   if (st & 16) return set_err(ctx, WMD_ERR_INVALID_ARG, "selection index out of range (status 0x%x)", st);
   return set_err(ctx, WMD_ERR_TIMEOUT, "a device-side wait exceeded its limit (status 0x%x)", st);
 }
@@ -223,7 +234,7 @@ wmd::FrameLaunch base_launch(wmd_ctx* ctx, const wmd_ref* ref, int64_t n_atoms, 
   L.ref = ref->info;
   L.ref.yc = ref->yc;
   L.status = ctx->status_dev;
-  L.tile_atoms = wmd::kConsumerThreads * 4;
+  L.tile_atoms = wmd::kConsumerThreads * 8;
   return L;
 }
 
@@ -237,18 +248,25 @@ int forward_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames, int64_t
   L.gather = dsel != nullptr || (reinterpret_cast<uintptr_t>(dcoords) & 15u) != 0;
   const int tiles = wmd::frame_tiles(L);
   const size_t per_frame = (size_t)tiles * wmd::kStatDoubles * sizeof(double);
-  int64_t batch = n_frames;
-  if (tiles > 1) {
-    batch = std::max<int64_t>(1, (int64_t)(kPartialBytesMax / per_frame));
-    batch = std::min(batch, n_frames);
+  int64_t batch = std::max<int64_t>(1, (int64_t)(kPartialBytesMax / per_frame));
+  batch = std::min(batch, n_frames);
+  {
     int rc = ensure(ctx, ctx->partial, per_frame * (size_t)batch);
     if (rc) return rc;
-    rc = ensure(ctx, ctx->counter, (size_t)batch * sizeof(unsigned), true);
+  }
+  if (align) {
+    int rc = ensure(ctx, ctx->refine, (size_t)batch * wmd::kStatDoubles * sizeof(double));
+    if (rc) return rc;
+    rc = ensure(ctx, ctx->refine_count, sizeof(unsigned), true);
     if (rc) return rc;
   }
   for (int64_t f0 = 0; f0 < n_frames; f0 += batch) {
     const int64_t nf = std::min(batch, n_frames - f0);
     wmd::FrameLaunch B = L;
+    if (align) {
+      B.refine = static_cast<double*>(ctx->refine.ptr);
+      B.refine_count = static_cast<unsigned*>(ctx->refine_count.ptr);
+    }
     B.coords = dcoords + (size_t)f0 * n_atoms * stride;
     B.n_frames = nf;
     B.out.rmsd = o.rmsd ? o.rmsd + f0 : nullptr;
@@ -257,7 +275,6 @@ int forward_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames, int64_t
     B.out.sum_x2 = o.sum_x2 ? o.sum_x2 + f0 : nullptr;
     B.out.sum_y2 = o.sum_y2 ? o.sum_y2 + f0 : nullptr;
     B.partial = static_cast<double*>(ctx->partial.ptr);
-    B.counter = static_cast<unsigned*>(ctx->counter.ptr);
     B.grid = wmd::frame_grid(B, ctx->sm_count, false);
     CU(wmd::launch_rmsd_forward(B, s), "rmsd forward launch");
   }
@@ -371,7 +388,7 @@ WMD_EXPORT int wmd_destroy(wmd_ctx* ctx) {
   if (!ctx) return WMD_OK;
   DeviceGuard g(ctx->device);
   cudaDeviceSynchronize();
-  for (DevBuf* b : {&ctx->partial, &ctx->counter, &ctx->rot, &ctx->chunk[0], &ctx->chunk[1], &ctx->out_tmp,
+  for (DevBuf* b : {&ctx->partial, &ctx->refine, &ctx->refine_count, &ctx->rot, &ctx->chunk[0], &ctx->chunk[1], &ctx->out_tmp,
                     &ctx->sel_buf, &ctx->aux})
     if (b->ptr) cudaFree(b->ptr);
   for (HostBuf* b : {&ctx->stage[0], &ctx->stage[1]})
@@ -407,27 +424,31 @@ WMD_EXPORT int wmd_reference_upload(wmd_ctx* ctx, const float* ref, int64_t n_se
   I.n_sel = n_sel;
   std::vector<double> yc((size_t)std::max<int64_t>(n_sel, 1) * 3, 0.0);
   if (n_sel > 0) {
-    // FP64 two-pass centring, as rmsd_aligned_selected does (plan.rs:1172-1190)
-    double m[3] = {0, 0, 0};
+    // FP64 two-pass centring, as rmsd_aligned_selected does (plan.rs:1172-1190).
+    // The sums run over up to ~1e5 atoms whose coordinates are far from the
+    // origin, so they are compensated (Neumaier): the kernels correct H with
+    // sum(y_c) and must see the exact sum of the stored centred values.
+    NeumaierSum m[3];
     for (int64_t i = 0; i < n_sel; ++i)
-      for (int c = 0; c < 3; ++c) m[c] += (double)h[i * stride + c];
-    for (int c = 0; c < 3; ++c) I.mean[c] = m[c] / (double)n_sel;
-    double sumsq = 0;
+      for (int c = 0; c < 3; ++c) m[c].add((double)h[i * stride + c]);
+    for (int c = 0; c < 3; ++c) I.mean[c] = m[c].value() / (double)n_sel;
+    NeumaierSum sc[3], sq;
     for (int64_t i = 0; i < n_sel; ++i)
       for (int c = 0; c < 3; ++c) {
         const double y = (double)h[i * stride + c];
         yc[i * 3 + c] = y - I.mean[c];
-        I.sum_c[c] += yc[i * 3 + c];
-        sumsq += y * y;
+        sc[c].add(yc[i * 3 + c]);
+        sq.add(y * y);
       }
-    I.sumsq = sumsq;
-    double gy = 0;
+    for (int c = 0; c < 3; ++c) I.sum_c[c] = sc[c].value();
+    I.sumsq = sq.value();
+    NeumaierSum gy;
     for (int64_t i = 0; i < n_sel; ++i)
       for (int c = 0; c < 3; ++c) {
         const double d = yc[i * 3 + c] - I.sum_c[c] / (double)n_sel;
-        gy += d * d;
+        gy.add(d * d);
       }
-    I.gy = gy;
+    I.gy = gy.value();
   }
   cudaError_t e = cudaMalloc(&r->yc, yc.size() * sizeof(double));
   if (e != cudaSuccess) {

@@ -7,12 +7,12 @@
 
 namespace wmd {
 
-// Per-frame kernel geometry: 8 consumer warps + 1 producer warp per CTA; each
-// consumer thread owns kAtomsPerThread atoms of an atom tile, whose reference
+// Per-frame kernel geometry: 4 warps per CTA (thread 0 also issues the bulk
+// copies); each thread owns 8 atoms of a 1024-atom tile, whose reference
 // coordinates it keeps in registers (FP64, centred) while frames stream past.
-constexpr int kConsumerWarps = 8;
+constexpr int kConsumerWarps = 4;
 constexpr int kConsumerThreads = kConsumerWarps * 32;
-constexpr int kThreads = kConsumerThreads + 32;
+constexpr int kThreads = kConsumerThreads;
 constexpr int kStatDoubles = 16;  // per-frame / per-tile partial record
 
 // Which outputs a per-frame forward launch writes.
@@ -48,14 +48,22 @@ struct FrameLaunch {
   const double* rot = nullptr;  // [n_frames][16] from the backward prologue
   float* grad = nullptr;        // [n_frames][n_atoms][3]
   // scratch
-  double* partial = nullptr;    // [n_frames][n_tiles][16]
-  unsigned* counter = nullptr;  // [n_frames], zero between launches
+  double* partial = nullptr;    // [n_frames][n_tiles][16] per-tile sums
+  double* refine = nullptr;     // [n_frames][16] records of frames needing the residual pass
+  unsigned* refine_count = nullptr;  // number of records, zeroed before each forward
   int* status = nullptr;        // device-visible status word (mapped host)
   int grid = 0;                 // CTAs (persistent)
 };
 
+// A frame whose RMSD is below kRefineScale * (G_x + G_y) / n (A^-1 * A^2) is
+// recomputed from explicit residuals: there the one-pass G_x + G_y - 2 lambda
+// route would leave cancellation noise of ~1e-14 (G_x + G_y) / n in the MSD.
+constexpr double kRefineScale = 1e-7;
+
 int frame_tiles(const FrameLaunch& L);
 size_t frame_smem_bytes(int stride, int tile_atoms);
+// Forward: zeroes L.refine_count, runs the fused kernel, then the residual pass
+// over the frames it flagged.
 cudaError_t launch_rmsd_forward(const FrameLaunch& L, cudaStream_t s);
 cudaError_t launch_rmsd_backward(const FrameLaunch& L, const double* stats, const float* grad_rmsd,
                                  double* rot_scratch, cudaStream_t s);
