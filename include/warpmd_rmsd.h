@@ -68,7 +68,8 @@ typedef struct wmd_ref wmd_ref;
 int wmd_create(int device, wmd_ctx** out);
 int wmd_destroy(wmd_ctx* ctx);
 /* Message of the last failing call on ctx (never NULL; "" when none).  With
- * ctx == NULL, the message of the last failing wmd_create on this thread. */
+ * ctx == NULL, the message of the last failing wmd_create or
+ * wmd_rmsd_frames_noalloc on this thread. */
 const char* wmd_last_error(const wmd_ctx* ctx);
 /* Library version string, e.g. "0.4.30+b200.1". */
 const char* wmd_version(void);
@@ -141,6 +142,27 @@ typedef struct wmd_batch_desc {
  * No counterpart in the reference, which runs one plan per trajectory. */
 int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, int n_traj, int with_grad);
 int wmd_batched_rmsd(wmd_ctx* ctx, const wmd_batch_desc* descs, int n_traj, int with_grad, void* stream);
+
+/* Per-frame aligned RMSD for callers that cannot allocate memory.  No
+ * counterpart in the reference.  Everything else in this header needs a
+ * wmd_ctx and a wmd_ref, which allocate device and pinned memory; this call
+ * allocates nothing, for code that runs where allocation is forbidden or
+ * unsafe (inside a host callback or a real-time loop, in a plugin whose host
+ * program owns all GPU memory, or without a context to keep workspaces in).
+ *   coords : device, [n_frames][n_atoms][stride]; the first n_sel atoms of each
+ *            frame are used (dense selection)
+ *   ref    : device, [n_sel][ref_stride] reference structure
+ *   out    : device, n_frames doubles -- the same values as wmd_rmsd_frames
+ *            with align = 1 (FP64 statistics and QCP)
+ * Runs asynchronously on `stream` on the current CUDA device.  Its scratch is
+ * one fixed 16 MiB array inside the library (held by every GPU that loads the
+ * library until exit), so n_sel is limited to 65,536 atoms; larger selections
+ * are rejected with WMD_ERR_INVALID_ARG (message via wmd_last_error(NULL)).
+ * The first call on a device looks up that array's device address; make it
+ * before any stream capture.  All calls on a device share the array: calls
+ * that may overlap on the GPU race and must be serialised by the caller. */
+int wmd_rmsd_frames_noalloc(const float* coords, int64_t n_frames, int64_t n_atoms, int stride, const float* ref,
+                            int64_t n_sel, int ref_stride, double* out, void* stream);
 
 #ifdef __cplusplus
 }

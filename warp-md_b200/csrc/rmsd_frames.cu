@@ -535,6 +535,11 @@ cudaError_t launch_rmsd_forward(const FrameLaunch& L, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+cudaError_t launch_rmsd_stream(const FrameLaunch& L, cudaStream_t s) {
+  if (L.n_frames == 0) return cudaSuccess;
+  return dispatch<kFwdFit>(L, s);
+}
+
 cudaError_t launch_rmsd_backward(const FrameLaunch& L, const double* stats, const float* grad_rmsd,
                                  double* rot_scratch, cudaStream_t s) {
   if (L.n_frames == 0) return cudaSuccess;

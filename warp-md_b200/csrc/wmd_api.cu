@@ -332,6 +332,8 @@ int forward_host(wmd_ctx* ctx, const float* hcoords, Mem kind, int64_t n_frames,
 
 }  // namespace
 
+void wmd::set_thread_error(const char* msg) { g_create_error = msg; }
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------

@@ -60,11 +60,17 @@ struct FrameLaunch {
 // route would leave cancellation noise of ~1e-14 (G_x + G_y) / n in the MSD.
 constexpr double kRefineScale = 1e-7;
 
+// Records the message wmd_last_error(NULL) returns on this thread.
+void set_thread_error(const char* msg);
+
 int frame_tiles(const FrameLaunch& L);
 size_t frame_smem_bytes(int stride, int tile_atoms);
 // Forward: zeroes L.refine_count, runs the fused kernel, then the residual pass
 // over the frames it flagged.
 cudaError_t launch_rmsd_forward(const FrameLaunch& L, cudaStream_t s);
+// Only the streaming kernel of the aligned forward (tile partials into
+// L.partial); the caller finishes the frames itself.
+cudaError_t launch_rmsd_stream(const FrameLaunch& L, cudaStream_t s);
 cudaError_t launch_rmsd_backward(const FrameLaunch& L, const double* stats, const float* grad_rmsd,
                                  double* rot_scratch, cudaStream_t s);
 // occupancy-derived persistent grid for a launch
