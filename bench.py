@@ -137,6 +137,86 @@ def cpu_baseline(threads: int, n_frames: int, seed: int = 7, frames=None, ref=No
     return (N_ATOMS * fr.shape[0]) / dt, dt, vals
 
 
+PAIR_ATOMS = 1000
+PAIR_WORKLOAD = ("all-pairs 2D-RMSD matrix: 20,000 frames x 1,000 atoms, slow random drift (N(0, 0.1 A) per "
+                 "atom per frame) under per-frame random rigid motions, float32")
+
+
+def _bf16_peak():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            return float(json.load(fh)["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
+def run_pairwise(args, ctx, stream, rank):
+    """All-pairs workload: plain FP32 CUDA-core form vs the tensor-core forms
+    (int8 limbs, exact int32 accumulation), each with an FP64 QCP epilogue.
+    Errors are measured against the FP64 oracle on a 512 x 512 block."""
+    import numpy as np
+    import torch
+
+    from warp_md import _native as N
+    from warp_md import synth
+    from warp_md.plans import _PAIR_MODES
+
+    F = args.pair_frames
+    n = PAIR_ATOMS
+    coords = synth.make_drift_trajectory_torch(n, F, 0.1, seed=3 + rank, device="cuda")
+    out = torch.empty(F, F, dtype=torch.float32, device="cuda")
+    pairs = F * (F - 1) / 2
+    res = {"metric": "2D-RMSD pairs/s", "unit": "pairs/s", "config": PAIR_WORKLOAD, "n_frames": F, "n_atoms": n}
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import oracle
+
+    blk = min(512, F)
+    host_blk = coords[:blk].cpu().numpy()
+    _, exact = oracle.pairwise(host_blk, "rms")
+    peak, peak_kind = _bf16_peak()
+    n_pad64 = (n + 63) // 64 * 64
+    for mode in args.pair_modes.split(","):
+        def step():
+            ctx.check(ctx.lib.wmd_pairwise_rmsd(ctx.handle, coords.data_ptr(), F, n, 3, None, n, N.PAIR_RMS,
+                                                _PAIR_MODES[mode], out.data_ptr(), stream.cuda_stream))
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.pair_steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.pair_steps
+        got = out[:blk, :blk].cpu().numpy()
+        err = np.abs(got - exact)
+        entry = {"ms": ms, "value": pairs / (ms / 1e3), "max_err_A": float(err.max()),
+                 "rms_err_A": float(np.sqrt((err ** 2).mean())),
+                 "useful_tflops": 18.0 * n * pairs / (ms / 1e3) / 1e12}
+        if mode in ("i8x3", "i8x2"):
+            limbs = 3 if mode == "i8x3" else 2
+            ni, nj = (F + 39) // 40, (F + 29) // 30
+            tiles = sum(1 for bi in range(ni) for bj in range(nj)
+                        if bi * 40 < min((bj + 1) * 30, F) - 1)
+            issued = 2.0 * 128 * 96 * limbs * limbs * n_pad64 * tiles
+            ach = issued / (ms / 1e3) / 1e12
+            entry["roofline"] = {"bound": "tensor", "achieved": ach, "peak": 2 * peak, "unit": "TOP/s (int8)",
+                                 "frac": ach / (2 * peak),
+                                 "peak_source": f"2 x {peak_kind} dense bf16 ({peak} TFLOP/s, MEASURED_PEAKS.json): "
+                                                "int8 MMA rate is twice the bf16 rate",
+                                 "issued_int8_ops": issued, "note": "includes whole tile launches"}
+        res[mode] = entry
+    if "fp32" in res and "i8x3" in res:
+        res["speedup_i8x3_vs_fp32"] = res["fp32"]["ms"] / res["i8x3"]["ms"]
+    if "fp32" in res and "i8x2" in res:
+        res["speedup_i8x2_vs_fp32"] = res["fp32"]["ms"] / res["i8x2"]["ms"]
+    del out, coords
+    torch.cuda.empty_cache()
+    return res
+
+
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
@@ -288,6 +368,9 @@ def run_ours(args):
                "max_abs_err_gpu_vs_cpu_A": err}
     del host
 
+    pairwise = None
+    if not args.skip_pairwise:
+        pairwise = run_pairwise(args, ctx, stream, rank)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -304,8 +387,9 @@ def run_ours(args):
                          "algorithmic_bytes_per_launch": alg_bytes},
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": args.steps,
+            "gpu_launches": 3 * args.steps,
             "clocks": clocks,
+            "pairwise": pairwise,
         }
         print(json.dumps(line), flush=True)
     r.close()
@@ -317,7 +401,7 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-frames", type=int, default=10_000)
@@ -327,6 +411,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-pairwise", action="store_true")
+    ap.add_argument("--pair-frames", type=int, default=20_000)
+    ap.add_argument("--pair-steps", type=int, default=3)
+    ap.add_argument("--pair-modes", default="fp32,i8x3,i8x2")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

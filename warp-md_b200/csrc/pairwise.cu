@@ -12,8 +12,9 @@
 // centred frames, and a per-pair FP64 epilogue turns each 3x3 block into an
 // RMSD (QCP for "rms"; G_i + G_j - 2 tr H + n |c_i - c_j|^2 for "nofit").
 //
-// This file holds the SIMT forms (FP32 and FP64 accumulation); the
-// tensor-core forms live in pairwise_tc.cu.
+// This file holds the SIMT forms (FP32 and FP64 accumulation, the plain GPU
+// baseline and the on-GPU accuracy reference); the tensor-core forms live in
+// pairwise_tc.cu.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -28,10 +29,15 @@
 
 namespace wmd {
 
-constexpr int kPairKc = 32;  // atoms per K step of the SIMT tiles
+constexpr int kPairKc = 32;      // atoms per K step of the SIMT tiles
+constexpr int kPanelFrames = 32;  // frames per panel (= per SIMT block side)
+constexpr int kPanelRows = 3 * kPanelFrames;
 
-// Centres each selected frame.  One CTA per frame.  Output layout
-// xc[f][c][n_pad] (atoms contiguous per component, zero padded).
+// Centres each selected frame (one CTA per frame) and stores it in the panel
+// layout the SIMT tiles read: panel b = frames [32b, 32b + 32) as
+// P[b][k][3 (f - 32b) + c] (k = atom, zero padded to n_pad), so one K step of
+// a tile is one contiguous 32 x 96 block.  G_f is the FP64 sum of squares of
+// the stored (rounded) values, so H and G describe the same coordinates.
 template <typename T>
 __global__ void __launch_bounds__(256) pair_prep(const float* __restrict__ coords, int64_t n_atoms, int stride,
                                                  const uint32_t* __restrict__ sel, int64_t n_sel, int64_t n_pad,
@@ -63,9 +69,10 @@ __global__ void __launch_bounds__(256) pair_prep(const float* __restrict__ coord
   const double inv = n_sel > 0 ? 1.0 / (double)n_sel : 0.0;
   c[0] *= inv; c[1] *= inv; c[2] *= inv;
   __syncthreads();
-  T* row = xc + (size_t)f * 3 * n_pad;
+  T* panel = xc + (size_t)(f / kPanelFrames) * n_pad * kPanelRows + 3 * (f % kPanelFrames);
   double g = 0;
   for (int64_t k = threadIdx.x; k < n_pad; k += blockDim.x) {
+    T* dst = panel + (size_t)k * kPanelRows;
     if (k < n_sel) {
       int64_t idx = sel ? (int64_t)sel[k] : k;
       if (idx >= n_atoms) idx = 0;
@@ -73,11 +80,11 @@ __global__ void __launch_bounds__(256) pair_prep(const float* __restrict__ coord
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
         const T v = (T)((double)p[q] - c[q]);
-        row[q * n_pad + k] = v;
+        dst[q] = v;
         g += (double)v * (double)v;
       }
     } else {
-      row[k] = T(0); row[n_pad + k] = T(0); row[2 * n_pad + k] = T(0);
+      dst[0] = T(0); dst[1] = T(0); dst[2] = T(0);
     }
   }
   for (int o = 16; o; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);
@@ -104,75 +111,95 @@ __device__ __forceinline__ double pair_rmsd(const double h[9], double gi, double
   return sqrt(msd_from(gi, gj, q.lambda, n));
 }
 
-// SIMT tile: 16x16 threads, each owning FA x FB frame pairs (full 3x3 blocks in
-// registers).  Block covers frames [I0, I0 + 16 FA) x [J0, J0 + 16 FB); only
-// pairs i < j are computed and written to both (i, j) and (j, i).
-template <typename T, int FA, int FB>
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Two consecutive T values from shared memory (8 or 16 bytes, aligned).
+template <typename T>
+struct Pair2 { T x, y; };
+
+// SIMT tile over one (row panel, column panel) pair of 32 frames each: 16 x 16
+// threads, thread (ty, tx) owns frames 2ty, 2ty+1 x 2tx, 2tx+1 -- four full 3x3
+// covariance blocks, 36 FMAs per atom against 6 vector shared loads.  K steps
+// of 32 atoms are double-buffered with cp.async.  Only pairs i < j are
+// finished (FP64 epilogue) and written to both (i, j) and (j, i).
+template <typename T>
 __global__ void __launch_bounds__(256) pair_tile_simt(const T* __restrict__ xc, const double* __restrict__ gsum,
                                                       const double* __restrict__ cen, int64_t F, int64_t n_pad,
                                                       double n, int metric, float* __restrict__ out) {
-  constexpr int BI = 16 * FA, BJ = 16 * FB;
-  constexpr int RA = 3 * BI, RB = 3 * BJ;
-  constexpr int LD = kPairKc + 1;
+  constexpr int kStep = kPairKc * kPanelRows;  // elements per panel K step
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* As = reinterpret_cast<T*>(smem_raw);
-  T* Bs = As + RA * LD;
-  const int64_t I0 = (int64_t)blockIdx.y * BI, J0 = (int64_t)blockIdx.x * BJ;
-  if (I0 >= J0 + BJ - 1 || I0 >= F || J0 >= F) return;  // no pair with i < j in this block
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  T acc[FA][FB][9];
+  T* As = reinterpret_cast<T*>(smem_raw);      // [2][kPairKc][96]
+  T* Bs = As + 2 * kStep;
+  const int bi = blockIdx.y, bj = blockIdx.x;
+  if (bi > bj) return;
+  const int64_t I0 = (int64_t)bi * kPanelFrames, J0 = (int64_t)bj * kPanelFrames;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const T* pa = xc + (size_t)bi * n_pad * kPanelRows;
+  const T* pb = xc + (size_t)bj * n_pad * kPanelRows;
+  constexpr int kVec = 16 / sizeof(T);         // elements per 16-byte copy
+  constexpr int kCopies = kStep / kVec;        // per operand per step
+  auto load = [&](int buf, int64_t k0) {
+    const T* ga = pa + (size_t)k0 * kPanelRows;
+    const T* gb = pb + (size_t)k0 * kPanelRows;
+    for (int c = tid; c < kCopies; c += 256) {
+      cp_async16(As + buf * kStep + c * kVec, ga + c * kVec);
+      cp_async16(Bs + buf * kStep + c * kVec, gb + c * kVec);
+    }
+    cp_async_commit();
+  };
+  T acc[2][2][9];
 #pragma unroll
-  for (int a = 0; a < FA; ++a)
+  for (int a = 0; a < 2; ++a)
 #pragma unroll
-    for (int b = 0; b < FB; ++b)
+    for (int b = 0; b < 2; ++b)
 #pragma unroll
       for (int e = 0; e < 9; ++e) acc[a][b][e] = T(0);
-
-  for (int64_t k0 = 0; k0 < n_pad; k0 += kPairKc) {
-    // stage rows (frame, component) x kPairKc atoms
-    for (int idx = threadIdx.x; idx < (RA + RB) * kPairKc; idx += 256) {
-      const int r = idx / kPairKc, kk = idx % kPairKc;
-      T v = T(0);
-      if (r < RA) {
-        const int64_t fr = I0 + r / 3;
-        if (fr < F) v = xc[((size_t)fr * 3 + (r % 3)) * n_pad + k0 + kk];
-        As[r * LD + kk] = v;
-      } else {
-        const int rb = r - RA;
-        const int64_t fr = J0 + rb / 3;
-        if (fr < F) v = xc[((size_t)fr * 3 + (rb % 3)) * n_pad + k0 + kk];
-        Bs[rb * LD + kk] = v;
-      }
+  const int steps = (int)(n_pad / kPairKc);
+  load(0, 0);
+  for (int st = 0; st < steps; ++st) {
+    const int buf = st & 1;
+    if (st + 1 < steps) {
+      load(buf ^ 1, (int64_t)(st + 1) * kPairKc);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
+    const T* A = As + buf * kStep + 6 * ty;
+    const T* B = Bs + buf * kStep + 6 * tx;
 #pragma unroll 4
     for (int kk = 0; kk < kPairKc; ++kk) {
-      T xa[FA][3], xb[FB][3];
+      T xa[6], xb[6];
 #pragma unroll
-      for (int a = 0; a < FA; ++a)
+      for (int v = 0; v < 3; ++v) {
+        const Pair2<T> qa = *reinterpret_cast<const Pair2<T>*>(A + kk * kPanelRows + 2 * v);
+        const Pair2<T> qb = *reinterpret_cast<const Pair2<T>*>(B + kk * kPanelRows + 2 * v);
+        xa[2 * v] = qa.x; xa[2 * v + 1] = qa.y;
+        xb[2 * v] = qb.x; xb[2 * v + 1] = qb.y;
+      }
 #pragma unroll
-        for (int q = 0; q < 3; ++q) xa[a][q] = As[((ty * FA + a) * 3 + q) * LD + kk];
+      for (int a = 0; a < 2; ++a)
 #pragma unroll
-      for (int b = 0; b < FB; ++b)
-#pragma unroll
-        for (int q = 0; q < 3; ++q) xb[b][q] = Bs[((tx * FB + b) * 3 + q) * LD + kk];
-#pragma unroll
-      for (int a = 0; a < FA; ++a)
-#pragma unroll
-        for (int b = 0; b < FB; ++b)
+        for (int b = 0; b < 2; ++b)
 #pragma unroll
           for (int p = 0; p < 3; ++p)
 #pragma unroll
-            for (int q = 0; q < 3; ++q) acc[a][b][p * 3 + q] = fma(xa[a][p], xb[b][q], acc[a][b][p * 3 + q]);
+            for (int q = 0; q < 3; ++q)
+              acc[a][b][p * 3 + q] = fma(xa[3 * a + p], xb[3 * b + q], acc[a][b][p * 3 + q]);
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int a = 0; a < FA; ++a) {
-    const int64_t i = I0 + ty * FA + a;
+  for (int a = 0; a < 2; ++a) {
+    const int64_t i = I0 + 2 * ty + a;
 #pragma unroll
-    for (int b = 0; b < FB; ++b) {
-      const int64_t j = J0 + tx * FB + b;
+    for (int b = 0; b < 2; ++b) {
+      const int64_t j = J0 + 2 * tx + b;
       if (i < j && j < F) {
         double h[9];
 #pragma unroll
@@ -209,17 +236,16 @@ static int grow(void** p, size_t* have, size_t want, std::string* msg) {
   return 0;
 }
 
-template <typename T, int FA, int FB>
+template <typename T>
 static cudaError_t run_simt(PairwiseWorkspace& w, int64_t F, int64_t n_pad, int64_t n_sel, int metric, float* out,
                             cudaStream_t s) {
-  constexpr int BI = 16 * FA, BJ = 16 * FB;
-  const size_t smem = (size_t)(3 * BI + 3 * BJ) * (kPairKc + 1) * sizeof(T);
-  auto kern = pair_tile_simt<T, FA, FB>;
+  const size_t smem = (size_t)4 * kPairKc * kPanelRows * sizeof(T);
+  auto kern = pair_tile_simt<T>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((unsigned)((F + BJ - 1) / BJ), (unsigned)((F + BI - 1) / BI));
-  kern<<<grid, 256, smem, s>>>(static_cast<const T*>(w.centred), w.gsum, w.cen, F, n_pad, (double)n_sel, metric,
-                               out);
+  const unsigned nb = (unsigned)((F + kPanelFrames - 1) / kPanelFrames);
+  dim3 grid(nb, nb);
+  kern<<<grid, 256, smem, s>>>(static_cast<const T*>(w.centred), w.gsum, w.cen, F, n_pad, (double)n_sel, metric, out);
   return cudaGetLastError();
 }
 
@@ -241,8 +267,15 @@ int pairwise_run(PairwiseWorkspace& w, int sm_count, const float* coords, int64_
   const bool f64 = mode == WMD_MODE_FP64;
   const int64_t n_pad = (n_sel + kPairKc - 1) / kPairKc * kPairKc;
   const size_t elem = f64 ? sizeof(double) : sizeof(float);
-  int rc = grow(&w.centred, &w.centred_bytes, (size_t)n_frames * 3 * n_pad * elem, msg);
+  const int64_t panels = (n_frames + kPanelFrames - 1) / kPanelFrames;
+  int rc = grow(&w.centred, &w.centred_bytes, (size_t)panels * n_pad * kPanelRows * elem, msg);
   if (rc) return rc;
+  // frames past the end of the last panel stay zero
+  e = cudaMemsetAsync(w.centred, 0, (size_t)panels * n_pad * kPanelRows * elem, s);
+  if (e != cudaSuccess) {
+    *msg = std::string("cuda driver error: ") + cudaGetErrorString(e);
+    return WMD_ERR_CUDA;
+  }
   if (w.frames_cap < (size_t)n_frames) {
     if (w.gsum) cudaFree(w.gsum);
     if (w.cen) cudaFree(w.cen);
@@ -264,8 +297,8 @@ int pairwise_run(PairwiseWorkspace& w, int sm_count, const float* coords, int64_
     pair_prep<float><<<(unsigned)n_frames, 256, 0, s>>>(coords, n_atoms, stride, sel, n_sel, n_pad,
                                                         static_cast<float*>(w.centred), w.gsum, w.cen, status);
   e = cudaGetLastError();
-  if (e == cudaSuccess) e = f64 ? run_simt<double, 2, 2>(w, n_frames, n_pad, n_sel, metric, out, s)
-                                : run_simt<float, 4, 2>(w, n_frames, n_pad, n_sel, metric, out, s);
+  if (e == cudaSuccess) e = f64 ? run_simt<double>(w, n_frames, n_pad, n_sel, metric, out, s)
+                                : run_simt<float>(w, n_frames, n_pad, n_sel, metric, out, s);
   if (e != cudaSuccess) {
     *msg = std::string("cuda driver error: pairwise launch: ") + cudaGetErrorString(e);
     return WMD_ERR_CUDA;

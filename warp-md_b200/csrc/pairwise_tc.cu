@@ -1,13 +1,632 @@
-// pairwise_tc.cu -- tensor-core forms of the pairwise RMSD matrix (pending).
+// pairwise_tc.cu -- all-pairs RMSD matrix on the tcgen05 tensor cores.
+//
+// Arithmetic.  Each frame is centred in FP64 and quantised to fixed point with
+// one scale s for the whole trajectory: q = round((x - c) / s), |q| <= qmax
+// (24-bit: qmax = 2^23 - 2^16; 16-bit: 2^15 - 2^8).  q is split into signed
+// int8 limbs q = sum_p a_p 2^(8p) (balanced digits in [-128, 127]).  The
+// covariance of a frame pair is then
+//     H_ij = s^2 sum_{p,r} 2^(8(p+r)) sum_k a_p(i,k) a_r(j,k),
+// i.e. 2*LIMBS - 1 "shift groups" g = p + r of int8 x int8 GEMMs whose int32
+// accumulation is exact (checked: 3 n 128^2 < 2^31 for n < 43,690 atoms).  The
+// tensor cores thus produce the exact Gram matrix of the quantised frames; the
+// only approximation is the quantisation (<= s/2 per coordinate, s ~ 1e-5 A for
+// 24-bit at 100 A extent), and the FP64 epilogue combines the groups and runs
+// QCP per pair.  Split-BF16 with FP32 accumulation cannot do this: dropping or
+// rounding the lo*lo products biases n*MSD by ~n |lo|^2, which at 1,000 atoms
+// is ~1e-2 A in RMSD for adjacent frames.
+//
+// Layout.  Rows of the GEMM are (frame, component); 10 frames occupy 32 rows
+// (30 used), so a 128-row tile holds 40 frames and a frame's three rows sit in
+// one warp's TMEM lane quarter.  The limb array is L[limb][row][k] (k = atom,
+// padded to 64) and serves as both A (tile of 128 rows = 40 frames) and B
+// (96 rows = 30 frames); D = A B^T, both operands K-major.
+//
+// Kernel.  Persistent, one CTA per SM, warp-specialised:
+//   warp 0     TMA producer: per 64-atom K chunk one 3-D box per operand
+//              (all limbs at once), SWIZZLE_64B, 3-4 stage mbarrier ring;
+//   warp 1     allocates 512 TMEM columns; lane 0 issues tcgen05.mma
+//              kind::i8 (M=128, N=96, K=32) for every limb pair into the
+//              pair's shift-group accumulator (5 x 96 columns for 3 limbs),
+//              commits stages back to the producer and tiles to the epilogue;
+//   warps 2-13 drain: tcgen05.ld of its 32 lanes x 32 columns per group,
+//              exact combination of the groups in int64, its 30 x 30 block of
+//              H staged in shared memory, release of TMEM (the next tile's
+//              MMAs start);
+//   warps 14-21 stage the tile's per-frame terms (G, centroids);
+//   warps 2-21 then run the FP64 pair epilogue (QCP) for the tile's 1,200
+//              pairs, one pair per lane per round, and the symmetric store.
+// Every wait is bounded; a wait that runs out raises the CTA's abort flag and
+// all roles leave, after the MMAs in flight are drained and TMEM is freed.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <string>
+
 #include "../../include/warpmd_rmsd.h"
+#include "device_util.cuh"
 #include "pairwise_tc.h"
+#include "qcp.cuh"
 
 namespace wmd {
+namespace {
 
-int pairwise_tc_run(PairwiseWorkspace&, int, const float*, int64_t, int64_t, int, const uint32_t*, int64_t, int, int,
-                    float*, int*, cudaStream_t, std::string* msg) {
-  *msg = "tensor-core pairwise modes are not built in this version";
-  return WMD_ERR_UNSUPPORTED;
+constexpr int kFramesPerQuarter = 10;  // frames per 32 TMEM lanes
+constexpr int kTileM = 128;            // GEMM rows per tile (40 frames)
+constexpr int kTileFramesM = 40;
+constexpr int kTileN = 96;             // GEMM columns per tile (30 frames)
+constexpr int kTileFramesN = 30;
+constexpr int kSliceCols = 32;         // epilogue columns per warp: one 32-row group of B
+constexpr int kSliceFrames = kFramesPerQuarter;  // 10 frames (30 columns + 2 pad)
+constexpr int kSlices = kTileN / kSliceCols;  // 3
+constexpr int kEpiWarps = 4 * kSlices; // 12 drain warps: every (lane quarter, slice)
+constexpr int kHelpWarps = 8;          // extra warps for the per-pair FP64 epilogue
+constexpr int kQcpWarps = kEpiWarps + kHelpWarps;
+constexpr int kTcThreads = 64 + 32 * kQcpWarps;
+constexpr int kKChunk = 64;            // atoms (= bytes per operand row) per stage
+constexpr int kTmemCols = 512;
+constexpr int kEpiLd = 31;             // row pitch (doubles) of the per-warp 30 x 30 H staging
+constexpr int kEpiWarpBytes = 30 * kEpiLd * 8;
+
+template <int LIMBS>
+struct TcGeo {
+  static constexpr int kGroups = 2 * LIMBS - 1;
+  static constexpr int kStages = LIMBS == 3 ? 3 : 4;  // fits 227 KB with the H staging
+  static constexpr int kALimbBytes = kTileM * kKChunk;  // 8 KB
+  static constexpr int kBLimbBytes = kTileN * kKChunk;  // 6 KB
+  static constexpr int kABytes = LIMBS * kALimbBytes;
+  static constexpr int kBBytes = LIMBS * kBLimbBytes;
+  static constexpr int kStageBytes = kABytes + kBBytes;
+  static constexpr int kEpiOffset = kStages * kStageBytes;
+  static constexpr int kFrameOffset = kEpiOffset + kEpiWarps * kEpiWarpBytes;  // per-tile frame terms
+  static constexpr int kBarOffset = kFrameOffset + 4 * (kTileFramesM + kTileFramesN) * 8;
+  // full[8], empty[8], tmem_full, tmem_empty, drain, tmem address, abort flag
+  static constexpr int kSmemBytes = kBarOffset + 24 * 8 + 64;
+  static constexpr int kQmax = LIMBS == 3 ? (1 << 23) - (1 << 16) : (1 << 15) - (1 << 8);
+};
+
+// ------------------------------------------------------------------ PTX --
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst_smem, int ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(dst_smem)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, int ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// 32 lanes x 8 consecutive 32-bit TMEM columns -> 8 registers per thread
+// (call tmem_wait_ld before using them)
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, int32_t* v) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// Shared-memory matrix descriptor, K-major, SWIZZLE_64B (rows of 64 bytes,
+// 8-row core groups 512 bytes apart), sm_100 descriptor version 1.
+__device__ __forceinline__ uint64_t desc_sw64(const void* p) {
+  const uint64_t start = (smem_addr(p) >> 4) & 0x3FFFu;
+  return start | (uint64_t(1) << 16) | (uint64_t(512 >> 4) << 32) | (uint64_t(1) << 46) | (uint64_t(4) << 61);
+}
+
+// kind::i8 instruction descriptor: D s32, A/B s8, both K-major, M=128, N=96.
+constexpr uint32_t kIdesc = (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(kTileN >> 3) << 17) |
+                            (uint32_t(kTileM >> 4) << 24);
+
+// bounded wait on an mbarrier phase (no shared abort fallback needed by
+// callers other than through the flag)
+__device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t parity, int* status, volatile int* abort) {
+  return mbar_wait(bar, parity, status, kStatusTimeoutFull, abort);
+}
+
+struct TileList {
+  int ni, nj;  // I blocks (40 frames) x J blocks (30 frames)
+  int64_t F;
+  __device__ __forceinline__ bool valid(int64_t t, int& bi, int& bj) const {
+    bi = (int)(t / nj);
+    bj = (int)(t - (int64_t)bi * nj);
+    const int64_t i0 = (int64_t)bi * kTileFramesM;
+    const int64_t jmax = min((int64_t)(bj + 1) * kTileFramesN, F) - 1;
+    return i0 < jmax && (int64_t)bj * kTileFramesN < F;  // some pair i < j in the tile
+  }
+};
+
+struct TcArgs {
+  int64_t F;
+  int64_t n_pad;      // atoms padded to kKChunk
+  double n;           // selected atoms
+  int metric;
+  const double* gsum;  // [F] sum |q|^2 (units of s^2)
+  const double* cen;   // [F][3] centroids (A)
+  const double* scale; // device scalar s
+  float* out;          // [F][F]
+  int* status;
+};
+
+// -------------------------------------------------------------- kernel --
+
+template <int LIMBS>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    pair_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
+                   const TcArgs args, const TileList tiles) {
+  using G = TcGeo<LIMBS>;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  constexpr int kStagesTc = G::kStages;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + G::kBarOffset);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + 8;
+  uint64_t* tmem_full = bars + 16;
+  uint64_t* tmem_empty = tmem_full + 1;
+  uint64_t* drain = tmem_full + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + G::kBarOffset + 24 * 8);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + G::kBarOffset + 24 * 8 + 16);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n_k = (int)(args.n_pad / kKChunk);
+  const int64_t n_tiles = (int64_t)tiles.ni * tiles.nj;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStagesTc; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(tmem_full, 1);
+    mbar_init(tmem_empty, kEpiWarps);
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    fence_barrier_init();
+  }
+  if (warp == 1) tmem_alloc(tmem_slot, kTmemCols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      uint32_t it = 0;
+      bool ok = true;
+      for (int64_t t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+        int bi, bj;
+        if (!tiles.valid(t, bi, bj)) continue;
+        for (int kc = 0; kc < n_k; ++kc, ++it) {
+          const int s = it % kStagesTc;
+          const uint32_t ph = (it / kStagesTc) & 1u;
+          if (!tc_wait(&empty[s], ph ^ 1u, args.status, abort_flag)) { ok = false; break; }
+          unsigned char* st = smem + s * G::kStageBytes;
+          mbar_arrive_expect_tx(&full[s], G::kStageBytes);
+          tma_load_3d(st, &map_a, kc * kKChunk, bi * kTileM, 0, &full[s]);
+          tma_load_3d(st + G::kABytes, &map_b, kc * kKChunk, bj * kTileN, 0, &full[s]);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      uint32_t it = 0, tc = 0;
+      bool ok = true;
+      for (int64_t t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+        int bi, bj;
+        if (!tiles.valid(t, bi, bj)) continue;
+        // the epilogue must have drained the previous tile's accumulators
+        if (!tc_wait(tmem_empty, (tc & 1u) ^ 1u, args.status, abort_flag)) { ok = false; break; }
+        tc_fence_after();
+        for (int kc = 0; kc < n_k; ++kc, ++it) {
+          const int s = it % kStagesTc;
+          const uint32_t ph = (it / kStagesTc) & 1u;
+          if (!tc_wait(&full[s], ph, args.status, abort_flag)) { ok = false; break; }
+          tc_fence_after();
+          const unsigned char* st = smem + s * G::kStageBytes;
+#pragma unroll
+          for (int p = 0; p < LIMBS; ++p) {
+#pragma unroll
+            for (int r = 0; r < LIMBS; ++r) {
+              const int g = p + r;
+              // the first MMA of a group in a tile overwrites, the rest add
+              const bool first_pair = (p == (g < LIMBS ? 0 : g - LIMBS + 1));
+#pragma unroll
+              for (int ks = 0; ks < kKChunk / 32; ++ks) {
+                const uint64_t da = desc_sw64(st + p * G::kALimbBytes + ks * 32);
+                const uint64_t db = desc_sw64(st + G::kABytes + r * G::kBLimbBytes + ks * 32);
+                const uint32_t acc = (kc > 0 || !first_pair || ks > 0) ? 1u : 0u;
+                mma_i8(tmem_base + (uint32_t)(g * kTileN), da, db, kIdesc, acc);
+              }
+            }
+          }
+          tc_commit(&empty[s]);  // stage free once these MMAs have read it
+        }
+        if (!ok) break;
+        tc_commit(tmem_full);  // accumulators of this tile complete
+        ++tc;
+      }
+      // all MMAs issued by this thread must finish before TMEM is freed
+      tc_commit(drain);
+      const uint64_t t0 = global_timer_ns();
+      while (!mbar_try_wait(drain, 0)) {
+        if (global_timer_ns() - t0 > kWaitLimitNs) {
+          atomicOr(args.status, kStatusTimeoutDrain);
+          break;
+        }
+      }
+    }
+  } else {
+    // ---------------- epilogue ----------------
+    // warps 2-13 drain TMEM (each its lane quarter x 32-column slice) into
+    // shared memory; warps 14-21 stage the tile's per-frame terms; then all 20
+    // run the tile's pair epilogue (QCP) two rounds deep, between two named
+    // barriers (id 1 after staging, id 2 before the staging is rewritten).
+    const int wq = warp - 2;       // 0..19
+    const bool drainer = wq < kEpiWarps;
+    const int quarter = warp & 3;  // TMEM lane quarter a drain warp may access
+    const int slice = wq >> 2;     // 32-column slice (10 frames) of a drain warp
+    const double s = *args.scale;
+    const double s2 = s * s;
+    double* frm = reinterpret_cast<double*>(smem + G::kFrameOffset);  // [4][70]: g, cx, cy, cz
+    constexpr int kTf = kTileFramesM + kTileFramesN;
+    uint32_t tc = 0;
+    for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+      int bi, bj;
+      if (!tiles.valid(t, bi, bj)) continue;
+      if (drainer) {
+        if (tc_wait(tmem_full, tc & 1u, args.status, abort_flag)) {
+          tc_fence_after();
+          double* epi = reinterpret_cast<double*>(smem + G::kEpiOffset + wq * kEpiWarpBytes);
+#pragma unroll
+          for (int half = 0; half < 2; ++half) {
+            // columns [16 half, 16 half + 16) of the slice; 30 are frame columns
+            long long acc[16];
+#pragma unroll
+            for (int c = 0; c < 16; ++c) acc[c] = 0;
+#pragma unroll
+            for (int g = 0; g < G::kGroups; ++g) {
+              int32_t v[16];
+              const uint32_t col = tmem_base + ((uint32_t)(quarter * 32) << 16) +
+                                   (uint32_t)(g * kTileN + slice * kSliceCols + 16 * half);
+              tmem_ld8(col, v);
+              tmem_ld8(col + 8, v + 8);
+              tmem_wait_ld();
+#pragma unroll
+              for (int c = 0; c < 16; ++c) acc[c] += (long long)v[c] << (8 * g);
+            }
+            if (lane < 30) {
+#pragma unroll
+              for (int c = 0; c < 16; ++c)
+                if (16 * half + c < 30) epi[lane * kEpiLd + 16 * half + c] = (double)acc[c] * s2;
+            }
+          }
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(tmem_empty);  // MMAs of the next tile may start
+        }
+      } else {
+        // per-frame terms of the tile's 40 row frames and 30 column frames
+        for (int q = (wq - kEpiWarps) * 32 + lane; q < kTf; q += kHelpWarps * 32) {
+          const int64_t f = q < kTileFramesM ? (int64_t)bi * kTileFramesM + q
+                                             : (int64_t)bj * kTileFramesN + (q - kTileFramesM);
+          const bool in = f < args.F;
+          frm[q] = in ? args.gsum[f] * s2 : 0.0;
+          frm[kTf + q] = in ? args.cen[f * 3 + 0] : 0.0;
+          frm[2 * kTf + q] = in ? args.cen[f * 3 + 1] : 0.0;
+          frm[3 * kTf + q] = in ? args.cen[f * 3 + 2] : 0.0;
+        }
+      }
+      ++tc;
+      named_barrier_sync(1, 32 * kQcpWarps);
+      if (*abort_flag) break;
+      // 12 blocks x 100 pairs, two rounds of 20 warps x 32 lanes
+      constexpr int kPairs = kEpiWarps * kFramesPerQuarter * kSliceFrames;  // 1200
+#pragma unroll 1
+      for (int gp = wq * 32 + lane; gp < kPairs; gp += kQcpWarps * 32) {
+        const int blk = gp / 100, pl = gp - blk * 100;
+        const int pi = pl / kSliceFrames, pj = pl - pi * kSliceFrames;
+        const int bq = (blk + 2) & 3, bs = blk >> 2;  // lane quarter and slice of drain warp blk
+        const int fi = bq * kFramesPerQuarter + pi, fj = kTileFramesM + bs * kSliceFrames + pj;
+        const int64_t i = (int64_t)bi * kTileFramesM + fi - 0;
+        const int64_t j = (int64_t)bj * kTileFramesN + bs * kSliceFrames + pj;
+        if (!(i < j && j < args.F)) continue;
+        const double* epi = reinterpret_cast<const double*>(smem + G::kEpiOffset + blk * kEpiWarpBytes);
+        double h[9];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int b = 0; b < 3; ++b) h[a * 3 + b] = epi[(3 * pi + a) * kEpiLd + 3 * pj + b];
+        const double gi = frm[fi], gj = frm[fj];
+        double v;
+        if (args.metric == WMD_PAIR_NOFIT) {
+          const double d0 = frm[kTf + fi] - frm[kTf + fj];
+          const double d1 = frm[2 * kTf + fi] - frm[2 * kTf + fj];
+          const double d2 = frm[3 * kTf + fi] - frm[3 * kTf + fj];
+          const double ssq = gi + gj - 2.0 * (h[0] + h[4] + h[8]) + args.n * (d0 * d0 + d1 * d1 + d2 * d2);
+          v = ssq > 0.0 ? sqrt(ssq / args.n) : 0.0;
+        } else {
+          const QcpOut q = qcp_lambda<true>(h, 0.5 * (gi + gj));
+          v = sqrt(msd_from(gi, gj, q.lambda, args.n));
+        }
+        args.out[(size_t)i * args.F + j] = (float)v;
+        args.out[(size_t)j * args.F + i] = (float)v;
+      }
+      named_barrier_sync(2, 32 * kQcpWarps);  // staging may be rewritten
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, kTmemCols);
+  }
+}
+
+// --------------------------------------------------------------- prep --
+
+// Pass 1 (one CTA per frame): FP64 centroid and max |x - c| over the frame,
+// folded into a global maximum (non-negative floats compare as unsigned).
+__global__ void __launch_bounds__(256) tc_prep_centre(const float* __restrict__ coords, int64_t n_atoms, int stride,
+                                                      const uint32_t* __restrict__ sel, int64_t n_sel,
+                                                      double* __restrict__ cen, unsigned* __restrict__ maxbits,
+                                                      int* status) {
+  __shared__ double red[8][3];
+  __shared__ float mred[8];
+  const int64_t f = blockIdx.x;
+  const float* fr = coords + (size_t)f * n_atoms * stride;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double s0 = 0, s1 = 0, s2 = 0;
+  for (int64_t k = threadIdx.x; k < n_sel; k += blockDim.x) {
+    int64_t idx = sel ? (int64_t)sel[k] : k;
+    if (idx >= n_atoms) {
+      atomicOr(status, kStatusBadIndex);
+      idx = 0;
+    }
+    const float* p = fr + idx * stride;
+    s0 += p[0]; s1 += p[1]; s2 += p[2];
+  }
+  for (int o = 16; o; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  }
+  if (lane == 0) { red[warp][0] = s0; red[warp][1] = s1; red[warp][2] = s2; }
+  __syncthreads();
+  double c[3] = {0, 0, 0};
+  for (int w = 0; w < 8; ++w) { c[0] += red[w][0]; c[1] += red[w][1]; c[2] += red[w][2]; }
+  const double inv = 1.0 / (double)n_sel;
+  c[0] *= inv; c[1] *= inv; c[2] *= inv;
+  float m = 0.f;
+  for (int64_t k = threadIdx.x; k < n_sel; k += blockDim.x) {
+    int64_t idx = sel ? (int64_t)sel[k] : k;
+    if (idx >= n_atoms) idx = 0;
+    const float* p = fr + idx * stride;
+    for (int q = 0; q < 3; ++q) m = fmaxf(m, (float)fabs((double)p[q] - c[q]));
+  }
+  for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) mred[warp] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float mm = 0.f;
+    for (int w = 0; w < 8; ++w) mm = fmaxf(mm, mred[w]);
+    atomicMax(maxbits, __float_as_uint(mm));
+    cen[f * 3 + 0] = c[0]; cen[f * 3 + 1] = c[1]; cen[f * 3 + 2] = c[2];
+  }
+}
+
+// Pass 2 (one CTA per frame): quantise with the trajectory-wide scale and
+// write the int8 limbs L[p][row(f, a)][k]; G_f = sum q^2 exactly (int64).
+template <int LIMBS>
+__global__ void __launch_bounds__(256) tc_prep_limbs(const float* __restrict__ coords, int64_t n_atoms, int stride,
+                                                     const uint32_t* __restrict__ sel, int64_t n_sel, int64_t n_pad,
+                                                     int64_t rows, const double* __restrict__ cen,
+                                                     const unsigned* __restrict__ maxbits,
+                                                     int8_t* __restrict__ limbs, double* __restrict__ gsum,
+                                                     double* __restrict__ scale_out) {
+  __shared__ long long red[8];
+  constexpr int qmax = TcGeo<LIMBS>::kQmax;
+  const int64_t f = blockIdx.x;
+  const float mx = __uint_as_float(*maxbits);
+  const double s = mx > 0.f ? (double)mx / (double)qmax * (1.0 + 1e-12) : 1.0;
+  if (f == 0 && threadIdx.x == 0) *scale_out = s;
+  const double inv_s = 1.0 / s;
+  const float* fr = coords + (size_t)f * n_atoms * stride;
+  const double c[3] = {cen[f * 3 + 0], cen[f * 3 + 1], cen[f * 3 + 2]};
+  const int64_t row0 = (f / kFramesPerQuarter) * 32 + (f % kFramesPerQuarter) * 3;
+  long long g = 0;
+  for (int64_t k = threadIdx.x; k < n_sel; k += blockDim.x) {
+    int64_t idx = sel ? (int64_t)sel[k] : k;
+    if (idx >= n_atoms) idx = 0;
+    const float* p = fr + idx * stride;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      long long q = llrint(((double)p[a] - c[a]) * inv_s);
+      q = q > qmax ? qmax : (q < -qmax ? -qmax : q);
+      g += q * q;
+      int32_t rem = (int32_t)q;
+#pragma unroll
+      for (int l = 0; l < LIMBS; ++l) {
+        // balanced base-256 digit in [-128, 127]
+        int32_t d = ((rem % 256) + 256 + 128) % 256 - 128;
+        if (l == LIMBS - 1) d = rem;
+        limbs[((size_t)l * rows + row0 + a) * n_pad + k] = (int8_t)d;
+        rem = (rem - d) / 256;
+      }
+    }
+  }
+  for (int o = 16; o; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = g;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long t = 0;
+    for (int w = 0; w < 8; ++w) t += red[w];
+    gsum[f] = (double)t;
+  }
+}
+
+// ---------------------------------------------------------------- host --
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn(std::string* msg) {
+  static EncodeTiled fn = nullptr;
+  if (fn) return fn;
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !p) {
+    cudaGetLastError();
+    *msg = "cuda driver error: cuTensorMapEncodeTiled unavailable";
+    return nullptr;
+  }
+  fn = reinterpret_cast<EncodeTiled>(p);
+  return fn;
+}
+
+template <int LIMBS>
+int run_tc(PairwiseWorkspace& w, int sm_count, const float* coords, int64_t F, int64_t n_atoms, int stride,
+           const uint32_t* sel, int64_t n_sel, int metric, float* out, int* status, cudaStream_t s,
+           std::string* msg) {
+  using G = TcGeo<LIMBS>;
+  const int64_t n_pad = (n_sel + kKChunk - 1) / kKChunk * kKChunk;
+  const int64_t rows = (F + kFramesPerQuarter - 1) / kFramesPerQuarter * 32;
+  const int64_t rows_pad = (rows + kTileM - 1) / kTileM * kTileM;  // whole 128-row tiles
+  const size_t limb_bytes = (size_t)LIMBS * rows_pad * n_pad;
+  const size_t small = 256 + (size_t)F * (sizeof(double) * 4);
+  // workspace: [scale, maxbits | gsum F | cen 3F][limbs]
+  const size_t need = small + limb_bytes + 1024;
+  if (!w.extra || w.extra_bytes < need) {
+    if (w.extra) cudaFree(w.extra);
+    w.extra = nullptr;
+    w.extra_bytes = 0;
+    cudaError_t e = cudaMalloc(&w.extra, need);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      *msg = std::string("cuda driver error: pairwise workspace allocation failed: ") + cudaGetErrorString(e);
+      return WMD_ERR_OOM;
+    }
+    w.extra_bytes = need;
+  }
+  unsigned char* base = static_cast<unsigned char*>(w.extra);
+  double* scale = reinterpret_cast<double*>(base);
+  unsigned* maxbits = reinterpret_cast<unsigned*>(base + 8);
+  double* gsum = reinterpret_cast<double*>(base + 256);
+  double* cen = gsum + F;
+  int8_t* limbs = reinterpret_cast<int8_t*>(base + ((small + 1023) & ~size_t(1023)));
+
+  cudaError_t e = cudaMemsetAsync(base, 0, 256, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(limbs, 0, limb_bytes, s);
+  if (e != cudaSuccess) {
+    *msg = std::string("cuda driver error: ") + cudaGetErrorString(e);
+    return WMD_ERR_CUDA;
+  }
+  tc_prep_centre<<<(unsigned)F, 256, 0, s>>>(coords, n_atoms, stride, sel, n_sel, cen, maxbits, status);
+  tc_prep_limbs<LIMBS><<<(unsigned)F, 256, 0, s>>>(coords, n_atoms, stride, sel, n_sel, n_pad, rows_pad, cen, maxbits,
+                                                   limbs, gsum, scale);
+  if ((e = cudaGetLastError()) != cudaSuccess) {
+    *msg = std::string("cuda driver error: pairwise prep: ") + cudaGetErrorString(e);
+    return WMD_ERR_CUDA;
+  }
+
+  EncodeTiled enc = encode_fn(msg);
+  if (!enc) return WMD_ERR_CUDA;
+  CUtensorMap map_a, map_b;
+  const cuuint64_t dims[3] = {(cuuint64_t)n_pad, (cuuint64_t)rows_pad, (cuuint64_t)LIMBS};
+  const cuuint64_t strides[2] = {(cuuint64_t)n_pad, (cuuint64_t)(rows_pad * n_pad)};
+  const cuuint32_t box_a[3] = {kKChunk, kTileM, LIMBS};
+  const cuuint32_t box_b[3] = {kKChunk, kTileN, LIMBS};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(&map_a, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, limbs, dims, strides, box_a, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r == CUDA_SUCCESS)
+    r = enc(&map_b, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, limbs, dims, strides, box_b, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    *msg = "cuda driver error: cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
+    return WMD_ERR_CUDA;
+  }
+
+  TcArgs a;
+  a.F = F;
+  a.n_pad = n_pad;
+  a.n = (double)n_sel;
+  a.metric = metric;
+  a.gsum = gsum;
+  a.cen = cen;
+  a.scale = scale;
+  a.out = out;
+  a.status = status;
+  TileList tl;
+  tl.ni = (int)((F + kTileFramesM - 1) / kTileFramesM);
+  tl.nj = (int)((F + kTileFramesN - 1) / kTileFramesN);
+  tl.F = F;
+  auto kern = pair_tc_kernel<LIMBS>;
+  if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::kSmemBytes)) != cudaSuccess) {
+    *msg = std::string("cuda driver error: ") + cudaGetErrorString(e);
+    return WMD_ERR_CUDA;
+  }
+  const int64_t n_tiles = (int64_t)tl.ni * tl.nj;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(sm_count, n_tiles));
+  kern<<<grid, kTcThreads, G::kSmemBytes, s>>>(map_a, map_b, a, tl);
+  if ((e = cudaGetLastError()) != cudaSuccess) {
+    *msg = std::string("cuda driver error: pairwise tensor-core launch: ") + cudaGetErrorString(e);
+    return WMD_ERR_CUDA;
+  }
+  return 0;
+}
+
+}  // namespace
+
+int pairwise_tc_run(PairwiseWorkspace& w, int sm_count, const float* coords, int64_t n_frames, int64_t n_atoms,
+                    int stride, const uint32_t* sel, int64_t n_sel, int metric, int limbs, float* out, int* status,
+                    cudaStream_t s, std::string* msg) {
+  // exact int32 accumulation: LIMBS n_pad 128^2 < 2^31
+  const int64_t max_atoms = limbs == 3 ? 43648 : 65472;
+  if (n_sel > max_atoms) {
+    *msg = "tensor-core pairwise modes accept at most " + std::to_string(max_atoms) +
+           " selected atoms (exact int32 accumulation); use WMD_MODE_FP64";
+    return WMD_ERR_UNSUPPORTED;
+  }
+  if (n_frames > (int64_t)1 << 31) {
+    *msg = "too many frames for one pairwise call";
+    return WMD_ERR_INVALID_ARG;
+  }
+  return limbs == 3 ? run_tc<3>(w, sm_count, coords, n_frames, n_atoms, stride, sel, n_sel, metric, out, status, s, msg)
+                    : run_tc<2>(w, sm_count, coords, n_frames, n_atoms, stride, sel, n_sel, metric, out, status, s, msg);
 }
 
 }  // namespace wmd

@@ -118,13 +118,38 @@ WMD_HD double lambda_from_svd(const double h[9]) {
   return det3(h) < 0.0 ? sum - 2.0 * smin : sum;
 }
 
+#if defined(__CUDACC__)
+// Device-side out-of-line SVD route, so that code paths that only rarely need
+// it do not carry its registers.
+__device__ __noinline__ inline double lambda_from_svd_call(const double* h) { return lambda_from_svd(h); }
+#endif
+
 struct QcpOut {
   double lambda;
   int iters;     // Newton iterations used
   int fallback;  // 1 when lambda came from the SVD
 };
 
+// p / d for the Newton step.  With FAST, on the device and for d within the
+// normal float range, a float reciprocal refined by two Newton-Raphson steps
+// in FP64 (each doubles the correct bits: 24 -> 48 -> 96); the iteration is
+// self-correcting, so the last-bit difference to an IEEE division does not
+// change the converged root.
+template <bool FAST>
+WMD_HD double newton_div(double p, double d) {
+#if defined(__CUDA_ARCH__)
+  if (FAST && fabs(d) > 1e-30 && fabs(d) < 1e30) {
+    double r = (double)__frcp_rn((float)d);
+    r = fma(r, fma(-d, r, 1.0), r);
+    r = fma(r, fma(-d, r, 1.0), r);
+    return p * r;
+  }
+#endif
+  return p / d;
+}
+
 // Largest eigenvalue of K(H); e0 = (G_x + G_y) / 2 >= lambda_max.
+template <bool FAST = false>
 WMD_HD QcpOut qcp_lambda(const double h[9], double e0) {
   QcpOut o{0.0, 0, 0};
   if (!(e0 > 0.0)) return o;
@@ -145,7 +170,7 @@ WMD_HD QcpOut qcp_lambda(const double h[9], double e0) {
     const double p = a * l + c0;               // P(l)  = l^4 + c2 l^2 + c1 l + c0
     const double dp = 2.0 * l2 * l + b + a;    // P'(l) = 4 l^3 + 2 c2 l + c1
     if (!(dp != 0.0)) break;
-    const double delta = p / dp;
+    const double delta = newton_div<FAST>(p, dp);
     l -= delta;
     if (fabs(delta) <= 1e-15 * fabs(l)) {
       converged = true;
@@ -159,13 +184,21 @@ WMD_HD QcpOut qcp_lambda(const double h[9], double e0) {
   const double l3 = l * l * l;
   const double dp = 4.0 * l3 + 2.0 * c2 * l + c1;
   if (!converged || !(fabs(dp) > 1e-6 * 4.0 * fabs(l3)) || !(l == l)) {
+#if defined(__CUDA_ARCH__)
+    double tmp[9];  // only this rare branch takes an address
+    for (int i = 0; i < 9; ++i) tmp[i] = h[i];
+    o.lambda = lambda_from_svd_call(tmp);
+#else
     o.lambda = lambda_from_svd(h);
+#endif
     o.fallback = 1;
   } else {
     o.lambda = l;
   }
   return o;
 }
+
+
 
 // Mean-square deviation from the QCP eigenvalue, clamped at zero as the
 // reference does (math.rs:34-37).
