@@ -135,11 +135,23 @@ typedef struct wmd_batch_desc {
   float* grad;         /* [n_frames][n_atoms][3] output, or NULL         */
 } wmd_batch_desc;
 
-/* Per-frame RMSD (+ gradients when with_grad != 0 and grad != NULL) of n_traj
- * independent trajectories of uneven size in one persistent launch.  Performs
- * no allocation and no host synchronization once the context's workspace is
- * large enough (see wmd_batched_prepare), so it can be captured in a CUDA graph.
- * No counterpart in the reference, which runs one plan per trajectory. */
+/* Per-frame aligned RMSD (+ dRMSD/dx when with_grad != 0 and grad != NULL) of
+ * n_traj independent trajectories of uneven size, each against its own
+ * reference, in one persistent launch sequence.  No counterpart in the
+ * reference, which runs one RmsdPlan per trajectory (plan.rs:164-418); the
+ * values are those of wmd_rmsd_forward per trajectory (align = 1, all atoms),
+ * and grad[f] is d rmsd[f] / d coords[f] (the reference's gradient with an
+ * upstream gradient of 1).
+ *
+ * wmd_batched_prepare validates the descriptors (device memory; coords 16-byte
+ * aligned; a trajectory with n_frames == 0 is skipped, one with n_atoms == 0
+ * gets RMSD 0), sizes the context's workspace, uploads the trajectory table
+ * and picks the tile shape by timing the batch once per candidate -- it runs
+ * the batch, so the coordinates must be valid, and it synchronizes.
+ * wmd_batched_rmsd then takes the same descriptors (checked bytewise; anything
+ * else is WMD_ERR_INVALID_ARG) and only enqueues kernels on `stream`: no
+ * allocation and no host synchronization, so it can be captured in a CUDA
+ * graph.  with_grad on wmd_batched_rmsd needs with_grad on the prepare. */
 int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, int n_traj, int with_grad);
 int wmd_batched_rmsd(wmd_ctx* ctx, const wmd_batch_desc* descs, int n_traj, int with_grad, void* stream);
 

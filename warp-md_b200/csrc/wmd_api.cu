@@ -17,11 +17,13 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "../../include/warpmd_rmsd.h"
+#include "batched.h"
 #include "pairwise.h"
 #include "wmd_internal.h"
 
@@ -79,6 +81,12 @@ struct wmd_ctx {
   HostBuf stage[2];
   std::string err;
   wmd::PairwiseWorkspace pw;
+  // batched launch prepared by wmd_batched_prepare
+  DevBuf b_segs, b_yc, b_partial, b_stats, b_rot, b_refine, b_count;
+  std::vector<wmd_batch_desc> b_descs;
+  bool b_grad = false;
+  bool b_ready = false;
+  wmd::BatchPlan b_plan;
 };
 
 namespace {
@@ -391,7 +399,8 @@ WMD_EXPORT int wmd_destroy(wmd_ctx* ctx) {
   DeviceGuard g(ctx->device);
   cudaDeviceSynchronize();
   for (DevBuf* b : {&ctx->partial, &ctx->refine, &ctx->refine_count, &ctx->rot, &ctx->chunk[0], &ctx->chunk[1], &ctx->out_tmp,
-                    &ctx->sel_buf, &ctx->aux})
+                    &ctx->sel_buf, &ctx->aux, &ctx->b_segs, &ctx->b_yc, &ctx->b_partial, &ctx->b_stats, &ctx->b_rot,
+                    &ctx->b_refine, &ctx->b_count})
     if (b->ptr) cudaFree(b->ptr);
   for (HostBuf* b : {&ctx->stage[0], &ctx->stage[1]})
     if (b->ptr) cudaFreeHost(b->ptr);
@@ -679,14 +688,151 @@ WMD_EXPORT int wmd_pairwise_rmsd(wmd_ctx* ctx, const float* coords, int64_t n_fr
   return WMD_OK;
 }
 
+// Builds the device trajectory table for a tile shape; returns total items.
+static int64_t build_segs(const std::vector<wmd_batch_desc>& d, int apt, double* yc_base,
+                          std::vector<wmd::BatchSeg>& segs, int64_t* total_frames) {
+  const int tile = wmd::batched_tile_atoms(apt);
+  segs.assign(d.size(), wmd::BatchSeg{});
+  int64_t items = 0, frames = 0, yoff = 0;
+  for (size_t i = 0; i < d.size(); ++i) {
+    wmd::BatchSeg& g = segs[i];
+    g.coords = d[i].coords;
+    g.ref = d[i].ref;
+    g.rmsd = d[i].rmsd;
+    g.grad = d[i].grad;
+    g.n_atoms = d[i].n_atoms;
+    g.n_frames = d[i].n_frames;
+    g.n_tiles = (int)((d[i].n_atoms + tile - 1) / tile);
+    g.yc = yc_base + yoff;
+    yoff += (d[i].n_atoms * 3 + 1) / 2 * 2;  // keep each block 16-byte aligned
+    g.item0 = items;
+    g.frame0 = frames;
+    items += (int64_t)g.n_tiles * g.n_frames;
+    frames += g.n_frames;
+  }
+  *total_frames = frames;
+  return items;
+}
+
 WMD_EXPORT int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, int n_traj, int with_grad) {
   if (!ctx) return WMD_ERR_INVALID_ARG;
-  (void)descs; (void)n_traj; (void)with_grad;
-  return set_err(ctx, WMD_ERR_UNSUPPORTED, "batched launch not built yet");
+  if (n_traj < 0 || (n_traj > 0 && !descs)) return set_err(ctx, WMD_ERR_INVALID_ARG, "invalid batch");
+  DeviceGuard g(ctx->device);
+  int rc = check_status(ctx);
+  if (rc) return rc;
+  ctx->b_ready = false;
+  std::vector<wmd_batch_desc> d(descs, descs + n_traj);
+  int64_t sum_atoms = 0;
+  for (int i = 0; i < n_traj; ++i) {
+    wmd_batch_desc& x = d[i];
+    if (x.n_atoms < 0 || x.n_frames < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "trajectory %d: negative size", i);
+    if (x.n_frames == 0) {
+      x.n_atoms = 0;  // nothing to read or write
+      continue;
+    }
+    if (!x.rmsd || classify(x.rmsd) != Mem::Device)
+      return set_err(ctx, WMD_ERR_INVALID_ARG, "trajectory %d: rmsd must be device memory", i);
+    if (x.n_atoms == 0) continue;  // RMSD 0 per frame, like an empty selection
+    if (!x.coords || !x.ref) return set_err(ctx, WMD_ERR_INVALID_ARG, "trajectory %d: coords and ref are required", i);
+    if (classify(x.coords) != Mem::Device || classify(x.ref) != Mem::Device ||
+        (x.grad && classify(x.grad) != Mem::Device))
+      return set_err(ctx, WMD_ERR_INVALID_ARG, "trajectory %d: batched buffers must be device memory", i);
+    if (reinterpret_cast<uintptr_t>(x.coords) & 15u)
+      return set_err(ctx, WMD_ERR_INVALID_ARG, "trajectory %d: coords must be 16-byte aligned", i);
+    if (!with_grad) x.grad = nullptr;
+    sum_atoms += (x.n_atoms * 3 + 1) / 2 * 2;
+  }
+  int64_t frames4 = 0, frames8 = 0;
+  std::vector<wmd::BatchSeg> s4, s8;
+  if ((rc = ensure(ctx, ctx->b_yc, (size_t)std::max<int64_t>(sum_atoms, 2) * sizeof(double)))) return rc;
+  double* yc = static_cast<double*>(ctx->b_yc.ptr);
+  const int64_t items4 = build_segs(d, 4, yc, s4, &frames4);
+  const int64_t items8 = build_segs(d, 8, yc, s8, &frames8);
+  const int64_t frames = frames4;
+  const size_t rec = wmd::kStatDoubles * sizeof(double);
+  if ((rc = ensure(ctx, ctx->b_segs, std::max<size_t>(1, (size_t)n_traj) * sizeof(wmd::BatchSeg))) ||
+      (rc = ensure(ctx, ctx->b_partial, (size_t)std::max<int64_t>(1, std::max(items4, items8)) * rec)) ||
+      (rc = ensure(ctx, ctx->b_refine, (size_t)std::max<int64_t>(1, frames) * rec)) ||
+      (rc = ensure(ctx, ctx->b_count, sizeof(unsigned), true)))
+    return rc;
+  if (with_grad) {
+    if ((rc = ensure(ctx, ctx->b_stats, (size_t)std::max<int64_t>(1, frames) * rec)) ||
+        (rc = ensure(ctx, ctx->b_rot, (size_t)std::max<int64_t>(1, frames) * rec)))
+      return rc;
+  }
+  wmd::BatchPlan P;
+  P.n_segs = n_traj;
+  P.segs_dev = static_cast<wmd::BatchSeg*>(ctx->b_segs.ptr);
+  P.launch.segs = P.segs_dev;
+  P.launch.n_segs = n_traj;
+  P.launch.total_frames = frames;
+  P.launch.partial = static_cast<double*>(ctx->b_partial.ptr);
+  P.launch.stats = with_grad ? static_cast<double*>(ctx->b_stats.ptr) : nullptr;
+  P.launch.rot = with_grad ? static_cast<double*>(ctx->b_rot.ptr) : nullptr;
+  P.launch.refine = static_cast<double*>(ctx->b_refine.ptr);
+  P.launch.refine_count = static_cast<unsigned*>(ctx->b_count.ptr);
+  P.launch.status = ctx->status_dev;
+  // autotune the tile shape: time the whole pipeline once per candidate
+  float best_ms = -1.f;
+  int best_apt = 8;
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0), "event");
+  CU(cudaEventCreate(&e1), "event");
+  // WARPMD_BATCHED_TILE_ATOMS=512|1024 pins the tile shape instead of timing both
+  std::vector<int> cands = {8, 4};
+  if (const char* env = std::getenv("WARPMD_BATCHED_TILE_ATOMS")) {
+    if (std::strcmp(env, "512") == 0) cands = {4};
+    else if (std::strcmp(env, "1024") == 0) cands = {8};
+  }
+  if (n_traj > 0 && cands.size() == 1) best_apt = cands[0];
+  if (n_traj > 0 && cands.size() > 1) {
+    for (int apt : cands) {
+      std::vector<wmd::BatchSeg>& sv = apt == 4 ? s4 : s8;
+      CU(cudaMemcpy(P.segs_dev, sv.data(), sv.size() * sizeof(wmd::BatchSeg), cudaMemcpyHostToDevice), "upload");
+      P.apt = apt;
+      P.launch.total_items = apt == 4 ? items4 : items8;
+      P.grid_fwd = wmd::batched_grid(apt, false, ctx->sm_count, P.launch.total_items);
+      P.grid_bwd = wmd::batched_grid(apt, true, ctx->sm_count, P.launch.total_items);
+      CU(wmd::batched_enqueue(P, with_grad != 0, 0), "batched warm-up");
+      CU(cudaEventRecord(e0, 0), "event");
+      CU(wmd::batched_enqueue(P, with_grad != 0, 0), "batched tuning run");
+      CU(cudaEventRecord(e1, 0), "event");
+      CU(cudaEventSynchronize(e1), "synchronize");
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (best_ms < 0.f || ms < best_ms) {
+        best_ms = ms;
+        best_apt = apt;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::vector<wmd::BatchSeg>& sv = best_apt == 4 ? s4 : s8;
+  if (n_traj > 0)
+    CU(cudaMemcpy(P.segs_dev, sv.data(), sv.size() * sizeof(wmd::BatchSeg), cudaMemcpyHostToDevice), "upload");
+  P.apt = best_apt;
+  P.launch.total_items = best_apt == 4 ? items4 : items8;
+  P.grid_fwd = wmd::batched_grid(best_apt, false, ctx->sm_count, P.launch.total_items);
+  P.grid_bwd = wmd::batched_grid(best_apt, true, ctx->sm_count, P.launch.total_items);
+  if ((rc = check_status(ctx))) return rc;
+  ctx->b_plan = P;
+  ctx->b_descs.assign(descs, descs + n_traj);
+  ctx->b_grad = with_grad != 0;
+  ctx->b_ready = true;
+  return WMD_OK;
 }
 
 WMD_EXPORT int wmd_batched_rmsd(wmd_ctx* ctx, const wmd_batch_desc* descs, int n_traj, int with_grad, void* stream) {
   if (!ctx) return WMD_ERR_INVALID_ARG;
-  (void)descs; (void)n_traj; (void)with_grad; (void)stream;
-  return set_err(ctx, WMD_ERR_UNSUPPORTED, "batched launch not built yet");
+  DeviceGuard g(ctx->device);
+  int rc = check_status(ctx);
+  if (rc) return rc;
+  if (!ctx->b_ready || n_traj != (int)ctx->b_descs.size() || (with_grad && !ctx->b_grad) ||
+      (n_traj > 0 && std::memcmp(descs, ctx->b_descs.data(), sizeof(wmd_batch_desc) * (size_t)n_traj) != 0))
+    return set_err(ctx, WMD_ERR_INVALID_ARG,
+                   "wmd_batched_rmsd needs the same descriptors wmd_batched_prepare was called with");
+  if (n_traj == 0) return WMD_OK;
+  CU(wmd::batched_enqueue(ctx->b_plan, with_grad != 0, static_cast<cudaStream_t>(stream)), "batched launch");
+  return WMD_OK;
 }
