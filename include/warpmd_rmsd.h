@@ -154,6 +154,8 @@ typedef struct wmd_batch_desc {
  * graph.  with_grad on wmd_batched_rmsd needs with_grad on the prepare. */
 int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, int n_traj, int with_grad);
 int wmd_batched_rmsd(wmd_ctx* ctx, const wmd_batch_desc* descs, int n_traj, int with_grad, void* stream);
+/* Atoms per tile of the prepared batch (512 or 1024; 0 when none is prepared). */
+int wmd_batched_tile_atoms(const wmd_ctx* ctx);
 
 /* Per-frame aligned RMSD for callers that cannot allocate memory.  No
  * counterpart in the reference.  Everything else in this header needs a

@@ -836,3 +836,8 @@ WMD_EXPORT int wmd_batched_rmsd(wmd_ctx* ctx, const wmd_batch_desc* descs, int n
   CU(wmd::batched_enqueue(ctx->b_plan, with_grad != 0, static_cast<cudaStream_t>(stream)), "batched launch");
   return WMD_OK;
 }
+
+WMD_EXPORT int wmd_batched_tile_atoms(const wmd_ctx* ctx) {
+  if (!ctx || !ctx->b_ready) return 0;
+  return wmd::batched_tile_atoms(ctx->b_plan.apt);
+}

@@ -85,5 +85,9 @@ class BatchedRmsd:
             self.run(s)
         return g
 
+    def tile_atoms(self) -> int:
+        """Atoms per work tile the prepare step chose (512 or 1024)."""
+        return int(self.ctx.lib.wmd_batched_tile_atoms(self.ctx.handle))
+
     def close(self) -> None:
         self.ctx.close()
