@@ -143,10 +143,11 @@ typedef struct wmd_batch_desc {
  * and grad[f] is d rmsd[f] / d coords[f] (the reference's gradient with an
  * upstream gradient of 1).
  *
- * wmd_batched_prepare validates the descriptors (device memory; coords 16-byte
- * aligned; a trajectory with n_frames == 0 is skipped, one with n_atoms == 0
+ * wmd_batched_prepare validates the descriptors (device memory; coords and grad
+ * 16-byte aligned; a trajectory with n_frames == 0 is skipped, one with n_atoms == 0
  * gets RMSD 0), sizes the context's workspace, uploads the trajectory table
- * and picks the tile shape by timing the batch once per candidate -- it runs
+ * and picks the layout and tile shape by timing the batch once per candidate
+ * (frame-major or tile-major, 512- or 1024-atom tiles) -- it runs
  * the batch, so the coordinates must be valid, and it synchronizes.
  * wmd_batched_rmsd then takes the same descriptors (checked bytewise; anything
  * else is WMD_ERR_INVALID_ARG) and only enqueues kernels on `stream`: no
@@ -154,8 +155,12 @@ typedef struct wmd_batch_desc {
  * graph.  with_grad on wmd_batched_rmsd needs with_grad on the prepare. */
 int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, int n_traj, int with_grad);
 int wmd_batched_rmsd(wmd_ctx* ctx, const wmd_batch_desc* descs, int n_traj, int with_grad, void* stream);
-/* Atoms per tile of the prepared batch (512 or 1024; 0 when none is prepared). */
-int wmd_batched_tile_atoms(const wmd_ctx* ctx);
+/* Layout the prepare step chose: atoms per tile (512 or 1024) and whether the
+ * launch is frame-major (1: each CTA owns whole frames, QCP in-kernel, the
+ * gradient pass re-reads the frame from L2) or tile-major (0: tiles of all
+ * frames spread over CTAs, separate finishing kernels).  Either pointer may be
+ * NULL.  WMD_ERR_INVALID_ARG when no batch is prepared. */
+int wmd_batched_layout(const wmd_ctx* ctx, int* tile_atoms, int* frame_major);
 
 /* Per-frame aligned RMSD for callers that cannot allocate memory.  No
  * counterpart in the reference.  Everything else in this header needs a

@@ -5,8 +5,9 @@ single-trajectory entry points.
 The reference has no batched form; each trajectory's values must be what its
 own RmsdPlan gives (plan.rs:164-418), so the pins are the oracle's FP64 RMSD
 (|d| <= 1e-5 A, the per-frame bar) and its analytic gradient
-(|g - g64| <= 1e-5 max|g| + 1e-7).  Both tile shapes (512 and 1024 atoms) are
-forced once each, and the timed choice is run too.
+(|g - g64| <= 1e-5 max|g| + 1e-7).  Both layouts (tile-major, frame-major)
+and both tile shapes (512 and 1024 atoms) are forced once each, and the
+autotuner's own choice is run too.
 """
 import os
 
@@ -41,21 +42,27 @@ def _batch(shapes, seed, near_zero=()):
     return xs, ys
 
 
-def _run(xs, ys, with_grad, tile=None):
+def _run(xs, ys, with_grad, tile=None, layout=None):
     from warp_md.batched import BatchedRmsd
 
-    old = os.environ.get("WARPMD_BATCHED_TILE_ATOMS")
-    if tile is not None:
-        os.environ["WARPMD_BATCHED_TILE_ATOMS"] = str(tile)
+    pins = {"WARPMD_BATCHED_TILE_ATOMS": None if tile is None else str(tile), "WARPMD_BATCHED_LAYOUT": layout}
+    old = {k: os.environ.get(k) for k in pins}
+    for k, v in pins.items():
+        if v is not None:
+            os.environ[k] = v
     try:
         b = BatchedRmsd([torch.from_numpy(x).cuda() for x in xs], [torch.from_numpy(y).cuda() for y in ys],
                         with_grad=with_grad)
     finally:
-        if tile is not None:
-            if old is None:
-                del os.environ["WARPMD_BATCHED_TILE_ATOMS"]
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
             else:
-                os.environ["WARPMD_BATCHED_TILE_ATOMS"] = old
+                os.environ[k] = v
+    if tile is not None:
+        assert b.layout()["tile_atoms"] == tile
+    if layout is not None:
+        assert b.layout()["frame_major"] == (layout == "frames")
     for r in b.rmsd:
         r.fill_(-1.0)
     b.run()
@@ -88,18 +95,21 @@ def _check_grad(b, xs, ys):
         assert err <= tol, (k, x.shape, err, tol)
 
 
-@pytest.mark.parametrize("tile", [512, 1024, None])
-def test_batched_forward_matches_oracle(tile):
+LAYOUTS = [(512, "tiles"), (1024, "tiles"), (512, "frames"), (1024, "frames"), (None, None)]
+
+
+@pytest.mark.parametrize("tile,layout", LAYOUTS)
+def test_batched_forward_matches_oracle(tile, layout):
     xs, ys = _batch(SHAPES, 11)
-    b = _run(xs, ys, with_grad=False, tile=tile)
+    b = _run(xs, ys, with_grad=False, tile=tile, layout=layout)
     _check_rmsd(b, xs, ys)
     b.close()
 
 
-@pytest.mark.parametrize("tile", [512, 1024])
-def test_batched_gradients_match_oracle(tile):
+@pytest.mark.parametrize("tile,layout", LAYOUTS)
+def test_batched_gradients_match_oracle(tile, layout):
     xs, ys = _batch(SHAPES, 23)
-    b = _run(xs, ys, with_grad=True, tile=tile)
+    b = _run(xs, ys, with_grad=True, tile=tile, layout=layout)
     _check_rmsd(b, xs, ys)
     _check_grad(b, xs, ys)
     b.close()
@@ -107,12 +117,16 @@ def test_batched_gradients_match_oracle(tile):
 
 def test_batched_equals_single_trajectory_path():
     """Each trajectory's values equal torch_ops.rmsd (wmd_rmsd_forward /
-    wmd_rmsd_backward) on it alone: same statistics, same QCP, so the two
-    differ only by the order of the reference sums (<= 1e-9 A here)."""
+    wmd_rmsd_backward) on it alone: the same FP64 statistics and QCP, so the
+    two differ only by summation order (<= 1e-9 A here)."""
+    xs, ys = _batch([(300, 8), (4100, 5), (1024, 9), (77, 30)], 31)
+    for layout in ("tiles", "frames"):
+        _compare_single(_run(xs, ys, with_grad=True, layout=layout), xs, ys)
+
+
+def _compare_single(b, xs, ys):
     from warp_md.torch_ops import rmsd
 
-    xs, ys = _batch([(300, 8), (4100, 5), (1024, 9), (77, 30)], 31)
-    b = _run(xs, ys, with_grad=True)
     for k, (x, y) in enumerate(zip(xs, ys)):
         xt = torch.from_numpy(x).cuda().requires_grad_(True)
         v = rmsd(xt, torch.from_numpy(y).cuda())
@@ -138,11 +152,14 @@ def test_batched_near_zero_rmsd_takes_residual_pass():
                           [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
                           [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
             xs[k][f] = (ys[k].astype(np.float64) @ R.T + rng.normal(0, 5, 3)).astype(np.float32)
-    b = _run(xs, ys, with_grad=False)
-    _check_rmsd(b, xs, ys)
-    for r in b.rmsd:
-        assert r.max().item() < 1e-3
-    b.close()
+    for layout in ("tiles", "frames"):
+        b = _run(xs, ys, with_grad=True, layout=layout)
+        _check_rmsd(b, xs, ys)
+        for r in b.rmsd:
+            assert r.max().item() < 1e-3
+        for g in b.grads:
+            assert torch.isfinite(g).all()
+        b.close()
 
 
 def test_batched_graph_replay_follows_inputs():
@@ -212,7 +229,8 @@ def test_batched_many_uneven_trajectories():
     rng = np.random.default_rng(3)
     shapes = [(int(np.exp(rng.uniform(np.log(50), np.log(6000)))), int(rng.integers(5, 60))) for _ in range(96)]
     xs, ys = _batch(shapes, 1000)
-    b = _run(xs, ys, with_grad=True)
-    _check_rmsd(b, xs, ys)
-    _check_grad(b, xs, ys)
-    b.close()
+    for layout in ("tiles", "frames"):
+        b = _run(xs, ys, with_grad=True, layout=layout)
+        _check_rmsd(b, xs, ys)
+        _check_grad(b, xs, ys)
+        b.close()

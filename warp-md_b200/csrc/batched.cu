@@ -114,7 +114,7 @@ __device__ __forceinline__ void batched_issue(const BatchSeg& s, int t, int64_t 
 }
 
 template <int APT, int MODE>
-__global__ void __launch_bounds__(kThreads, 3) batched_stream_kernel(const BatchLaunch B) {
+__global__ void __launch_bounds__(kThreads, 4) batched_stream_kernel(const BatchLaunch B) {
   using G = BGeo<APT>;
   constexpr int T = G::kTile;
   constexpr int S = G::kStages;
@@ -150,7 +150,9 @@ __global__ void __launch_bounds__(kThreads, 3) batched_stream_kernel(const Batch
   int s = 0;
   uint32_t phase = 0;
   for (int64_t i = 0; i < n_items; ++i) {
-    if (tid == 0 && issued < n_items) {
+    // forward: refill at the top of the iteration; backward: after the
+    // stage's gradient store has been issued (see below)
+    if (MODE == kBFwd && tid == 0 && issued < n_items) {
       const int sp = (int)(issued % S);
       batched_issue<APT>(B.segs[pc.seg], pc.t, pc.f, smem + sp * G::kStageBytes, &full[sp]);
       ++issued;
@@ -178,30 +180,62 @@ __global__ void __launch_bounds__(kThreads, 3) batched_stream_kernel(const Batch
                       (int)(((uint64_t)(c.f * sg.n_atoms + a0) * 3) & 3ull);
     const int64_t gitem = w0 + i;
     if (MODE == kBBwd) {
-      if (ok) {
+      // dRMSD/dx is written over x in the stage (each thread its own atoms),
+      // then leaves by one bulk store of the tile's 16-byte-aligned middle and
+      // at most 2 x 3 scalar floats at its ends.
+      float* gs = const_cast<float*>(xs);
+      const bool has_grad = sg.grad != nullptr;
+      if (ok && has_grad) {
         const double* rt = B.rot + (sg.frame0 + c.f) * kStatDoubles;
         double R[9], cc[3];
 #pragma unroll
         for (int e = 0; e < 9; ++e) R[e] = rt[e];
         cc[0] = rt[9]; cc[1] = rt[10]; cc[2] = rt[11];
-        const double scale = sg.grad ? rt[12] : 0.0;
-        float* gframe = sg.grad ? sg.grad + (size_t)c.f * sg.n_atoms * 3 : nullptr;
+        const double scale = rt[12];
 #pragma unroll
         for (int j = 0; j < APT; ++j) {
           const int k = tid + j * kConsumerThreads;
-          if (gframe && k < len) {
-            const float x0 = xs[k * 3 + 0], x1 = xs[k * 3 + 1], x2 = xs[k * 3 + 2];
+          if (k < len) {
+            const float x0 = gs[k * 3 + 0], x1 = gs[k * 3 + 1], x2 = gs[k * 3 + 2];
             const double ty0 = R[0] * yr[j][0] + R[3] * yr[j][1] + R[6] * yr[j][2];
             const double ty1 = R[1] * yr[j][0] + R[4] * yr[j][1] + R[7] * yr[j][2];
             const double ty2 = R[2] * yr[j][0] + R[5] * yr[j][1] + R[8] * yr[j][2];
-            float* g = gframe + (size_t)(a0 + k) * 3;
-            g[0] = (float)(scale * (((double)x0 - cc[0]) - ty0));
-            g[1] = (float)(scale * (((double)x1 - cc[1]) - ty1));
-            g[2] = (float)(scale * (((double)x2 - cc[2]) - ty2));
+            gs[k * 3 + 0] = (float)(scale * (((double)x0 - cc[0]) - ty0));
+            gs[k * 3 + 1] = (float)(scale * (((double)x1 - cc[1]) - ty1));
+            gs[k * 3 + 2] = (float)(scale * (((double)x2 - cc[2]) - ty2));
           }
         }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       }
       named_barrier_sync(1, kConsumerThreads);
+      // byte range of this item in the gradient array and its aligned middle
+      const uint64_t b0 = (uint64_t)(c.f * sg.n_atoms + a0) * 12ull;
+      const uint64_t b1 = b0 + (uint64_t)len * 12ull;
+      const uint64_t m0 = (b0 + 15ull) & ~15ull, m1 = b1 & ~15ull;
+      const bool mid = m1 > m0;
+      unsigned char* gbase = reinterpret_cast<unsigned char*>(sg.grad);
+      const unsigned char* sbase = reinterpret_cast<const unsigned char*>(gs) - (b0 & 15ull);  // holds byte b0 & ~15
+      if (tid == 0) {
+        if (ok && has_grad && !*abort_flag && mid) {
+          bulk_copy_s2g(gbase + m0, sbase + (m0 - (b0 & ~15ull)), (uint32_t)(m1 - m0));
+        }
+        bulk_commit();
+        // the stage read by the previous item's store is refilled next
+        bulk_wait_read<1>();
+        if (issued < n_items) {
+          const int sp = (int)(issued % S);
+          batched_issue<APT>(B.segs[pc.seg], pc.t, pc.f, smem + sp * G::kStageBytes, &full[sp]);
+          ++issued;
+          cursor_next(B, pc);
+        }
+      } else if (ok && has_grad && tid >= 32 && tid < 38) {
+        // ends outside the aligned middle: [b0, m0) and [m1, b1), or all of [b0, b1)
+        const int q = tid - 32;  // 0..2 head, 3..5 tail
+        const uint64_t at = mid ? (q < 3 ? b0 + 4ull * q : m1 + 4ull * (q - 3)) : b0 + 4ull * q;
+        const uint64_t lim = mid ? (q < 3 ? m0 : b1) : b1;
+        if (at < lim)
+          *reinterpret_cast<float*>(gbase + at) = *reinterpret_cast<const float*>(sbase + (at - (b0 & ~15ull)));
+      }
     } else {
       double acc[16];
 #pragma unroll
@@ -235,6 +269,7 @@ __global__ void __launch_bounds__(kThreads, 3) batched_stream_kernel(const Batch
     cursor_next(B, c);
   }
   if (tid == 0) {
+    if (MODE == kBBwd) bulk_wait_all<0>();
     const int64_t first = issued > S ? issued - S : 0;
     for (int64_t j = first; j < issued; ++j) {
       const int st = (int)(j % S);
@@ -277,12 +312,18 @@ __global__ void __launch_bounds__(256) batched_ref_prep(BatchSeg* segs) {
     a = bc[0]; b = bc[1]; c = bc[2];
     __syncthreads();
   };
-  if (n == 0 || s.n_frames == 0) return;
+  if (n == 0) {
+    // empty selection: RMSD 0 for every frame
+    for (int64_t f = tid; f < s.n_frames; f += blockDim.x) s.rmsd[f] = 0.0;
+    return;
+  }
+  if (s.n_frames == 0) return;
   double m0 = 0, m1 = 0, m2 = 0;
   for (int64_t k = tid; k < n; k += blockDim.x) { m0 += ref[k * 3]; m1 += ref[k * 3 + 1]; m2 += ref[k * 3 + 2]; }
   sum3(m0, m1, m2);
   const double inv = 1.0 / (double)n;
   m0 *= inv; m1 *= inv; m2 *= inv;
+  if (tid == 0) { s.mean_y[0] = m0; s.mean_y[1] = m1; s.mean_y[2] = m2; }
   double c0 = 0, c1 = 0, c2 = 0;
   for (int64_t k = tid; k < n; k += blockDim.x) {
     const double a = (double)ref[k * 3] - m0, b = (double)ref[k * 3 + 1] - m1, c = (double)ref[k * 3 + 2] - m2;
@@ -302,27 +343,41 @@ __global__ void __launch_bounds__(256) batched_ref_prep(BatchSeg* segs) {
   }
 }
 
-// One warp per frame of the batch: partials in tile order, QCP, outputs.
+// Frames of the batch, a lane each: the warp first sums the tile partials of
+// its 32 frames in tile order (two frames at a time, 16 lanes per frame, into
+// shared memory), then every lane runs QCP for its own frame -- the FP64
+// Newton iteration and, with gradients, the rotation from the eigenvector --
+// so the warp issues each instruction once for 32 frames.
 __global__ void __launch_bounds__(256) batched_finalize(const BatchLaunch B) {
-  const int64_t g = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+  __shared__ double st[8][32][17];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t base = ((int64_t)blockIdx.x * 8 + warp) * 32;
+  if (base >= B.total_frames) return;
+  for (int i = 0; i < 16; ++i) {
+    const int fl = 2 * i + (lane >> 4);
+    const int64_t g = base + fl;
+    double v = 0.0;
+    if (g < B.total_frames) {
+      const BatchSeg& sg = B.segs[seg_of(B.segs, B.n_segs, g, true)];
+      const int64_t f = g - sg.frame0;
+      for (int t = 0; t < sg.n_tiles; ++t)
+        v += B.partial[(size_t)(sg.item0 + (int64_t)t * sg.n_frames + f) * kStatDoubles + (lane & 15)];
+    }
+    st[warp][fl][lane & 15] = v;
+  }
+  __syncwarp();
+  const int64_t g = base + lane;
   if (g >= B.total_frames) return;
-  const int lane = threadIdx.x & 31;
   const BatchSeg& sg = B.segs[seg_of(B.segs, B.n_segs, g, true)];
   const int64_t f = g - sg.frame0;
-  double s = 0.0;
-  if (lane < 16)
-    for (int t = 0; t < sg.n_tiles; ++t) s += B.partial[(size_t)(sg.item0 + (int64_t)t * sg.n_frames + f) * kStatDoubles + lane];
-  double tot[16];
-#pragma unroll
-  for (int e = 0; e < 16; ++e) tot[e] = __shfl_sync(0xffffffffu, s, e);
-  if (lane != 0) return;
   if (sg.n_atoms == 0) {
     // empty selection: RMSD 0, no rotation (the single-trajectory path writes the same)
     sg.rmsd[f] = 0.0;
-    if (B.stats)
-      for (int e = 0; e < 16; ++e) B.stats[g * kStatDoubles + e] = 0.0;
+    if (B.rot)
+      for (int e = 0; e < 16; ++e) B.rot[g * kStatDoubles + e] = 0.0;
     return;
   }
+  const double* tot = st[warp][lane];
   const double n = (double)sg.n_atoms, inv_n = 1.0 / n;
   const double sx[3] = {tot[0], tot[1], tot[2]};
   double h[9];
@@ -332,11 +387,14 @@ __global__ void __launch_bounds__(256) batched_finalize(const BatchLaunch B) {
   const QcpOut q = qcp_lambda(h, 0.5 * (gx + sg.gy));
   const double rmsd = sqrt(msd_from(gx, sg.gy, q.lambda, n));
   sg.rmsd[f] = rmsd;
-  if (B.stats) {
-    double* st = B.stats + g * kStatDoubles;
-    st[0] = sx[0] * inv_n; st[1] = sx[1] * inv_n; st[2] = sx[2] * inv_n;
-    for (int e = 0; e < 9; ++e) st[3 + e] = h[e];
-    st[12] = q.lambda; st[13] = rmsd; st[14] = n; st[15] = gx + sg.gy;
+  if (B.rot) {
+    // per frame: R from the QCP eigenvector, centroid, 1 / (n rmsd)
+    double r[9];
+    rotation_from_qcp(h, q.lambda, r);
+    double* o = B.rot + g * kStatDoubles;
+    for (int e = 0; e < 9; ++e) o[e] = r[e];
+    o[9] = sx[0] * inv_n; o[10] = sx[1] * inv_n; o[11] = sx[2] * inv_n;
+    o[12] = rmsd > 0.0 ? 1.0 / (n * rmsd) : 0.0;
   }
   if (rmsd < kRefineScale * (gx + sg.gy) * inv_n) {
     const unsigned slot = atomicAdd(B.refine_count, 1u);
@@ -386,25 +444,407 @@ __global__ void __launch_bounds__(256) batched_refine(const BatchLaunch B) {
       for (int w = 0; w < 8; ++w) t += red[w];
       const double rmsd = sqrt(t * inv_n);
       sg.rmsd[f] = rmsd;
-      if (B.stats) B.stats[g * kStatDoubles + 13] = rmsd;
+      if (B.rot) B.rot[g * kStatDoubles + 12] = rmsd > 0.0 ? 1.0 / ((double)sg.n_atoms * rmsd) : 0.0;
     }
     __syncthreads();
   }
 }
 
-// Per frame: R from the QCP eigenvector, centroid, 1 / (n rmsd).
-__global__ void batched_bwd_prologue(const BatchLaunch B) {
-  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= B.total_frames) return;
-  const double* st = B.stats + g * kStatDoubles;
-  double h[9], r[9];
-  for (int e = 0; e < 9; ++e) h[e] = st[3 + e];
-  rotation_from_qcp(h, st[12], r);
-  const double rmsd = st[13], n = st[14];
-  double* o = B.rot + g * kStatDoubles;
-  for (int e = 0; e < 9; ++e) o[e] = r[e];
-  o[9] = st[0]; o[10] = st[1]; o[11] = st[2];
-  o[12] = (rmsd > 0.0 && n > 0.0) ? 1.0 / (n * rmsd) : 0.0;
+// ---------------------------------------------------------------------------
+// Frame-major fused kernel.  Frames are taken in groups: up to kGroupFrames
+// consecutive frames of one trajectory holding at most kGroupBytes of
+// coordinates (one frame when a frame is larger).  Each persistent CTA owns a
+// contiguous run of groups of equal estimated cost.  Per group:
+//   pass 1  the frames' 1-D chunks stream through the shared-memory ring; each
+//           thread keeps its 15 FP64 sums of the current frame (sum x, sum x^2,
+//           sum x y^T with the raw float reference y) in registers across the
+//           frame's chunks; one reduction per frame;
+//   finish  warp 0 runs QCP, the rotation and the near-zero residual check for
+//           all frames of the group at once, one lane per frame (the residual
+//           pass, when needed, re-reads the frame with plain loads);
+//   pass 2  (gradients) the group's chunks stream again -- from L2, since the
+//           group was read a few microseconds earlier -- and dRMSD/dx =
+//           (x - xbar - R^T (y - ybar)) / (n RMSD) is written over x in the
+//           stage and leaves by one bulk store per chunk.
+// HBM traffic is 12 B per atom-frame read + 12 B written.  H = sum x y^T -
+// (sum x) ybar^T loses nothing that matters in FP64: every product of two
+// floats is exact and the correction is one rounding of a sum.
+
+constexpr int kFrameConsts = 24;
+
+template <int APT>
+struct FGeo {
+  using G = BGeo<APT>;
+  static constexpr int kStatsOffset = G::kAbortOffset + 16;                         // [kGroupFrames][16]
+  static constexpr int kConstOffset = kStatsOffset + kGroupFrames * 16 * 8;          // [kGroupFrames][24]
+  static constexpr int kSmemBytes = kConstOffset + kGroupFrames * kFrameConsts * 8;
+};
+
+// global group whose start cost is the first at or after X
+__device__ __forceinline__ int64_t group_at(const BatchLaunch& B, int64_t X) {
+  int lo = 0, hi = B.n_segs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (B.segs[mid].cost0 <= X) lo = mid;
+    else hi = mid - 1;
+  }
+  const BatchSeg& s = B.segs[lo];
+  if (s.n_groups == 0) return s.group0;
+  const int64_t gi = (X - s.cost0 + s.group_cost - 1) / s.group_cost;
+  return s.group0 + (gi < s.n_groups ? gi : s.n_groups);
+}
+
+struct GroupCursor {
+  int seg;
+  int64_t gi;  // group index within the segment
+  int pass;
+  int j;       // frame within the group
+  int t;       // chunk within the frame
+};
+
+__device__ __forceinline__ void group_seek(const BatchLaunch& B, int64_t grp, GroupCursor& c) {
+  c.seg = 0;
+  int lo = 0, hi = B.n_segs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (B.segs[mid].group0 <= grp) lo = mid;
+    else hi = mid - 1;
+  }
+  c.seg = lo;
+  c.gi = grp - B.segs[lo].group0;
+  c.pass = 0;
+  c.j = 0;
+  c.t = 0;
+}
+
+__device__ __forceinline__ int group_count(const BatchSeg& s, int64_t gi) {
+  const int64_t f0 = gi * s.m_group;
+  const int64_t left = s.n_frames - f0;
+  return (int)(left < s.m_group ? left : s.m_group);
+}
+
+template <int T, bool GRAD>
+__device__ __forceinline__ void group_next_item(const BatchLaunch& B, GroupCursor& c) {
+  const BatchSeg& s = B.segs[c.seg];
+  const int nc = (int)((s.n_atoms + T - 1) / T);
+  if (++c.t < nc) return;
+  c.t = 0;
+  if (++c.j < group_count(s, c.gi)) return;
+  c.j = 0;
+  if (GRAD && c.pass == 0 && s.grad != nullptr) {
+    c.pass = 1;
+    return;
+  }
+  c.pass = 0;
+  if (++c.gi < s.n_groups) return;
+  c.gi = 0;
+  do {
+    ++c.seg;
+  } while (c.seg < B.n_segs && B.segs[c.seg].n_groups == 0);
+}
+
+// One lane: statistics -> RMSD, rotation and gradient constants.
+// consts: [0..8] R (R (x - xbar) ~ y - ybar), [9..11] xbar - R^T ybar,
+// [12] 1/(n rmsd), [13] rmsd, [14] residual pass needed, [16..18] xbar.
+__device__ __noinline__ void frame_finish(const double* tot, const BatchSeg& sg, double* consts) {
+  const double n = (double)sg.n_atoms, inv_n = 1.0 / n;
+  const double sx[3] = {tot[0], tot[1], tot[2]};
+  double h[9];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) h[a * 3 + b] = tot[6 + a * 3 + b] - sx[a] * sg.mean_y[b];
+  const double gx = tot[3] + tot[4] + tot[5] - (sx[0] * sx[0] + sx[1] * sx[1] + sx[2] * sx[2]) * inv_n;
+  const QcpOut q = qcp_lambda(h, 0.5 * (gx + sg.gy));
+  const double rmsd = sqrt(msd_from(gx, sg.gy, q.lambda, n));
+  double r[9];
+  rotation_from_qcp(h, q.lambda, r);
+  const double xb[3] = {sx[0] * inv_n, sx[1] * inv_n, sx[2] * inv_n};
+  for (int e = 0; e < 9; ++e) consts[e] = r[e];
+  for (int i = 0; i < 3; ++i)
+    consts[9 + i] = xb[i] - (r[0 * 3 + i] * sg.mean_y[0] + r[1 * 3 + i] * sg.mean_y[1] + r[2 * 3 + i] * sg.mean_y[2]);
+  consts[12] = rmsd > 0.0 ? 1.0 / (n * rmsd) : 0.0;
+  consts[13] = rmsd;
+  consts[14] = rmsd < kRefineScale * (gx + sg.gy) * inv_n ? 1.0 : 0.0;
+  consts[16] = xb[0]; consts[17] = xb[1]; consts[18] = xb[2];
+}
+
+template <int APT, bool GRAD>
+__global__ void __launch_bounds__(kThreads, 4) batched_frame_kernel(const BatchLaunch B) {
+  using G = BGeo<APT>;
+  using FG = FGeo<APT>;
+  constexpr int T = G::kTile;
+  constexpr int S = G::kStages;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + G::kBarOffset);
+  double* red = reinterpret_cast<double*>(smem + G::kRedOffset);   // [2][4 warps][16]
+  double* stats = reinterpret_cast<double*>(smem + FG::kStatsOffset);
+  double* consts = reinterpret_cast<double*>(smem + FG::kConstOffset);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + G::kAbortOffset);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int64_t TC = B.total_cost;
+  const int64_t G0 = blockIdx.x == 0 ? 0 : group_at(B, TC * (int64_t)blockIdx.x / gridDim.x);
+  const int64_t G1 = blockIdx.x + 1 == gridDim.x ? B.total_groups
+                                                 : group_at(B, TC * (int64_t)(blockIdx.x + 1) / gridDim.x);
+  if (tid == 0) {
+    for (int st = 0; st < S; ++st) mbar_init(&full[st], 1);
+    *abort_flag = 0;
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (G1 <= G0) return;
+
+  // producer (thread 0): walks the (group, pass, frame, chunk) items of [G0, G1)
+  GroupCursor pc{0, 0, 0, 0, 0};
+  int64_t issued = 0;
+  auto producer_live = [&]() { return pc.seg < B.n_segs && B.segs[pc.seg].group0 + pc.gi < G1; };
+  auto issue = [&]() {
+    const int sp = (int)(issued % S);
+    const BatchSeg& ps = B.segs[pc.seg];
+    batched_issue<APT>(ps, pc.t, pc.gi * ps.m_group + pc.j, smem + sp * G::kStageBytes, &full[sp]);
+    ++issued;
+    group_next_item<T, GRAD>(B, pc);
+  };
+  if (tid == 0) {
+    group_seek(B, G0, pc);
+    while (issued < S - 1 && producer_live()) issue();
+  }
+  // end of every item: all consumers are done with the previous item's stage
+  // and its gradient store (if any) has been read out, so it is refilled
+  auto item_end = [&]() {
+    if (tid == 0) {
+      bulk_commit();
+      bulk_wait_read<1>();
+      if (producer_live()) issue();
+    }
+  };
+
+  GroupCursor cc;
+  group_seek(B, G0, cc);
+  int s = 0;
+  uint32_t phase = 0;
+  int cache_seg = -1, cache_t = -1, pre_seg = -1, pre_t = -1;
+  double yr[APT][3];
+  float yn[APT][3];  // next chunk of the reference, loaded one item ahead
+  bool stop = false;
+  for (int64_t grp = G0; grp < G1 && !stop; ++grp) {
+    while (cc.gi >= B.segs[cc.seg].n_groups) {  // segments without groups are never current
+      cc.gi = 0;
+      ++cc.seg;
+    }
+    const BatchSeg& sg = B.segs[cc.seg];
+    const int64_t n = sg.n_atoms;
+    const int nc = (int)((n + T - 1) / T);
+    const int64_t f0 = cc.gi * sg.m_group;
+    const int cnt = group_count(sg, cc.gi);
+    auto fetch = [&](int t, float (&dst)[APT][3]) {
+      const int64_t a0 = (int64_t)t * T;
+      const int len = (int)(min(n, a0 + T) - a0);
+#pragma unroll
+      for (int j = 0; j < APT; ++j) {
+        const int k = tid + j * kConsumerThreads;
+        if (k < len) {
+          const float* y = sg.ref + (a0 + k) * 3;
+          dst[j][0] = __ldg(y); dst[j][1] = __ldg(y + 1); dst[j][2] = __ldg(y + 2);
+        } else {
+          dst[j][0] = dst[j][1] = dst[j][2] = 0.f;
+        }
+      }
+    };
+    // reference chunk t into yr; for frames of several chunks the next
+    // chunk's loads are issued now and land while this item is processed
+    auto load_ref = [&](int t) {
+      if (cc.seg != cache_seg || t != cache_t) {
+        if (!(cc.seg == pre_seg && t == pre_t)) fetch(t, yn);
+#pragma unroll
+        for (int j = 0; j < APT; ++j) {
+          yr[j][0] = (double)yn[j][0]; yr[j][1] = (double)yn[j][1]; yr[j][2] = (double)yn[j][2];
+        }
+        cache_seg = cc.seg;
+        cache_t = t;
+      }
+      if (nc > 1) {
+        const int tn = t + 1 < nc ? t + 1 : 0;
+        fetch(tn, yn);
+        pre_seg = cc.seg;
+        pre_t = tn;
+      }
+    };
+    // ---- pass 1: statistics, one reduction per frame ----
+    for (int j = 0; j < cnt && !stop; ++j) {
+      const int64_t f = f0 + j;
+      double acc[16];
+#pragma unroll
+      for (int e = 0; e < 16; ++e) acc[e] = 0.0;
+      for (int t = 0; t < nc; ++t) {
+        load_ref(t);
+        const int64_t a0 = (int64_t)t * T;
+        const int len = (int)(min(n, a0 + T) - a0);
+        const bool ok = mbar_wait(&full[s], phase, B.status, kStatusTimeoutFull, abort_flag);
+        const float* xs = reinterpret_cast<const float*>(smem + s * G::kStageBytes) +
+                          (int)(((uint64_t)(f * n + a0) * 3) & 3ull);
+#pragma unroll
+        for (int q = 0; q < APT; ++q) {
+          const int k = tid + q * kConsumerThreads;
+          const bool in = ok && k < len;
+          const double x0 = in ? (double)xs[k * 3 + 0] : 0.0;
+          const double x1 = in ? (double)xs[k * 3 + 1] : 0.0;
+          const double x2 = in ? (double)xs[k * 3 + 2] : 0.0;
+          acc[0] += x0; acc[1] += x1; acc[2] += x2;
+          acc[3] = fma(x0, x0, acc[3]); acc[4] = fma(x1, x1, acc[4]); acc[5] = fma(x2, x2, acc[5]);
+          acc[6] = fma(x0, yr[q][0], acc[6]);  acc[7] = fma(x0, yr[q][1], acc[7]);  acc[8] = fma(x0, yr[q][2], acc[8]);
+          acc[9] = fma(x1, yr[q][0], acc[9]);  acc[10] = fma(x1, yr[q][1], acc[10]); acc[11] = fma(x1, yr[q][2], acc[11]);
+          acc[12] = fma(x2, yr[q][0], acc[12]); acc[13] = fma(x2, yr[q][1], acc[13]); acc[14] = fma(x2, yr[q][2], acc[14]);
+        }
+        double* rb = red + (j & 1) * (kConsumerWarps * 16);
+        if (t == nc - 1) {
+          const double v = warp_reduce_scatter16(acc);
+          if ((lane & 1) == 0) rb[warp * 16 + (lane >> 1)] = v;
+        }
+        named_barrier_sync(1, kConsumerThreads);
+        if (t == nc - 1 && tid < 16)
+          stats[j * 16 + tid] = rb[tid] + rb[16 + tid] + rb[32 + tid] + rb[48 + tid];
+        item_end();
+        if (++s == S) { s = 0; phase ^= 1u; }
+        if (*abort_flag) { stop = true; break; }
+      }
+    }
+    if (stop) break;
+    // ---- finish: QCP for the whole group, one lane per frame ----
+    named_barrier_sync(1, kConsumerThreads);
+    if (warp == 0 && lane < cnt) {
+      double* cj = consts + lane * kFrameConsts;
+      frame_finish(stats + lane * 16, sg, cj);
+      if (cj[14] == 0.0) sg.rmsd[f0 + lane] = cj[13];
+    }
+    named_barrier_sync(1, kConsumerThreads);
+    for (int j = 0; j < cnt; ++j) {
+      double* cj = consts + j * kFrameConsts;
+      if (cj[14] == 0.0) continue;
+      // near-zero RMSD: explicit residual |R (x - xbar) - (y - ybar)|^2 in FP64
+      double R[9];
+#pragma unroll
+      for (int e = 0; e < 9; ++e) R[e] = cj[e];
+      const double xb0 = cj[16], xb1 = cj[17], xb2 = cj[18];
+      const double yb0 = sg.mean_y[0], yb1 = sg.mean_y[1], yb2 = sg.mean_y[2];
+      const float* frame = sg.coords + (size_t)(f0 + j) * n * 3;
+      double r2 = 0.0;
+      for (int64_t k = tid; k < n; k += kConsumerThreads) {
+        const double d0 = (double)frame[k * 3] - xb0, d1 = (double)frame[k * 3 + 1] - xb1,
+                     d2 = (double)frame[k * 3 + 2] - xb2;
+        const double e0 = R[0] * d0 + R[1] * d1 + R[2] * d2 - ((double)sg.ref[k * 3] - yb0);
+        const double e1 = R[3] * d0 + R[4] * d1 + R[5] * d2 - ((double)sg.ref[k * 3 + 1] - yb1);
+        const double e2 = R[6] * d0 + R[7] * d1 + R[8] * d2 - ((double)sg.ref[k * 3 + 2] - yb2);
+        r2 += e0 * e0 + e1 * e1 + e2 * e2;
+      }
+      for (int o = 16; o; o >>= 1) r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+      if (lane == 0) red[warp] = r2;
+      named_barrier_sync(1, kConsumerThreads);
+      if (tid == 0) {
+        const double rmsd = sqrt((red[0] + red[1] + red[2] + red[3]) / (double)n);
+        cj[13] = rmsd;
+        cj[12] = rmsd > 0.0 ? 1.0 / ((double)n * rmsd) : 0.0;
+        cj[14] = 0.0;
+        sg.rmsd[f0 + j] = rmsd;
+      }
+      named_barrier_sync(1, kConsumerThreads);
+    }
+    // ---- pass 2: gradients ----
+    if (GRAD && sg.grad != nullptr) {
+      unsigned char* gbase = reinterpret_cast<unsigned char*>(sg.grad);
+      for (int j = 0; j < cnt && !stop; ++j) {
+        const int64_t f = f0 + j;
+        const double* cj = consts + j * kFrameConsts;
+        double R[9], dd[3];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) R[e] = cj[e];
+        dd[0] = cj[9]; dd[1] = cj[10]; dd[2] = cj[11];
+        const double scale = cj[12];
+        for (int t = 0; t < nc; ++t) {
+          load_ref(t);
+          const int64_t a0 = (int64_t)t * T;
+          const int len = (int)(min(n, a0 + T) - a0);
+          const bool ok = mbar_wait(&full[s], phase, B.status, kStatusTimeoutFull, abort_flag);
+          float* gs = reinterpret_cast<float*>(smem + s * G::kStageBytes) + (int)(((uint64_t)(f * n + a0) * 3) & 3ull);
+          if (ok) {
+#pragma unroll
+            for (int q = 0; q < APT; ++q) {
+              const int k = tid + q * kConsumerThreads;
+              if (k < len) {
+                const double x0 = gs[k * 3 + 0], x1 = gs[k * 3 + 1], x2 = gs[k * 3 + 2];
+                const double ty0 = R[0] * yr[q][0] + R[3] * yr[q][1] + R[6] * yr[q][2];
+                const double ty1 = R[1] * yr[q][0] + R[4] * yr[q][1] + R[7] * yr[q][2];
+                const double ty2 = R[2] * yr[q][0] + R[5] * yr[q][1] + R[8] * yr[q][2];
+                gs[k * 3 + 0] = (float)(scale * ((x0 - ty0) - dd[0]));
+                gs[k * 3 + 1] = (float)(scale * ((x1 - ty1) - dd[1]));
+                gs[k * 3 + 2] = (float)(scale * ((x2 - ty2) - dd[2]));
+              }
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          }
+          named_barrier_sync(1, kConsumerThreads);
+          const uint64_t b0 = (uint64_t)(f * n + a0) * 12ull;
+          const uint64_t b1 = b0 + (uint64_t)len * 12ull;
+          const uint64_t m0 = (b0 + 15ull) & ~15ull, m1 = b1 & ~15ull;
+          const bool mid = m1 > m0;
+          const unsigned char* sbase = reinterpret_cast<const unsigned char*>(gs) - (b0 & 15ull);
+          if (tid == 0) {
+            if (ok && !*abort_flag && mid)
+              bulk_copy_s2g(gbase + m0, sbase + (m0 - (b0 & ~15ull)), (uint32_t)(m1 - m0));
+          } else if (ok && tid >= 32 && tid < 38) {
+            const int q = tid - 32;
+            const uint64_t at = mid ? (q < 3 ? b0 + 4ull * q : m1 + 4ull * (q - 3)) : b0 + 4ull * q;
+            const uint64_t lim = mid ? (q < 3 ? m0 : b1) : b1;
+            if (at < lim)
+              *reinterpret_cast<float*>(gbase + at) = *reinterpret_cast<const float*>(sbase + (at - (b0 & ~15ull)));
+          }
+          item_end();
+          if (++s == S) { s = 0; phase ^= 1u; }
+          if (*abort_flag) { stop = true; break; }
+        }
+      }
+    }
+    ++cc.gi;
+  }
+  if (tid == 0) {
+    bulk_wait_all<0>();
+    const int64_t first = issued > S ? issued - S : 0;
+    for (int64_t j = first; j < issued; ++j) {
+      const int st = (int)(j % S);
+      const uint32_t ph = (uint32_t)((j / S) & 1);
+      const uint64_t t0 = global_timer_ns();
+      while (!mbar_try_wait(&full[st], ph)) {
+        if (global_timer_ns() - t0 > kWaitLimitNs) {
+          atomicOr(B.status, kStatusTimeoutDrain);
+          break;
+        }
+      }
+    }
+  }
+}
+
+template <int APT, bool GRAD>
+cudaError_t launch_frames(const BatchLaunch& B, int grid, cudaStream_t s) {
+  auto kern = batched_frame_kernel<APT, GRAD>;
+  static bool attr_done[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!attr_done[dev]) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, FGeo<APT>::kSmemBytes);
+    if (e != cudaSuccess) return e;
+    attr_done[dev] = true;
+  }
+  kern<<<grid, kThreads, FGeo<APT>::kSmemBytes, s>>>(B);
+  return cudaGetLastError();
+}
+
+template <int APT, bool GRAD>
+int frame_occupancy() {
+  auto kern = batched_frame_kernel<APT, GRAD>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, FGeo<APT>::kSmemBytes);
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, kThreads, FGeo<APT>::kSmemBytes) != cudaSuccess)
+    blocks = 1;
+  return blocks < 1 ? 1 : blocks;
 }
 
 template <int APT, int MODE>
@@ -442,23 +882,25 @@ cudaError_t batched_enqueue(const BatchPlan& P, bool with_grad, cudaStream_t s) 
   cudaError_t e;
   batched_ref_prep<<<P.n_segs, 256, 0, s>>>(P.segs_dev);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (P.variant == kBatchFrames) {
+    if (B.total_groups == 0) return cudaSuccess;
+    if (P.apt == 4)
+      return with_grad ? launch_frames<4, true>(B, P.grid_fwd, s) : launch_frames<4, false>(B, P.grid_fwd, s);
+    return with_grad ? launch_frames<8, true>(B, P.grid_fwd, s) : launch_frames<8, false>(B, P.grid_fwd, s);
+  }
   if ((e = cudaMemsetAsync(B.refine_count, 0, sizeof(unsigned), s)) != cudaSuccess) return e;
   if (B.total_items > 0) {
     e = P.apt == 4 ? launch_stream<4, kBFwd>(B, P.grid_fwd, s) : launch_stream<8, kBFwd>(B, P.grid_fwd, s);
     if (e != cudaSuccess) return e;
   }
   if (B.total_frames > 0) {
-    batched_finalize<<<(unsigned)((B.total_frames + 7) / 8), 256, 0, s>>>(B);
+    batched_finalize<<<(unsigned)((B.total_frames + 255) / 256), 256, 0, s>>>(B);
     batched_refine<<<(unsigned)std::min<int64_t>(B.total_frames, 148), 256, 0, s>>>(B);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
-  if (with_grad && B.total_frames > 0) {
-    batched_bwd_prologue<<<(unsigned)((B.total_frames + 127) / 128), 128, 0, s>>>(B);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (B.total_items > 0) {
-      e = P.apt == 4 ? launch_stream<4, kBBwd>(B, P.grid_bwd, s) : launch_stream<8, kBBwd>(B, P.grid_bwd, s);
-      if (e != cudaSuccess) return e;
-    }
+  if (with_grad && B.total_items > 0) {
+    e = P.apt == 4 ? launch_stream<4, kBBwd>(B, P.grid_bwd, s) : launch_stream<8, kBBwd>(B, P.grid_bwd, s);
+    if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
@@ -467,6 +909,12 @@ int batched_grid(int apt, bool backward, int sm_count, int64_t items) {
   const int occ = apt == 4 ? (backward ? occupancy_of<4, kBBwd>() : occupancy_of<4, kBFwd>())
                            : (backward ? occupancy_of<8, kBBwd>() : occupancy_of<8, kBFwd>());
   return (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)sm_count * occ));
+}
+
+int batched_frame_grid(int apt, bool with_grad, int sm_count, int64_t groups) {
+  const int occ = apt == 4 ? (with_grad ? frame_occupancy<4, true>() : frame_occupancy<4, false>())
+                           : (with_grad ? frame_occupancy<8, true>() : frame_occupancy<8, false>());
+  return (int)std::max<int64_t>(1, std::min<int64_t>(groups, (int64_t)sm_count * occ));
 }
 
 }  // namespace wmd

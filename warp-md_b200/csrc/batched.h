@@ -18,10 +18,15 @@ struct BatchSeg {
   int64_t n_frames;
   int64_t item0;        // first global work item (items: n_tiles x n_frames)
   int64_t frame0;       // first global frame
+  int64_t group0;       // frame-major layout: first global frame group
+  int64_t n_groups;     //   groups of this trajectory (m_group frames each, the last may be short)
+  int64_t cost0;        //   estimated cost of all groups before this trajectory's
+  int64_t group_cost;   //   estimated cost of one full group
   int n_tiles;
-  int pad;
+  int m_group;          //   frames per group
   double sum_c[3];      // sum of y_c, written on the device each call
   double gy;            // G_y, written on the device each call
+  double mean_y[3];     // mean of the reference, written on the device each call
 };
 
 struct BatchLaunch {
@@ -29,9 +34,10 @@ struct BatchLaunch {
   int n_segs = 0;
   int64_t total_items = 0;
   int64_t total_frames = 0;
+  int64_t total_groups = 0;          // frame-major layout
+  int64_t total_cost = 0;
   double* partial = nullptr;         // [total_items][16]
-  double* stats = nullptr;           // [total_frames][16] (with gradients)
-  double* rot = nullptr;             // [total_frames][16] (with gradients)
+  double* rot = nullptr;             // [total_frames][16] (with gradients): R, xbar, 1/(n rmsd)
   double* refine = nullptr;          // [total_frames][16]
   unsigned* refine_count = nullptr;
   int* status = nullptr;
@@ -42,12 +48,31 @@ struct BatchPlan {
   BatchSeg* segs_dev = nullptr;
   int n_segs = 0;
   int apt = 8;       // atoms per thread: 4 (512-atom tiles) or 8 (1024-atom tiles)
+  int variant = 0;   // kBatchTiles or kBatchFrames
   int grid_fwd = 0;
   int grid_bwd = 0;
 };
 
+// Tile-major: work items (atom tile, frame) spread over persistent CTAs, frame
+// statistics finished by a second kernel, gradients by a second streaming pass
+// (36 B per atom-frame with gradients).  Frame-major: each CTA owns whole
+// frames, finishes QCP in-kernel and re-reads the frame from L2 for the
+// gradient (24 B per atom-frame from HBM).
+enum BatchVariant : int { kBatchTiles = 0, kBatchFrames = 1 };
+
+// Frame-major grouping: up to kGroupFrames consecutive frames of one
+// trajectory with at most kGroupBytes of coordinates form a group, whose QCP
+// runs on one warp, a lane per frame.  CTAs take runs of groups of equal
+// estimated cost: kCostItem per chunk streamed (each pass) + kCostFinish per
+// group (QCP and rotation, about six chunk-times of latency).
+constexpr int kGroupFrames = 16;
+constexpr int kGroupBytes = 64 * 1024;
+constexpr int64_t kCostItem = 4;
+constexpr int64_t kCostFinish = 24;
+
 int batched_tile_atoms(int apt);
 int batched_grid(int apt, bool backward, int sm_count, int64_t items);
+int batched_frame_grid(int apt, bool with_grad, int sm_count, int64_t groups);
 // Enqueues the whole batched pipeline on s (no allocation, no host sync).
 cudaError_t batched_enqueue(const BatchPlan& P, bool with_grad, cudaStream_t s);
 

@@ -264,43 +264,49 @@ WMD_HD void rotation_from_svd(const double h[9], double r[9]) {
 // Rotation from the QCP eigenvector of K(H) for eigenvalue lambda: the
 // eigenvector is a column of adj(K - lambda I); the column with the largest
 // diagonal entry is the best conditioned.  Falls back to the SVD rotation when
-// the adjugate vanishes (degenerate lambda_max).
+// the adjugate vanishes (degenerate lambda_max).  The adjugate comes from the
+// Laplace expansion over the 2x2 minors of rows {0,1} and {2,3}, written out
+// entry by entry so that everything stays in registers.
 WMD_HD void rotation_from_qcp(const double h[9], double lambda, double r[9]) {
   double k[16];
   key_matrix(h, k);
-  for (int i = 0; i < 4; ++i) k[i * 5] -= lambda;
-  // cofactor C_ij = (-1)^(i+j) det(minor_ij)
-  double best = -1.0;
+  k[0] -= lambda; k[5] -= lambda; k[10] -= lambda; k[15] -= lambda;
+  // 2x2 minors of the top rows (s) and bottom rows (c), column pairs
+  // (01, 02, 03, 12, 13, 23)
+  const double s01 = k[0] * k[5] - k[4] * k[1], s02 = k[0] * k[6] - k[4] * k[2], s03 = k[0] * k[7] - k[4] * k[3];
+  const double s12 = k[1] * k[6] - k[5] * k[2], s13 = k[1] * k[7] - k[5] * k[3], s23 = k[2] * k[7] - k[6] * k[3];
+  const double c01 = k[8] * k[13] - k[12] * k[9], c02 = k[8] * k[14] - k[12] * k[10];
+  const double c03 = k[8] * k[15] - k[12] * k[11], c12 = k[9] * k[14] - k[13] * k[10];
+  const double c13 = k[9] * k[15] - k[13] * k[11], c23 = k[10] * k[15] - k[14] * k[11];
+  // adjugate a[i][j] = cofactor C_ji
+  const double a00 = k[5] * c23 - k[6] * c13 + k[7] * c12;
+  const double a01 = -k[1] * c23 + k[2] * c13 - k[3] * c12;
+  const double a02 = k[13] * s23 - k[14] * s13 + k[15] * s12;
+  const double a03 = -k[9] * s23 + k[10] * s13 - k[11] * s12;
+  const double a10 = -k[4] * c23 + k[6] * c03 - k[7] * c02;
+  const double a11 = k[0] * c23 - k[2] * c03 + k[3] * c02;
+  const double a12 = -k[12] * s23 + k[14] * s03 - k[15] * s02;
+  const double a13 = k[8] * s23 - k[10] * s03 + k[11] * s02;
+  const double a20 = k[4] * c13 - k[5] * c03 + k[7] * c01;
+  const double a21 = -k[0] * c13 + k[1] * c03 - k[3] * c01;
+  const double a22 = k[12] * s13 - k[13] * s03 + k[15] * s01;
+  const double a23 = -k[8] * s13 + k[9] * s03 - k[11] * s01;
+  const double a30 = -k[4] * c12 + k[5] * c02 - k[6] * c01;
+  const double a31 = k[0] * c12 - k[1] * c02 + k[2] * c01;
+  const double a32 = -k[12] * s12 + k[13] * s02 - k[14] * s01;
+  const double a33 = k[8] * s12 - k[9] * s02 + k[10] * s01;
+  // column m of the adjugate, m = argmax |a_mm|
   int m = 0;
-  double diag[4];
-  for (int i = 0; i < 4; ++i) {
-    int r0 = i == 0 ? 1 : 0, r1 = i <= 1 ? 2 : 1, r2 = i <= 2 ? 3 : 2;
-    const double mm[9] = {k[r0 * 4 + r0], k[r0 * 4 + r1], k[r0 * 4 + r2],
-                          k[r1 * 4 + r0], k[r1 * 4 + r1], k[r1 * 4 + r2],
-                          k[r2 * 4 + r0], k[r2 * 4 + r1], k[r2 * 4 + r2]};
-    diag[i] = det3(mm);
-    if (fabs(diag[i]) > best) { best = fabs(diag[i]); m = i; }
-  }
+  double best = fabs(a00);
+  if (fabs(a11) > best) { best = fabs(a11); m = 1; }
+  if (fabs(a22) > best) { best = fabs(a22); m = 2; }
+  if (fabs(a33) > best) { best = fabs(a33); m = 3; }
   double q[4];
-  double norm2 = 0.0;
-  for (int j = 0; j < 4; ++j) {
-    if (j == m) {
-      q[j] = diag[m];
-    } else {
-      // cofactor C_mj: delete row m and column j
-      int rows[3], cols[3], nr = 0, nc = 0;
-      for (int t = 0; t < 4; ++t) {
-        if (t != m) rows[nr++] = t;
-        if (t != j) cols[nc++] = t;
-      }
-      double mm[9];
-      for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) mm[a * 3 + b] = k[rows[a] * 4 + cols[b]];
-      const double sgn = ((m + j) & 1) ? -1.0 : 1.0;
-      q[j] = sgn * det3(mm);
-    }
-    norm2 += q[j] * q[j];
-  }
+  q[0] = m == 0 ? a00 : m == 1 ? a01 : m == 2 ? a02 : a03;
+  q[1] = m == 0 ? a10 : m == 1 ? a11 : m == 2 ? a12 : a13;
+  q[2] = m == 0 ? a20 : m == 1 ? a21 : m == 2 ? a22 : a23;
+  q[3] = m == 0 ? a30 : m == 1 ? a31 : m == 2 ? a32 : a33;
+  const double norm2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
   // scale-free degeneracy test: |adj column|^2 vs (|K|_F^3)^2
   double kf = 0.0;
   for (int i = 0; i < 16; ++i) kf += k[i] * k[i];

@@ -82,7 +82,7 @@ struct wmd_ctx {
   std::string err;
   wmd::PairwiseWorkspace pw;
   // batched launch prepared by wmd_batched_prepare
-  DevBuf b_segs, b_yc, b_partial, b_stats, b_rot, b_refine, b_count;
+  DevBuf b_segs, b_yc, b_partial, b_rot, b_refine, b_count;
   std::vector<wmd_batch_desc> b_descs;
   bool b_grad = false;
   bool b_ready = false;
@@ -399,7 +399,7 @@ WMD_EXPORT int wmd_destroy(wmd_ctx* ctx) {
   DeviceGuard g(ctx->device);
   cudaDeviceSynchronize();
   for (DevBuf* b : {&ctx->partial, &ctx->refine, &ctx->refine_count, &ctx->rot, &ctx->chunk[0], &ctx->chunk[1], &ctx->out_tmp,
-                    &ctx->sel_buf, &ctx->aux, &ctx->b_segs, &ctx->b_yc, &ctx->b_partial, &ctx->b_stats, &ctx->b_rot,
+                    &ctx->sel_buf, &ctx->aux, &ctx->b_segs, &ctx->b_yc, &ctx->b_partial, &ctx->b_rot,
                     &ctx->b_refine, &ctx->b_count})
     if (b->ptr) cudaFree(b->ptr);
   for (HostBuf* b : {&ctx->stage[0], &ctx->stage[1]})
@@ -688,12 +688,14 @@ WMD_EXPORT int wmd_pairwise_rmsd(wmd_ctx* ctx, const float* coords, int64_t n_fr
   return WMD_OK;
 }
 
-// Builds the device trajectory table for a tile shape; returns total items.
-static int64_t build_segs(const std::vector<wmd_batch_desc>& d, int apt, double* yc_base,
-                          std::vector<wmd::BatchSeg>& segs, int64_t* total_frames) {
+// Builds the device trajectory table for a tile shape; returns total items
+// (tile-major layout) and fills the frame-group partition (frame-major).
+static int64_t build_segs(const std::vector<wmd_batch_desc>& d, int apt, double* yc_base, bool with_grad,
+                          std::vector<wmd::BatchSeg>& segs, int64_t* total_frames, int64_t* total_groups,
+                          int64_t* total_cost) {
   const int tile = wmd::batched_tile_atoms(apt);
   segs.assign(d.size(), wmd::BatchSeg{});
-  int64_t items = 0, frames = 0, yoff = 0;
+  int64_t items = 0, frames = 0, yoff = 0, groups = 0, cost = 0;
   for (size_t i = 0; i < d.size(); ++i) {
     wmd::BatchSeg& g = segs[i];
     g.coords = d[i].coords;
@@ -709,8 +711,28 @@ static int64_t build_segs(const std::vector<wmd_batch_desc>& d, int apt, double*
     g.frame0 = frames;
     items += (int64_t)g.n_tiles * g.n_frames;
     frames += g.n_frames;
+    // frame groups
+    g.group0 = groups;
+    g.cost0 = cost;
+    if (g.n_atoms > 0 && g.n_frames > 0) {
+      const int64_t fb = g.n_atoms * 12;
+      g.m_group = (int)std::max<int64_t>(1, std::min<int64_t>(wmd::kGroupFrames, wmd::kGroupBytes / fb));
+      g.n_groups = (g.n_frames + g.m_group - 1) / g.m_group;
+      const int64_t passes = (with_grad && g.grad) ? 2 : 1;
+      const int64_t frame_cost = (int64_t)g.n_tiles * passes * wmd::kCostItem;
+      g.group_cost = g.m_group * frame_cost + wmd::kCostFinish;
+      const int64_t last = g.n_frames - (g.n_groups - 1) * g.m_group;
+      groups += g.n_groups;
+      cost += (g.n_groups - 1) * g.group_cost + last * frame_cost + wmd::kCostFinish;
+    } else {
+      g.m_group = 1;
+      g.n_groups = 0;
+      g.group_cost = 1;
+    }
   }
   *total_frames = frames;
+  *total_groups = groups;
+  *total_cost = cost;
   return items;
 }
 
@@ -739,6 +761,8 @@ WMD_EXPORT int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, in
       return set_err(ctx, WMD_ERR_INVALID_ARG, "trajectory %d: batched buffers must be device memory", i);
     if (reinterpret_cast<uintptr_t>(x.coords) & 15u)
       return set_err(ctx, WMD_ERR_INVALID_ARG, "trajectory %d: coords must be 16-byte aligned", i);
+    if (with_grad && (reinterpret_cast<uintptr_t>(x.grad) & 15u))
+      return set_err(ctx, WMD_ERR_INVALID_ARG, "trajectory %d: grad must be 16-byte aligned", i);
     if (!with_grad) x.grad = nullptr;
     sum_atoms += (x.n_atoms * 3 + 1) / 2 * 2;
   }
@@ -746,8 +770,9 @@ WMD_EXPORT int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, in
   std::vector<wmd::BatchSeg> s4, s8;
   if ((rc = ensure(ctx, ctx->b_yc, (size_t)std::max<int64_t>(sum_atoms, 2) * sizeof(double)))) return rc;
   double* yc = static_cast<double*>(ctx->b_yc.ptr);
-  const int64_t items4 = build_segs(d, 4, yc, s4, &frames4);
-  const int64_t items8 = build_segs(d, 8, yc, s8, &frames8);
+  int64_t groups4 = 0, groups8 = 0, cost4 = 0, cost8 = 0;
+  const int64_t items4 = build_segs(d, 4, yc, with_grad != 0, s4, &frames4, &groups4, &cost4);
+  const int64_t items8 = build_segs(d, 8, yc, with_grad != 0, s8, &frames8, &groups8, &cost8);
   const int64_t frames = frames4;
   const size_t rec = wmd::kStatDoubles * sizeof(double);
   if ((rc = ensure(ctx, ctx->b_segs, std::max<size_t>(1, (size_t)n_traj) * sizeof(wmd::BatchSeg))) ||
@@ -755,11 +780,7 @@ WMD_EXPORT int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, in
       (rc = ensure(ctx, ctx->b_refine, (size_t)std::max<int64_t>(1, frames) * rec)) ||
       (rc = ensure(ctx, ctx->b_count, sizeof(unsigned), true)))
     return rc;
-  if (with_grad) {
-    if ((rc = ensure(ctx, ctx->b_stats, (size_t)std::max<int64_t>(1, frames) * rec)) ||
-        (rc = ensure(ctx, ctx->b_rot, (size_t)std::max<int64_t>(1, frames) * rec)))
-      return rc;
-  }
+  if (with_grad && (rc = ensure(ctx, ctx->b_rot, (size_t)std::max<int64_t>(1, frames) * rec))) return rc;
   wmd::BatchPlan P;
   P.n_segs = n_traj;
   P.segs_dev = static_cast<wmd::BatchSeg*>(ctx->b_segs.ptr);
@@ -767,54 +788,67 @@ WMD_EXPORT int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, in
   P.launch.n_segs = n_traj;
   P.launch.total_frames = frames;
   P.launch.partial = static_cast<double*>(ctx->b_partial.ptr);
-  P.launch.stats = with_grad ? static_cast<double*>(ctx->b_stats.ptr) : nullptr;
   P.launch.rot = with_grad ? static_cast<double*>(ctx->b_rot.ptr) : nullptr;
   P.launch.refine = static_cast<double*>(ctx->b_refine.ptr);
   P.launch.refine_count = static_cast<unsigned*>(ctx->b_count.ptr);
   P.launch.status = ctx->status_dev;
-  // autotune the tile shape: time the whole pipeline once per candidate
-  float best_ms = -1.f;
-  int best_apt = 8;
-  cudaEvent_t e0, e1;
-  CU(cudaEventCreate(&e0), "event");
-  CU(cudaEventCreate(&e1), "event");
-  // WARPMD_BATCHED_TILE_ATOMS=512|1024 pins the tile shape instead of timing both
-  std::vector<int> cands = {8, 4};
-  if (const char* env = std::getenv("WARPMD_BATCHED_TILE_ATOMS")) {
-    if (std::strcmp(env, "512") == 0) cands = {4};
-    else if (std::strcmp(env, "1024") == 0) cands = {8};
-  }
-  if (n_traj > 0 && cands.size() == 1) best_apt = cands[0];
-  if (n_traj > 0 && cands.size() > 1) {
-    for (int apt : cands) {
-      std::vector<wmd::BatchSeg>& sv = apt == 4 ? s4 : s8;
+  // Autotuner: time the whole pipeline once per candidate layout (tile-major
+  // or frame-major) and tile shape (512 or 1024 atoms) on this batch.
+  // WARPMD_BATCHED_LAYOUT=tiles|frames and WARPMD_BATCHED_TILE_ATOMS=512|1024
+  // pin either choice.
+  auto configure = [&](int variant, int apt) -> int {
+    std::vector<wmd::BatchSeg>& sv = apt == 4 ? s4 : s8;
+    if (n_traj > 0)
       CU(cudaMemcpy(P.segs_dev, sv.data(), sv.size() * sizeof(wmd::BatchSeg), cudaMemcpyHostToDevice), "upload");
-      P.apt = apt;
-      P.launch.total_items = apt == 4 ? items4 : items8;
+    P.variant = variant;
+    P.apt = apt;
+    P.launch.total_items = apt == 4 ? items4 : items8;
+    P.launch.total_groups = apt == 4 ? groups4 : groups8;
+    P.launch.total_cost = apt == 4 ? cost4 : cost8;
+    if (variant == wmd::kBatchFrames) {
+      P.grid_fwd = wmd::batched_frame_grid(apt, with_grad != 0, ctx->sm_count, P.launch.total_groups);
+      P.grid_bwd = P.grid_fwd;
+    } else {
       P.grid_fwd = wmd::batched_grid(apt, false, ctx->sm_count, P.launch.total_items);
       P.grid_bwd = wmd::batched_grid(apt, true, ctx->sm_count, P.launch.total_items);
-      CU(wmd::batched_enqueue(P, with_grad != 0, 0), "batched warm-up");
-      CU(cudaEventRecord(e0, 0), "event");
-      CU(wmd::batched_enqueue(P, with_grad != 0, 0), "batched tuning run");
-      CU(cudaEventRecord(e1, 0), "event");
-      CU(cudaEventSynchronize(e1), "synchronize");
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      if (best_ms < 0.f || ms < best_ms) {
-        best_ms = ms;
-        best_apt = apt;
-      }
     }
+    return WMD_OK;
+  };
+  std::vector<int> apts = {8, 4}, layouts = {wmd::kBatchFrames, wmd::kBatchTiles};
+  if (const char* env = std::getenv("WARPMD_BATCHED_TILE_ATOMS")) {
+    if (std::strcmp(env, "512") == 0) apts = {4};
+    else if (std::strcmp(env, "1024") == 0) apts = {8};
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  std::vector<wmd::BatchSeg>& sv = best_apt == 4 ? s4 : s8;
-  if (n_traj > 0)
-    CU(cudaMemcpy(P.segs_dev, sv.data(), sv.size() * sizeof(wmd::BatchSeg), cudaMemcpyHostToDevice), "upload");
-  P.apt = best_apt;
-  P.launch.total_items = best_apt == 4 ? items4 : items8;
-  P.grid_fwd = wmd::batched_grid(best_apt, false, ctx->sm_count, P.launch.total_items);
-  P.grid_bwd = wmd::batched_grid(best_apt, true, ctx->sm_count, P.launch.total_items);
+  if (const char* env = std::getenv("WARPMD_BATCHED_LAYOUT")) {
+    if (std::strcmp(env, "tiles") == 0) layouts = {wmd::kBatchTiles};
+    else if (std::strcmp(env, "frames") == 0) layouts = {wmd::kBatchFrames};
+  }
+  float best_ms = -1.f;
+  int best_apt = apts[0], best_layout = layouts[0];
+  if (n_traj > 0 && apts.size() * layouts.size() > 1) {
+    cudaEvent_t e0, e1;
+    CU(cudaEventCreate(&e0), "event");
+    CU(cudaEventCreate(&e1), "event");
+    for (int layout : layouts)
+      for (int apt : apts) {
+        if ((rc = configure(layout, apt))) return rc;
+        CU(wmd::batched_enqueue(P, with_grad != 0, 0), "batched warm-up");
+        CU(cudaEventRecord(e0, 0), "event");
+        CU(wmd::batched_enqueue(P, with_grad != 0, 0), "batched tuning run");
+        CU(cudaEventRecord(e1, 0), "event");
+        CU(cudaEventSynchronize(e1), "synchronize");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (best_ms < 0.f || ms < best_ms) {
+          best_ms = ms;
+          best_apt = apt;
+          best_layout = layout;
+        }
+      }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  if ((rc = configure(best_layout, best_apt))) return rc;
   if ((rc = check_status(ctx))) return rc;
   ctx->b_plan = P;
   ctx->b_descs.assign(descs, descs + n_traj);
@@ -837,7 +871,10 @@ WMD_EXPORT int wmd_batched_rmsd(wmd_ctx* ctx, const wmd_batch_desc* descs, int n
   return WMD_OK;
 }
 
-WMD_EXPORT int wmd_batched_tile_atoms(const wmd_ctx* ctx) {
-  if (!ctx || !ctx->b_ready) return 0;
-  return wmd::batched_tile_atoms(ctx->b_plan.apt);
+WMD_EXPORT int wmd_batched_layout(const wmd_ctx* ctx, int* tile_atoms, int* frame_major) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  if (!ctx->b_ready) return set_err(const_cast<wmd_ctx*>(ctx), WMD_ERR_INVALID_ARG, "no batch is prepared");
+  if (tile_atoms) *tile_atoms = wmd::batched_tile_atoms(ctx->b_plan.apt);
+  if (frame_major) *frame_major = ctx->b_plan.variant == wmd::kBatchFrames ? 1 : 0;
+  return WMD_OK;
 }

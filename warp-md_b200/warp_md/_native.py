@@ -38,7 +38,7 @@ FRAME_STATS = 16
 EXPORTED = (
     "wmd_create", "wmd_destroy", "wmd_last_error", "wmd_version", "wmd_reference_upload", "wmd_reference_free",
     "wmd_rmsd_frames", "wmd_rmsd_forward", "wmd_rmsd_backward", "wmd_rmsd_covariance", "wmd_pairwise_rmsd",
-    "wmd_batched_prepare", "wmd_batched_rmsd", "wmd_batched_tile_atoms", "wmd_rmsd_frames_noalloc",
+    "wmd_batched_prepare", "wmd_batched_rmsd", "wmd_batched_layout", "wmd_rmsd_frames_noalloc",
 )
 
 
@@ -92,7 +92,7 @@ def load() -> ctypes.CDLL:
         L.wmd_pairwise_rmsd.argtypes = [vp, vp, i64, i64, i32, vp, i64, i32, i32, vp, vp]
         L.wmd_batched_prepare.argtypes = [vp, ctypes.POINTER(BatchDesc), i32, i32]
         L.wmd_batched_rmsd.argtypes = [vp, ctypes.POINTER(BatchDesc), i32, i32, vp]
-        L.wmd_batched_tile_atoms.argtypes = [vp]
+        L.wmd_batched_layout.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32)]
         L.wmd_rmsd_frames_noalloc.argtypes = [vp, i64, i64, i32, vp, i64, i32, vp, vp]
         for name in EXPORTED:
             getattr(L, name).restype = getattr(L, name).restype if name in ("wmd_last_error", "wmd_version") else i32

@@ -85,9 +85,11 @@ class BatchedRmsd:
             self.run(s)
         return g
 
-    def tile_atoms(self) -> int:
-        """Atoms per work tile the prepare step chose (512 or 1024)."""
-        return int(self.ctx.lib.wmd_batched_tile_atoms(self.ctx.handle))
+    def layout(self) -> dict:
+        """The layout the prepare step's autotuner chose."""
+        t, fm = ctypes.c_int(), ctypes.c_int()
+        self.ctx.check(self.ctx.lib.wmd_batched_layout(self.ctx.handle, ctypes.byref(t), ctypes.byref(fm)))
+        return {"tile_atoms": t.value, "frame_major": bool(fm.value)}
 
     def close(self) -> None:
         self.ctx.close()
