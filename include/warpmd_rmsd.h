@@ -162,6 +162,38 @@ int wmd_batched_rmsd(wmd_ctx* ctx, const wmd_batch_desc* descs, int n_traj, int 
  * NULL.  WMD_ERR_INVALID_ARG when no batch is prepared. */
 int wmd_batched_layout(const wmd_ctx* ctx, int* tile_atoms, int* frame_major);
 
+/* ---- Optimal superposition (AlignPlan, RotationMatrixPlan, SuperposePlan,
+ *      SuperposeTrajectoryPlan: crates/traj-engine/src/plans/geometry/align/
+ *      plan_exec.rs:76-523, align_matrix.rs:16-70) ---- */
+
+/* Reference with per-atom weights (the reference's `mass=True`: the masses of
+ * the selected atoms).  weights: n_sel floats, host or device, or NULL (all
+ * weights 1, the same as wmd_reference_upload).  A weighted reference serves
+ * only wmd_superpose_transforms and wmd_superpose; the RMSD entry points
+ * reject it with WMD_ERR_INVALID_ARG. */
+int wmd_reference_upload_weighted(wmd_ctx* ctx, const float* ref, int64_t n_sel, int stride, const float* weights,
+                                  wmd_ref** out);
+
+/* Per frame, the weighted Kabsch superposition of the selection onto the
+ * reference (kabsch_rotation_weighted, geometry_math.rs:235-300): R (3x3,
+ * row-major, R (x - c_x) ~ y - c_y) and t = c_y - R c_x, written as 12 floats
+ * per frame [n_frames][12] = R00..R22, t0..t2 -- AlignPlan's rows
+ * (plan_exec.rs:225-238); RotationMatrixPlan keeps the first 9.  norotate:
+ * R = I, t = c_y - c_x.  An empty selection or zero total weight gives R = I,
+ * t = 0 (centroid_weighted returns 0 then).  coords and transforms may be host
+ * or device memory; with any host pointer the call synchronizes. */
+int wmd_superpose_transforms(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                             const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, int norotate, float* transforms,
+                             void* stream);
+
+/* SuperposePlan: every atom of every frame moved by its frame's transform,
+ * out[f][a] = R_f coords[f][a] + t_f in FP64 rounded to float32, packed xyz
+ * [n_frames][n_atoms][3] (plan_exec.rs:431-444).  transforms, if not NULL,
+ * also receives the [n_frames][12] rows.  Host or device pointers as above. */
+int wmd_superpose(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                  const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, int norotate, float* out,
+                  float* transforms, void* stream);
+
 /* Per-frame aligned RMSD for callers that cannot allocate memory.  No
  * counterpart in the reference.  Everything else in this header needs a
  * wmd_ctx and a wmd_ref, which allocate device and pinned memory; this call

@@ -51,6 +51,8 @@ def lib():
         L.wmdo_svd3.restype = _int
         L.wmdo_kabsch_rotation.argtypes = [_f64p, _f64p, ctypes.POINTER(ctypes.c_double)]
         L.wmdo_kabsch_rotation.restype = None
+        L.wmdo_superpose.argtypes = [_vp, _i64, _i64, _int, _vp, _i64, _vp, _int, _vp, _int, _vp, _vp, _int]
+        L.wmdo_superpose.restype = None
         _lib = L
     return _lib
 
@@ -130,3 +132,20 @@ def kabsch_rotation(h):
     ss = ctypes.c_double()
     lib().wmdo_kabsch_rotation(h, r, ctypes.byref(ss))
     return r.reshape(3, 3), ss.value
+
+
+def superpose(coords, reference, selection=None, weights=None, norotate: bool = False, apply: bool = True,
+              threads: int = 0):
+    """AlignPlan / SuperposePlan semantics: per-frame transforms [F][12] (R
+    row-major, t; FP64) and, with apply, every atom moved (float32 [F][N][3])."""
+    c, stride = _coords(coords)
+    ref = np.ascontiguousarray(reference, dtype=np.float32)
+    sel = None if selection is None else np.ascontiguousarray(selection, dtype=np.uint32)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float32)
+    if sel is not None and sel.shape[0] != ref.shape[0]:
+        raise ValueError("selection and reference lengths differ")
+    xf = np.empty((c.shape[0], 12), np.float64)
+    out = np.empty((c.shape[0], c.shape[1], 3), np.float32) if apply else None
+    lib().wmdo_superpose(_ptr(c), c.shape[0], c.shape[1], stride, _ptr(sel), ref.shape[0], _ptr(ref), ref.shape[1],
+                         _ptr(w), int(bool(norotate)), _ptr(xf), _ptr(out), int(threads))
+    return xf, out

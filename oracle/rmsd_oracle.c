@@ -15,6 +15,10 @@
  *   - rmsd_raw                plan.rs:1081-1091   (pairwise metric "nofit")
  *   - PairwiseRmsdPlan::finalize  plan.rs:593-674 (symmetric fill, zero
  *       diagonal, n_sel < 2 -> all zeros)
+ *   - AlignPlan / SuperposePlan   crates/traj-engine/src/plans/geometry/align/
+ *       plan_exec.rs:125-266, 325-459 with kabsch_rotation_weighted and
+ *       centroid_weighted (crates/traj-engine/src/plans/geometry/
+ *       geometry_math.rs:202-300): weighted Kabsch, t = cy - R cx, R x + t.
  *
  * The SVD in the reference is nalgebra 0.32.6 (Cargo.lock:792-793), which is
  * not vendored.  Here it is a one-sided Jacobi SVD (Hestenes 1958; Demmel &
@@ -397,4 +401,78 @@ WMDO_API double wmdo_qcp_rmsd(const float* x, const float* y, int64_t n, int str
  * rotation convention): r maps frame coordinates onto the reference. */
 WMDO_API void wmdo_kabsch_rotation(const double h[9], double r[9], double* sigma_sum) {
   kabsch_rotation(h, r, sigma_sum);
+}
+
+/* ------------------------------------------------------------------ */
+/* Superposition plans (AlignPlan / SuperposePlan)                     */
+/* ------------------------------------------------------------------ */
+
+/* centroid_weighted (crates/traj-engine/src/plans/geometry/geometry_math.rs:
+ * 202-233): weighted mean, 0 when the weights sum to 0. */
+static void centroid_w(const float* pts, int stride, const uint32_t* sel, int64_t n, const float* w, double c[3]) {
+  double s[3] = {0, 0, 0}, ws = 0.0;
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t idx = sel ? (int64_t)sel[i] : i;
+    const float* p = pts + idx * stride;
+    const double wi = w ? (double)w[i] : 1.0;
+    s[0] += (double)p[0] * wi; s[1] += (double)p[1] * wi; s[2] += (double)p[2] * wi;
+    ws += wi;
+  }
+  if (!w) ws = (double)n;
+  for (int k = 0; k < 3; ++k) c[k] = ws == 0.0 ? 0.0 : s[k] / ws;
+}
+
+/* Per frame: kabsch_rotation_weighted (geometry_math.rs:235-300) of the
+ * selection onto the reference -- weighted centroids, H = sum w (x - cx)
+ * (y - cy)^T, R = V U^T with the reflection fix; norotate: R = I -- then
+ * t = cy - R cx (plan_exec.rs:224 / 415).  xf [n_frames][12] = R row-major,
+ * t.  When out is not NULL every atom of the frame is moved: out = R x + t in
+ * FP64, rounded to f32 (plan_exec.rs:431-444). */
+WMDO_API void wmdo_superpose(const float* coords, int64_t n_frames, int64_t n_atoms, int stride, const uint32_t* sel,
+                             int64_t n_sel, const float* ref, int ref_stride, const float* weights, int norotate,
+                             double* xf, float* out, int n_threads) {
+#ifdef _OPENMP
+  int nt = n_threads > 0 ? n_threads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
+#endif
+  for (int64_t f = 0; f < n_frames; ++f) {
+    const float* frame = coords + f * n_atoms * stride;
+    double r[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, cx[3] = {0, 0, 0}, cy[3] = {0, 0, 0};
+    if (n_sel > 0) {
+      centroid_w(frame, stride, sel, n_sel, weights, cx);
+      centroid_w(ref, ref_stride, NULL, n_sel, weights, cy);
+      if (!norotate) {
+        double h[9] = {0};
+        for (int64_t i = 0; i < n_sel; ++i) {
+          const int64_t idx = sel ? (int64_t)sel[i] : i;
+          const float* p = frame + idx * stride;
+          const float* q = ref + i * ref_stride;
+          const double wi = weights ? (double)weights[i] : 1.0;
+          const double px = p[0] - cx[0], py = p[1] - cx[1], pz = p[2] - cx[2];
+          const double qx = q[0] - cy[0], qy = q[1] - cy[1], qz = q[2] - cy[2];
+          h[0] += px * qx * wi; h[1] += px * qy * wi; h[2] += px * qz * wi;
+          h[3] += py * qx * wi; h[4] += py * qy * wi; h[5] += py * qz * wi;
+          h[6] += pz * qx * wi; h[7] += pz * qy * wi; h[8] += pz * qz * wi;
+        }
+        kabsch_rotation(h, r, NULL);
+      }
+    }
+    double t[3];
+    for (int i = 0; i < 3; ++i) t[i] = cy[i] - (r[i * 3] * cx[0] + r[i * 3 + 1] * cx[1] + r[i * 3 + 2] * cx[2]);
+    if (xf) {
+      memcpy(xf + f * 12, r, sizeof(r));
+      memcpy(xf + f * 12 + 9, t, sizeof(t));
+    }
+    if (out) {
+      float* o = out + f * n_atoms * 3;
+      for (int64_t a = 0; a < n_atoms; ++a) {
+        const float* p = frame + a * stride;
+        const double x = p[0], y = p[1], z = p[2];
+        o[a * 3 + 0] = (float)(r[0] * x + r[1] * y + r[2] * z + t[0]);
+        o[a * 3 + 1] = (float)(r[3] * x + r[4] * y + r[5] * z + t[1]);
+        o[a * 3 + 2] = (float)(r[6] * x + r[7] * y + r[8] * z + t[2]);
+      }
+    }
+  }
+  (void)n_threads;
 }

@@ -242,6 +242,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_stream_kernel(const Batch
       for (int e = 0; e < 16; ++e) acc[e] = 0.0;
 #pragma unroll
       for (int j = 0; j < APT; ++j) {
+        if ((warp << 5) + j * kConsumerThreads >= len) break;  // warp-uniform: the rest of the tile is empty
         const int k = tid + j * kConsumerThreads;
         const bool in = ok && k < len;
         const double x0 = in ? (double)xs[k * 3 + 0] : 0.0;

@@ -41,7 +41,7 @@
 
 namespace wmd {
 
-enum Mode : int { kFwdFit = 0, kFwdRaw = 1, kBwd = 2 };
+enum Mode : int { kFwdFit = 0, kFwdRaw = 1, kBwd = 2, kFwdW = 3 };
 
 template <int STRIDE, int APT>
 struct Geo {
@@ -207,6 +207,7 @@ __global__ void __launch_bounds__(kThreads, 3) rmsd_frames_kernel(const FrameLau
   }
 
   double yr[APT][3];
+  float wr[MODE == kFwdW ? APT : 1];
   uint32_t gidx[GATHER ? APT : 1];
   int t = (int)(w0 / F);
   int64_t f = w0 - (int64_t)t * F;
@@ -230,6 +231,7 @@ __global__ void __launch_bounds__(kThreads, 3) rmsd_frames_kernel(const FrameLau
         if (k < len) {
           const double* y = L.ref.yc + (a0 + k) * 3;
           yr[j][0] = __ldg(y + 0); yr[j][1] = __ldg(y + 1); yr[j][2] = __ldg(y + 2);
+          if (MODE == kFwdW) wr[MODE == kFwdW ? j : 0] = __ldg(L.ref.w + a0 + k);
           if (GATHER) {
             uint32_t idx = L.sel ? __ldg(L.sel + a0 + k) : (uint32_t)(a0 + k);
             if ((int64_t)idx >= L.n_atoms) {  // bad device-side selection: report, read atom 0
@@ -240,6 +242,7 @@ __global__ void __launch_bounds__(kThreads, 3) rmsd_frames_kernel(const FrameLau
           }
         } else {
           yr[j][0] = yr[j][1] = yr[j][2] = 0.0;
+          if (MODE == kFwdW) wr[MODE == kFwdW ? j : 0] = 0.f;
           if (GATHER) gidx[GATHER ? j : 0] = 0;
         }
       }
@@ -333,6 +336,21 @@ __global__ void __launch_bounds__(kThreads, 3) rmsd_frames_kernel(const FrameLau
         }
         acc[0] += acc[1] + acc[2];
         acc[1] = acc[2] = 0.0;
+      } else if (MODE == kFwdW) {
+        // weighted: sum w x, sum w x_a^2, sum x (w y_c)^T (the weight is folded
+        // into the stored reference)
+#pragma unroll
+        for (int j = 0; j < APT; ++j) {
+          float f0, f1, f2;
+          load_x(j, f0, f1, f2);
+          const double x0 = f0, x1 = f1, x2 = f2, w = wr[MODE == kFwdW ? j : 0];
+          const double u0 = w * x0, u1 = w * x1, u2 = w * x2;
+          acc[0] += u0; acc[1] += u1; acc[2] += u2;
+          acc[3] = fma(u0, x0, acc[3]); acc[4] = fma(u1, x1, acc[4]); acc[5] = fma(u2, x2, acc[5]);
+          acc[6] = fma(x0, yr[j][0], acc[6]);  acc[7] = fma(x0, yr[j][1], acc[7]);  acc[8] = fma(x0, yr[j][2], acc[8]);
+          acc[9] = fma(x1, yr[j][0], acc[9]);  acc[10] = fma(x1, yr[j][1], acc[10]); acc[11] = fma(x1, yr[j][2], acc[11]);
+          acc[12] = fma(x2, yr[j][0], acc[12]); acc[13] = fma(x2, yr[j][1], acc[13]); acc[14] = fma(x2, yr[j][2], acc[14]);
+        }
       } else {
 #pragma unroll
         for (int j = 0; j < APT; ++j) {
@@ -538,6 +556,11 @@ cudaError_t launch_rmsd_forward(const FrameLaunch& L, cudaStream_t s) {
 cudaError_t launch_rmsd_stream(const FrameLaunch& L, cudaStream_t s) {
   if (L.n_frames == 0) return cudaSuccess;
   return dispatch<kFwdFit>(L, s);
+}
+
+cudaError_t launch_rmsd_stream_weighted(const FrameLaunch& L, cudaStream_t s) {
+  if (L.n_frames == 0) return cudaSuccess;
+  return dispatch<kFwdW>(L, s);
 }
 
 cudaError_t launch_rmsd_backward(const FrameLaunch& L, const double* stats, const float* grad_rmsd,

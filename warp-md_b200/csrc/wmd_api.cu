@@ -25,6 +25,7 @@
 #include "../../include/warpmd_rmsd.h"
 #include "batched.h"
 #include "pairwise.h"
+#include "superpose.h"
 #include "wmd_internal.h"
 
 #define WMD_EXPORT extern "C" __attribute__((visibility("default")))
@@ -66,6 +67,7 @@ struct HostBuf {
 
 struct wmd_ref {
   double* yc = nullptr;
+  float* w = nullptr;  // per-atom weights (weighted references only)
   wmd::RefInfo info;
 };
 
@@ -77,7 +79,7 @@ struct wmd_ctx {
   cudaEvent_t kern_done[2] = {nullptr, nullptr};
   int* status_host = nullptr;  // mapped pinned word the kernels report into
   int* status_dev = nullptr;
-  DevBuf partial, refine, refine_count, rot, chunk[2], out_tmp, sel_buf, aux;
+  DevBuf partial, refine, refine_count, rot, chunk[2], out_tmp, sel_buf, aux, out_chunk;
   HostBuf stage[2];
   std::string err;
   wmd::PairwiseWorkspace pw;
@@ -204,6 +206,8 @@ int check_common(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_
   if (stride != 3 && stride != 4) return set_err(ctx, WMD_ERR_INVALID_ARG, "stride must be 3 or 4 (got %d)", stride);
   if (n_frames < 0 || n_atoms < 0 || n_sel < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "negative size");
   if (n_frames > 0 && !coords) return set_err(ctx, WMD_ERR_INVALID_ARG, "coords is null");
+  if (ref->info.w)
+    return set_err(ctx, WMD_ERR_INVALID_ARG, "a weighted reference serves the superposition entry points only");
   if (n_sel != ref->info.n_sel)
     return set_err(ctx, WMD_ERR_MISMATCH, "reference has %lld atoms but the selection has %lld",
                    (long long)ref->info.n_sel, (long long)n_sel);
@@ -399,7 +403,7 @@ WMD_EXPORT int wmd_destroy(wmd_ctx* ctx) {
   DeviceGuard g(ctx->device);
   cudaDeviceSynchronize();
   for (DevBuf* b : {&ctx->partial, &ctx->refine, &ctx->refine_count, &ctx->rot, &ctx->chunk[0], &ctx->chunk[1], &ctx->out_tmp,
-                    &ctx->sel_buf, &ctx->aux, &ctx->b_segs, &ctx->b_yc, &ctx->b_partial, &ctx->b_rot,
+                    &ctx->sel_buf, &ctx->aux, &ctx->out_chunk, &ctx->b_segs, &ctx->b_yc, &ctx->b_partial, &ctx->b_rot,
                     &ctx->b_refine, &ctx->b_count})
     if (b->ptr) cudaFree(b->ptr);
   for (HostBuf* b : {&ctx->stage[0], &ctx->stage[1]})
@@ -415,7 +419,8 @@ WMD_EXPORT int wmd_destroy(wmd_ctx* ctx) {
   return WMD_OK;
 }
 
-WMD_EXPORT int wmd_reference_upload(wmd_ctx* ctx, const float* ref, int64_t n_sel, int stride, wmd_ref** out) {
+static int reference_upload(wmd_ctx* ctx, const float* ref, int64_t n_sel, int stride, const float* weights,
+                            wmd_ref** out) {
   if (!ctx) return WMD_ERR_INVALID_ARG;
   if (!out) return set_err(ctx, WMD_ERR_INVALID_ARG, "out is null");
   *out = nullptr;
@@ -423,18 +428,25 @@ WMD_EXPORT int wmd_reference_upload(wmd_ctx* ctx, const float* ref, int64_t n_se
   if (n_sel < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "negative size");
   if (n_sel > 0 && !ref) return set_err(ctx, WMD_ERR_INVALID_ARG, "reference is null");
   DeviceGuard g(ctx->device);
-  std::vector<float> host;
+  std::vector<float> host, hw;
   const float* h = ref;
   if (n_sel > 0 && classify(ref) == Mem::Device) {
     host.resize((size_t)n_sel * stride);
     CU(cudaMemcpy(host.data(), ref, host.size() * sizeof(float), cudaMemcpyDeviceToHost), "download reference");
     h = host.data();
   }
+  const float* wt = weights;
+  if (weights && n_sel > 0 && classify(weights) == Mem::Device) {
+    hw.resize((size_t)n_sel);
+    CU(cudaMemcpy(hw.data(), weights, hw.size() * sizeof(float), cudaMemcpyDeviceToHost), "download weights");
+    wt = hw.data();
+  }
   wmd_ref* r = new wmd_ref();
   wmd::RefInfo& I = r->info;
   I.n_sel = n_sel;
+  I.wsum = (double)n_sel;
   std::vector<double> yc((size_t)std::max<int64_t>(n_sel, 1) * 3, 0.0);
-  if (n_sel > 0) {
+  if (n_sel > 0 && !weights) {
     // FP64 two-pass centring, as rmsd_aligned_selected does (plan.rs:1172-1190).
     // The sums run over up to ~1e5 atoms whose coordinates are far from the
     // origin, so they are compensated (Neumaier): the kernels correct H with
@@ -460,22 +472,67 @@ WMD_EXPORT int wmd_reference_upload(wmd_ctx* ctx, const float* ref, int64_t n_se
         gy.add(d * d);
       }
     I.gy = gy.value();
+  } else if (n_sel > 0) {
+    // weighted (centroid_weighted / kabsch_rotation_weighted,
+    // geometry_math.rs:202-300): mean_w = sum w y / sum w; the stored rows
+    // are w (y - mean_w), sum_c their exact sum, G_y = sum w |y - mean_w|^2
+    NeumaierSum ws, m[3];
+    for (int64_t i = 0; i < n_sel; ++i) {
+      const double w = (double)wt[i];
+      ws.add(w);
+      for (int c = 0; c < 3; ++c) m[c].add(w * (double)h[i * stride + c]);
+    }
+    I.wsum = ws.value();
+    for (int c = 0; c < 3; ++c) I.mean[c] = I.wsum != 0.0 ? m[c].value() / I.wsum : 0.0;
+    NeumaierSum sc[3], sq;
+    std::vector<double> d((size_t)n_sel * 3);
+    for (int64_t i = 0; i < n_sel; ++i)
+      for (int c = 0; c < 3; ++c) {
+        const double y = (double)h[i * stride + c];
+        d[i * 3 + c] = y - I.mean[c];
+        yc[i * 3 + c] = (double)wt[i] * d[i * 3 + c];
+        sc[c].add(yc[i * 3 + c]);
+        sq.add((double)wt[i] * y * y);
+      }
+    for (int c = 0; c < 3; ++c) I.sum_c[c] = sc[c].value();
+    I.sumsq = sq.value();
+    NeumaierSum gy;
+    for (int64_t i = 0; i < n_sel; ++i)
+      for (int c = 0; c < 3; ++c) {
+        const double e = d[i * 3 + c] - (I.wsum != 0.0 ? I.sum_c[c] / I.wsum : 0.0);
+        gy.add((double)wt[i] * e * e);
+      }
+    I.gy = gy.value();
   }
   cudaError_t e = cudaMalloc(&r->yc, yc.size() * sizeof(double));
+  if (e == cudaSuccess && weights && n_sel > 0) e = cudaMalloc(&r->w, (size_t)n_sel * sizeof(float));
   if (e != cudaSuccess) {
+    cudaFree(r->yc);
     delete r;
     cudaGetLastError();
     return set_err(ctx, WMD_ERR_OOM, "cuda driver error: reference allocation failed: %s", cudaGetErrorString(e));
   }
   e = cudaMemcpy(r->yc, yc.data(), yc.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && r->w) e = cudaMemcpy(r->w, wt, (size_t)n_sel * sizeof(float), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     cudaFree(r->yc);
+    cudaFree(r->w);
     delete r;
     return cuda_err(ctx, e, "upload reference");
   }
   I.yc = r->yc;
+  I.w = r->w;
   *out = r;
   return WMD_OK;
+}
+
+WMD_EXPORT int wmd_reference_upload(wmd_ctx* ctx, const float* ref, int64_t n_sel, int stride, wmd_ref** out) {
+  return reference_upload(ctx, ref, n_sel, stride, nullptr, out);
+}
+
+WMD_EXPORT int wmd_reference_upload_weighted(wmd_ctx* ctx, const float* ref, int64_t n_sel, int stride,
+                                             const float* weights, wmd_ref** out) {
+  return reference_upload(ctx, ref, n_sel, stride, weights, out);
 }
 
 WMD_EXPORT int wmd_reference_free(wmd_ctx* ctx, wmd_ref* ref) {
@@ -483,8 +540,10 @@ WMD_EXPORT int wmd_reference_free(wmd_ctx* ctx, wmd_ref* ref) {
   if (ctx) {
     DeviceGuard g(ctx->device);
     cudaFree(ref->yc);
+    if (ref->w) cudaFree(ref->w);
   } else {
     cudaFree(ref->yc);
+    if (ref->w) cudaFree(ref->w);
   }
   delete ref;
   return WMD_OK;
@@ -591,6 +650,138 @@ static int require_device(wmd_ctx* ctx, const void* p, const char* name) {
   if (p && classify(p) != Mem::Device)
     return set_err(ctx, WMD_ERR_INVALID_ARG, "%s must be device memory for this entry point", name);
   return WMD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// superposition (AlignPlan / RotationMatrixPlan / SuperposePlan)
+// ---------------------------------------------------------------------------
+
+// Device-resident frames: statistics, per-frame transforms into dxf32 (if not
+// null) and, when dout is not null, every atom moved into dout.
+static int superpose_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames, int64_t n_atoms, int stride,
+                            const uint32_t* dsel, const wmd_ref* ref, int norotate, float* dxf32, float* dout,
+                            cudaStream_t s) {
+  if (n_frames == 0) return WMD_OK;
+  wmd::FrameLaunch L = base_launch(ctx, ref, n_atoms, stride, dsel);
+  L.align = 1;
+  L.gather = dsel != nullptr || (reinterpret_cast<uintptr_t>(dcoords) & 15u) != 0;
+  const int tiles = wmd::frame_tiles(L);
+  const size_t per_frame = (size_t)std::max(tiles, 1) * wmd::kStatDoubles * sizeof(double);
+  const int64_t batch = std::min<int64_t>(n_frames, std::max<int64_t>(1, (int64_t)(kPartialBytesMax / per_frame)));
+  int rc;
+  if ((rc = ensure(ctx, ctx->partial, per_frame * (size_t)batch)) ||
+      (rc = ensure(ctx, ctx->rot, (size_t)batch * wmd::kStatDoubles * sizeof(double))))
+    return rc;
+  for (int64_t f0 = 0; f0 < n_frames; f0 += batch) {
+    const int64_t nf = std::min(batch, n_frames - f0);
+    wmd::FrameLaunch B = L;
+    B.coords = dcoords + (size_t)f0 * n_atoms * stride;
+    B.n_frames = nf;
+    B.partial = static_cast<double*>(ctx->partial.ptr);
+    B.grid = wmd::frame_grid(B, ctx->sm_count, false);
+    if (ref->info.n_sel > 0) {
+      if (ref->info.w) CU(wmd::launch_rmsd_stream_weighted(B, s), "superpose statistics");
+      else CU(wmd::launch_rmsd_stream(B, s), "superpose statistics");
+    }
+    double* xf = static_cast<double*>(ctx->rot.ptr);
+    CU(wmd::launch_superpose_finalize(B, norotate, xf, dxf32 ? dxf32 + f0 * 12 : nullptr, s), "superpose transforms");
+    if (dout)
+      CU(wmd::launch_superpose_apply(B.coords, nf, n_atoms, stride, xf, dout + (size_t)f0 * n_atoms * 3, ctx->sm_count,
+                                     s),
+         "superpose apply");
+  }
+  return WMD_OK;
+}
+
+static int superpose_common(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                            const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, int norotate, float* out,
+                            float* transforms, cudaStream_t s) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  if (!ref) return set_err(ctx, WMD_ERR_INVALID_ARG, "reference is null");
+  if (stride != 3 && stride != 4) return set_err(ctx, WMD_ERR_INVALID_ARG, "stride must be 3 or 4 (got %d)", stride);
+  if (n_frames < 0 || n_atoms < 0 || n_sel < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "negative size");
+  if (n_frames > 0 && !coords) return set_err(ctx, WMD_ERR_INVALID_ARG, "coords is null");
+  if (n_sel != ref->info.n_sel)
+    return set_err(ctx, WMD_ERR_MISMATCH, "reference has %lld atoms but the selection has %lld",
+                   (long long)ref->info.n_sel, (long long)n_sel);
+  if (!sel && n_sel > n_atoms)
+    return set_err(ctx, WMD_ERR_MISMATCH, "selection of %lld atoms exceeds the frame's %lld atoms", (long long)n_sel,
+                   (long long)n_atoms);
+  DeviceGuard g(ctx->device);
+  int rc = check_status(ctx);
+  if (rc) return rc;
+  if (n_frames == 0) return WMD_OK;
+  const uint32_t* dsel = nullptr;
+  if ((rc = resolve_sel(ctx, sel, n_sel, n_atoms, &dsel, s))) return rc;
+  const Mem cm = classify(coords);
+  const bool out_host = out && is_host(classify(out));
+  const bool xf_host = transforms && is_host(classify(transforms));
+  if (cm == Mem::Device && !out_host && !xf_host)
+    return superpose_device(ctx, coords, n_frames, n_atoms, stride, dsel, ref, norotate, transforms, out, s);
+  // host memory somewhere: chunks of frames through device buffers
+  const size_t frame_bytes = (size_t)n_atoms * stride * sizeof(float);
+  const size_t out_frame_bytes = (size_t)n_atoms * 3 * sizeof(float);
+  const int64_t chunk = std::max<int64_t>(
+      1, std::min<int64_t>(n_frames, (int64_t)(kChunkBytes / std::max<size_t>(frame_bytes, 1))));
+  if (cm != Mem::Device) {
+    for (int b = 0; b < 2; ++b) {
+      if ((rc = ensure(ctx, ctx->chunk[b], (size_t)chunk * frame_bytes + 16))) return rc;
+      if (cm == Mem::PageableHost && (rc = ensure_host(ctx, ctx->stage[b], (size_t)chunk * frame_bytes + 16))) return rc;
+    }
+    CU(cudaEventRecord(ctx->kern_done[0], s), "event");
+    CU(cudaEventRecord(ctx->kern_done[1], s), "event");
+    CU(cudaEventRecord(ctx->h2d_done[0], ctx->copy_stream), "event");
+    CU(cudaEventRecord(ctx->h2d_done[1], ctx->copy_stream), "event");
+  }
+  if (out_host && (rc = ensure(ctx, ctx->out_chunk, (size_t)chunk * out_frame_bytes + 16))) return rc;
+  if (xf_host && (rc = ensure(ctx, ctx->out_tmp, (size_t)chunk * 12 * sizeof(float)))) return rc;
+  int64_t k = 0;
+  for (int64_t f0 = 0; f0 < n_frames; f0 += chunk, ++k) {
+    const int b = (int)(k & 1);
+    const int64_t nf = std::min(chunk, n_frames - f0);
+    const float* dc = coords + (size_t)f0 * n_atoms * stride;
+    if (cm != Mem::Device) {
+      const size_t bytes = (size_t)nf * frame_bytes;
+      const char* src = reinterpret_cast<const char*>(dc);
+      if (cm == Mem::PageableHost) {
+        CU(cudaEventSynchronize(ctx->h2d_done[b]), "staging wait");
+        std::memcpy(ctx->stage[b].ptr, src, bytes);
+        src = static_cast<const char*>(ctx->stage[b].ptr);
+      }
+      CU(cudaStreamWaitEvent(ctx->copy_stream, ctx->kern_done[b], 0), "stream wait");
+      CU(cudaMemcpyAsync(ctx->chunk[b].ptr, src, bytes, cudaMemcpyHostToDevice, ctx->copy_stream), "H2D");
+      CU(cudaEventRecord(ctx->h2d_done[b], ctx->copy_stream), "event");
+      CU(cudaStreamWaitEvent(s, ctx->h2d_done[b], 0), "stream wait");
+      dc = static_cast<const float*>(ctx->chunk[b].ptr);
+    }
+    float* dout = !out ? nullptr : out_host ? static_cast<float*>(ctx->out_chunk.ptr) : out + (size_t)f0 * n_atoms * 3;
+    float* dxf = !transforms ? nullptr : xf_host ? static_cast<float*>(ctx->out_tmp.ptr) : transforms + f0 * 12;
+    if ((rc = superpose_device(ctx, dc, nf, n_atoms, stride, dsel, ref, norotate, dxf, dout, s))) return rc;
+    if (cm != Mem::Device) CU(cudaEventRecord(ctx->kern_done[b], s), "event");
+    if (out_host)
+      CU(cudaMemcpyAsync(out + (size_t)f0 * n_atoms * 3, dout, (size_t)nf * out_frame_bytes, cudaMemcpyDeviceToHost, s),
+         "D2H");
+    if (xf_host)
+      CU(cudaMemcpyAsync(transforms + f0 * 12, dxf, (size_t)nf * 12 * sizeof(float), cudaMemcpyDeviceToHost, s), "D2H");
+  }
+  CU(cudaStreamSynchronize(s), "synchronize");
+  return check_status(ctx);
+}
+
+WMD_EXPORT int wmd_superpose_transforms(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms,
+                                        int stride, const uint32_t* sel, int64_t n_sel, const wmd_ref* ref,
+                                        int norotate, float* transforms, void* stream) {
+  if (ctx && n_frames > 0 && !transforms) return set_err(ctx, WMD_ERR_INVALID_ARG, "transforms is null");
+  return superpose_common(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, ref, norotate, nullptr, transforms,
+                          static_cast<cudaStream_t>(stream));
+}
+
+WMD_EXPORT int wmd_superpose(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                             const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, int norotate, float* out,
+                             float* transforms, void* stream) {
+  if (ctx && n_frames > 0 && !out) return set_err(ctx, WMD_ERR_INVALID_ARG, "out is null");
+  return superpose_common(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, ref, norotate, out, transforms,
+                          static_cast<cudaStream_t>(stream));
 }
 
 WMD_EXPORT int wmd_rmsd_forward(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,

@@ -25,12 +25,14 @@ struct FrameOutputs {
 };
 
 struct RefInfo {
-  const double* yc = nullptr;  // device [n_sel][3]: y - mean(y) in FP64
+  const double* yc = nullptr;  // device [n_sel][3]: y - mean(y) in FP64 (weighted: w (y - mean_w(y)))
+  const float* w = nullptr;    // device [n_sel] per-atom weights (masses), or null
   int64_t n_sel = 0;
   double sum_c[3] = {0, 0, 0};  // sum of yc (round-off residue of the centring)
   double gy = 0;                // sum |yc - mean(yc)|^2
   double mean[3] = {0, 0, 0};   // mean(y), for the no-fit RMSD
   double sumsq = 0;             // sum |y|^2, for the no-fit RMSD
+  double wsum = 0;              // sum of the weights (n_sel when unweighted)
 };
 
 struct FrameLaunch {
@@ -71,6 +73,9 @@ cudaError_t launch_rmsd_forward(const FrameLaunch& L, cudaStream_t s);
 // Only the streaming kernel of the aligned forward (tile partials into
 // L.partial); the caller finishes the frames itself.
 cudaError_t launch_rmsd_stream(const FrameLaunch& L, cudaStream_t s);
+// Only the streaming kernel, weighted statistics: per tile sum w x (3),
+// sum w x_a^2 (3) and sum x (w y_c)^T (9) into L.partial (needs L.ref.w).
+cudaError_t launch_rmsd_stream_weighted(const FrameLaunch& L, cudaStream_t s);
 cudaError_t launch_rmsd_backward(const FrameLaunch& L, const double* stats, const float* grad_rmsd,
                                  double* rot_scratch, cudaStream_t s);
 // occupancy-derived persistent grid for a launch

@@ -9,6 +9,8 @@ crates/traj-py/src/io.rs):
     sel = system.select("name CA")
     RmsdPlan(sel, reference="frame0", align=True).run(traj, system, device="cuda:0")
     PairwiseRmsdPlan(sel, metric="rms").run(traj, system)
+    AlignPlan(sel, mass=True).run(traj, system)           # (frames, 12): R, t
+    SuperposePlan(sel).run(traj, system)                   # every atom superposed
 
 Every plan runs on the CUDA library in ``_native/libwarpmd_rmsd.so``; there is
 no CPU path.  ``device="cpu"`` raises, ``"auto"`` means ``"cuda:0"``.
@@ -19,7 +21,8 @@ __version__ = "0.4.30"
 
 from ._native import WarpMdError  # noqa: F401
 from .core import Selection, System, Trajectory  # noqa: F401
-from .plans import PairwiseRmsdPlan, RmsdPlan  # noqa: F401
+from .plans import (AlignPlan, PairwiseRmsdPlan, RmsdPlan, RotationMatrixPlan, SuperposePlan,  # noqa: F401
+                    SuperposeTrajectoryPlan)
 from . import synth  # noqa: F401
 
 __rust_cuda_enabled__ = True
@@ -32,4 +35,5 @@ def native_version() -> str:
     return version()
 
 
-__all__ = ["System", "Selection", "Trajectory", "RmsdPlan", "PairwiseRmsdPlan", "WarpMdError", "synth"]
+__all__ = ["System", "Selection", "Trajectory", "RmsdPlan", "PairwiseRmsdPlan", "AlignPlan", "RotationMatrixPlan",
+           "SuperposePlan", "SuperposeTrajectoryPlan", "WarpMdError", "synth"]

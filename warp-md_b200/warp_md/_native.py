@@ -39,6 +39,7 @@ EXPORTED = (
     "wmd_create", "wmd_destroy", "wmd_last_error", "wmd_version", "wmd_reference_upload", "wmd_reference_free",
     "wmd_rmsd_frames", "wmd_rmsd_forward", "wmd_rmsd_backward", "wmd_rmsd_covariance", "wmd_pairwise_rmsd",
     "wmd_batched_prepare", "wmd_batched_rmsd", "wmd_batched_layout", "wmd_rmsd_frames_noalloc",
+    "wmd_reference_upload_weighted", "wmd_superpose_transforms", "wmd_superpose",
 )
 
 
@@ -93,6 +94,9 @@ def load() -> ctypes.CDLL:
         L.wmd_batched_prepare.argtypes = [vp, ctypes.POINTER(BatchDesc), i32, i32]
         L.wmd_batched_rmsd.argtypes = [vp, ctypes.POINTER(BatchDesc), i32, i32, vp]
         L.wmd_batched_layout.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32)]
+        L.wmd_reference_upload_weighted.argtypes = [vp, vp, i64, i32, vp, ctypes.POINTER(vp)]
+        L.wmd_superpose_transforms.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, i32, vp, vp]
+        L.wmd_superpose.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, i32, vp, vp, vp]
         L.wmd_rmsd_frames_noalloc.argtypes = [vp, i64, i64, i32, vp, i64, i32, vp, vp]
         for name in EXPORTED:
             getattr(L, name).restype = getattr(L, name).restype if name in ("wmd_last_error", "wmd_version") else i32
@@ -135,20 +139,29 @@ class Context:
 class Reference:
     """A reference structure uploaded to the device (wmd_ref)."""
 
-    def __init__(self, ctx: Context, coords_ptr: int, n_sel: int, stride: int, keepalive=None):
+    def __init__(self, ctx: Context, coords_ptr: int, n_sel: int, stride: int, keepalive=None, weights_ptr=None):
         self.ctx = ctx
         self.n_sel = int(n_sel)
         h = ctypes.c_void_p()
-        ctx.check(ctx.lib.wmd_reference_upload(ctx.handle, coords_ptr, int(n_sel), int(stride), ctypes.byref(h)))
+        if weights_ptr is None:
+            ctx.check(ctx.lib.wmd_reference_upload(ctx.handle, coords_ptr, int(n_sel), int(stride), ctypes.byref(h)))
+        else:
+            ctx.check(ctx.lib.wmd_reference_upload_weighted(ctx.handle, coords_ptr, int(n_sel), int(stride),
+                                                            weights_ptr, ctypes.byref(h)))
         self.handle = h
         self._keep = keepalive
 
     @classmethod
-    def from_numpy(cls, ctx: Context, ref: np.ndarray) -> "Reference":
+    def from_numpy(cls, ctx: Context, ref: np.ndarray, weights: Optional[np.ndarray] = None) -> "Reference":
         r = np.ascontiguousarray(ref, dtype=np.float32)
         if r.ndim != 2 or r.shape[1] not in (3, 4):
             raise WarpMdError(WMD_ERR_INVALID_ARG, "reference must have shape (atoms, 3) or (atoms, 4)")
-        return cls(ctx, r.ctypes.data, r.shape[0], r.shape[1], keepalive=r)
+        if weights is None:
+            return cls(ctx, r.ctypes.data, r.shape[0], r.shape[1], keepalive=r)
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        if w.shape != (r.shape[0],):
+            raise WarpMdError(WMD_ERR_MISMATCH, "weights must have one entry per reference atom")
+        return cls(ctx, r.ctypes.data, r.shape[0], r.shape[1], keepalive=(r, w), weights_ptr=w.ctypes.data)
 
     def close(self) -> None:
         if getattr(self, "handle", None) and self.ctx.handle:

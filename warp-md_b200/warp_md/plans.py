@@ -169,3 +169,146 @@ class PairwiseRmsdPlan:
         ctx.check(ctx.lib.wmd_pairwise_rmsd(ctx.handle, coords.ctypes.data, n, coords.shape[1], 3, N.ptr(sel_arr),
                                             int(sel.size), metric, _PAIR_MODES[self.mode], out.ctypes.data, None))
         return out
+
+
+# ---------------------------------------------------------------------------
+# superposition plans
+# ---------------------------------------------------------------------------
+
+def _superpose_inputs(plan, traj: Trajectory, system: System, frame_indices):
+    """Selection, (subset) frames and reference of a superposition plan: the
+    topology positions0 or the first processed frame (plan_exec.rs:82-100,
+    131-140), with the selected atoms' masses as weights when mass=True."""
+    sel = _check_inputs(traj, system, plan.selection)
+    coords = traj.coords
+    sub = frame_subset(coords.shape[0], frame_indices)
+    if sub is not None:
+        coords = np.ascontiguousarray(coords[sub])
+    if plan.reference_mode == "topology":
+        if system.positions0 is None:
+            raise RuntimeError("mismatch: no topology reference coords")
+        ref = system.positions0[sel]
+    else:
+        ref = coords[0][sel] if coords.shape[0] else None
+    weights = np.ascontiguousarray(system.masses[sel], dtype=np.float32) if plan.mass else None
+    return sel, coords, sub, ref, weights
+
+
+def superpose_arrays(coords: np.ndarray, sel: np.ndarray, ref: Optional[np.ndarray], weights: Optional[np.ndarray],
+                     norotate: bool, apply: bool, device: str = "auto"):
+    """Per-frame transforms [F][12] float32 of frames (F, N, 3) onto ``ref``
+    (the selected atoms) and, with ``apply``, every atom moved (F, N, 3)."""
+    dev = parse_device(device)
+    coords = np.ascontiguousarray(coords, dtype=np.float32)
+    n_frames, n_atoms = coords.shape[0], coords.shape[1]
+    xf = np.empty((n_frames, 12), np.float32)
+    out = np.empty((n_frames, n_atoms, 3), np.float32) if apply else None
+    if n_frames == 0:
+        return xf, out
+    ctx = N.context(dev)
+    r = N.Reference.from_numpy(ctx, np.asarray(ref, dtype=np.float32).reshape(-1, 3), weights=weights)
+    try:
+        dense = _dense_prefix(sel)
+        sel_arr = None if dense else np.ascontiguousarray(sel, dtype=np.uint32)
+        if apply:
+            ctx.check(ctx.lib.wmd_superpose(ctx.handle, coords.ctypes.data, n_frames, n_atoms, 3, N.ptr(sel_arr),
+                                            int(sel.size), r.handle, int(norotate), out.ctypes.data,
+                                            xf.ctypes.data, None))
+        else:
+            ctx.check(ctx.lib.wmd_superpose_transforms(ctx.handle, coords.ctypes.data, n_frames, n_atoms, 3,
+                                                       N.ptr(sel_arr), int(sel.size), r.handle, int(norotate),
+                                                       xf.ctypes.data, None))
+    finally:
+        r.close()
+    return xf, out
+
+
+def _run_superpose(plan, traj: Trajectory, system: System, device: str, frame_indices, apply: bool):
+    parse_device(device)
+    sel, coords, sub, ref, weights = _superpose_inputs(plan, traj, system, frame_indices)
+    if coords.shape[0] == 0:
+        return (np.empty((0, 12), np.float32), np.empty((0, coords.shape[1], 3), np.float32) if apply else None,
+                sub)
+    xf, out = superpose_arrays(coords, sel, ref, weights, plan.norotate, apply, device)
+    return xf, out, sub
+
+
+class AlignPlan:
+    """Per-frame superposition transforms (warp_md.AlignPlan,
+    crates/traj-py/src/transform.rs:1802-1837): rows of 12 float32 -- R
+    row-major (R maps the frame onto the reference) then t = c_ref - R c_frame
+    (plan_exec.rs:224-238)."""
+
+    def __init__(self, selection: Selection, reference: str = "topology", mass: bool = False, norotate: bool = False):
+        self.selection = selection
+        self.reference_mode = parse_reference(reference)
+        self.mass = bool(mass)
+        self.norotate = bool(norotate)
+
+    def run(self, traj: Trajectory, system: System, chunk_frames: Optional[int] = None,
+            device: str = "auto") -> np.ndarray:
+        xf, _, _ = _run_superpose(self, traj, system, device, None, apply=False)
+        return xf
+
+
+class RotationMatrixPlan:
+    """Per-frame rotation matrices, (frames, 9) float32 (warp_md.RotationMatrixPlan,
+    crates/traj-py/src/correlation.rs:313-349; align_matrix.rs:16-70: the
+    first 9 columns of AlignPlan's rows)."""
+
+    def __init__(self, selection: Selection, reference: str = "topology", mass: bool = False):
+        self.selection = selection
+        self.reference_mode = parse_reference(reference)
+        self.mass = bool(mass)
+        self.norotate = False
+
+    def run(self, traj: Trajectory, system: System, chunk_frames: Optional[int] = None, device: str = "auto",
+            frame_indices: Optional[Sequence[int]] = None) -> np.ndarray:
+        xf, _, _ = _run_superpose(self, traj, system, device, frame_indices, apply=False)
+        return np.ascontiguousarray(xf[:, :9])
+
+
+class SuperposePlan:
+    """Every atom of every (selected) frame superposed onto the reference
+    (warp_md.SuperposePlan, correlation.rs:269-304): a flat float32 series of
+    frames x atoms x 3 (plan_exec.rs:431-462)."""
+
+    def __init__(self, selection: Selection, reference: str = "topology", mass: bool = False, norotate: bool = False):
+        self.selection = selection
+        self.reference_mode = parse_reference(reference)
+        self.mass = bool(mass)
+        self.norotate = bool(norotate)
+
+    def run(self, traj: Trajectory, system: System, chunk_frames: Optional[int] = None, device: str = "auto",
+            frame_indices: Optional[Sequence[int]] = None) -> np.ndarray:
+        _, out, _ = _run_superpose(self, traj, system, device, frame_indices, apply=True)
+        return out.reshape(-1)
+
+
+class SuperposeTrajectoryPlan:
+    """SuperposePlan returning a trajectory payload (warp_md.SuperposeTrajectoryPlan,
+    transform.rs:1839-1875, trajectory_output_to_py transform.rs:1353-1391):
+    {"coords": (frames, atoms, 3) float32, "box": (frames, 3) or None,
+    "time_ps": (frames,) or None}."""
+
+    def __init__(self, selection: Selection, reference: str = "topology", mass: bool = False, norotate: bool = False):
+        self.inner = SuperposePlan(selection, reference, mass, norotate)
+
+    def run(self, traj: Trajectory, system: System, chunk_frames: Optional[int] = None, device: str = "auto",
+            frame_indices: Optional[Sequence[int]] = None) -> dict:
+        _, out, sub = _run_superpose(self.inner, traj, system, device, frame_indices, apply=True)
+        n = out.shape[0]
+
+        def per_frame(values):
+            if values is None:
+                return None
+            a = np.asarray(values)
+            if sub is not None and a.shape[0] == traj.coords.shape[0]:
+                a = a[sub]
+            return a if a.shape[0] == n and n > 0 else None
+
+        box = per_frame(traj.box)
+        time = per_frame(traj.time_ps)
+        return {"coords": out,
+                "box": None if box is None else np.asarray(box, dtype=np.float32).reshape(n, -1)[:, :3],
+                "time_ps": None if time is None else np.asarray(time, dtype=np.float32).reshape(n)}
