@@ -13,8 +13,9 @@
 //      runs, one lane per frame, QCP and the rotation from the QCP
 //      eigenvector in FP64 (the same rotation the SVD gives, with the
 //      reflection handled by construction), writing the 12-number transform;
-//   3. superpose_apply_kernel moves every atom of every frame, FP64
-//      arithmetic rounded to float32 as the reference does.
+//   3. superpose_apply_staged (packed, aligned buffers) or
+//      superpose_apply_kernel (the rest) moves every atom of every frame,
+//      FP64 arithmetic rounded to float32 as the reference does.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -107,6 +108,148 @@ __global__ void __launch_bounds__(256) superpose_apply_kernel(const float* __res
   }
 }
 
+// Staged apply for packed xyz input and output with 16-byte aligned bases:
+// work items are (frame, 1024-atom chunk), frame-major; persistent CTAs walk
+// contiguous runs.  Thread 0 streams each item's 16-byte hull into a 4-stage
+// shared-memory ring (1-D bulk copies on mbarriers), every thread moves its
+// atoms in place in the stage, and the item leaves by one bulk store of its
+// aligned middle plus at most 2 x 3 scalar floats at its ends.  The stage of
+// item i-1 is refilled at the end of item i, once its store has been read
+// out (bulk wait_group.read).
+constexpr int kApplyTile = 1024;
+struct AGeo {
+  static constexpr int kStageBytes = ((kApplyTile * 12 + 32) + 127) / 128 * 128;
+  static constexpr int kStages = 4;
+  static constexpr int kBarOffset = kStages * kStageBytes;
+  static constexpr int kAbortOffset = kBarOffset + kStages * 8;
+  static constexpr int kSmemBytes = kAbortOffset + 16;
+};
+
+__device__ __forceinline__ void apply_issue(const float* coords, int64_t n_frames, int64_t n_atoms, int64_t f, int c,
+                                            unsigned char* dst, uint64_t* bar) {
+  const int64_t a0 = (int64_t)c * kApplyTile;
+  const int64_t a1 = min(n_atoms, a0 + kApplyTile);
+  const unsigned char* base = reinterpret_cast<const unsigned char*>(coords);
+  const uint64_t total_al = ((uint64_t)n_frames * (uint64_t)n_atoms * 12ull) & ~15ull;
+  const uint64_t b0 = (uint64_t)(f * n_atoms + a0) * 12ull;
+  const uint64_t b1 = (uint64_t)(f * n_atoms + a1) * 12ull;
+  const uint64_t c0 = b0 & ~15ull;
+  uint64_t c1 = (b1 + 15ull) & ~15ull;
+  if (c1 > total_al) {
+    const uint64_t tail0 = total_al > c0 ? total_al : c0;
+    for (uint64_t bb = tail0; bb < b1; bb += 4)
+      *reinterpret_cast<float*>(dst + (bb - c0)) = __ldg(reinterpret_cast<const float*>(base + bb));
+    c1 = tail0;
+  }
+  const uint32_t core = (uint32_t)(c1 - c0);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  mbar_arrive_expect_tx(bar, core);
+  if (core) bulk_copy_g2s(dst, base + c0, core, bar);
+}
+
+__global__ void __launch_bounds__(kThreads, 4) superpose_apply_staged(const float* __restrict__ coords,
+                                                                      int64_t n_frames, int64_t n_atoms,
+                                                                      const double* __restrict__ xf,
+                                                                      float* __restrict__ out, int* status) {
+  constexpr int S = AGeo::kStages;
+  constexpr int APT = kApplyTile / kConsumerThreads;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + AGeo::kBarOffset);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + AGeo::kAbortOffset);
+  const int tid = threadIdx.x;
+  const int nc = (int)((n_atoms + kApplyTile - 1) / kApplyTile);
+  const int64_t W = (int64_t)nc * n_frames;
+  const int64_t w0 = W * blockIdx.x / gridDim.x, w1 = W * (blockIdx.x + 1) / gridDim.x;
+  const int64_t n_items = w1 - w0;
+  if (tid == 0) {
+    for (int st = 0; st < S; ++st) mbar_init(&full[st], 1);
+    *abort_flag = 0;
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (n_items <= 0) return;
+  int64_t pf = w0 / nc;
+  int pc = (int)(w0 - pf * nc);
+  int64_t issued = 0;
+  auto issue = [&]() {
+    const int sp = (int)(issued % S);
+    apply_issue(coords, n_frames, n_atoms, pf, pc, smem + sp * AGeo::kStageBytes, &full[sp]);
+    ++issued;
+    if (++pc == nc) { pc = 0; ++pf; }
+  };
+  if (tid == 0)
+    while (issued < S - 1 && issued < n_items) issue();
+  int64_t f = w0 / nc;
+  int c = (int)(w0 - f * nc);
+  int64_t cur_f = -1;
+  double R[9], t[3];
+  int s = 0;
+  uint32_t phase = 0;
+  unsigned char* obase = reinterpret_cast<unsigned char*>(out);
+  for (int64_t i = 0; i < n_items; ++i) {
+    if (f != cur_f) {
+      cur_f = f;
+      const double* x = xf + f * kStatDoubles;
+#pragma unroll
+      for (int e = 0; e < 9; ++e) R[e] = __ldg(x + e);
+      t[0] = __ldg(x + 9); t[1] = __ldg(x + 10); t[2] = __ldg(x + 11);
+    }
+    const int64_t a0 = (int64_t)c * kApplyTile;
+    const int len = (int)(min(n_atoms, a0 + kApplyTile) - a0);
+    const uint64_t b0 = (uint64_t)(f * n_atoms + a0) * 12ull;
+    const bool ok = mbar_wait(&full[s], phase, status, kStatusTimeoutFull, abort_flag);
+    float* xs = reinterpret_cast<float*>(smem + s * AGeo::kStageBytes) + (int)((b0 & 15ull) >> 2);
+    if (ok) {
+#pragma unroll
+      for (int j = 0; j < APT; ++j) {
+        const int k = tid + j * kConsumerThreads;
+        if (k < len) {
+          const double p0 = xs[k * 3 + 0], p1 = xs[k * 3 + 1], p2 = xs[k * 3 + 2];
+          xs[k * 3 + 0] = (float)(R[0] * p0 + R[1] * p1 + R[2] * p2 + t[0]);
+          xs[k * 3 + 1] = (float)(R[3] * p0 + R[4] * p1 + R[5] * p2 + t[1]);
+          xs[k * 3 + 2] = (float)(R[6] * p0 + R[7] * p1 + R[8] * p2 + t[2]);
+        }
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    named_barrier_sync(1, kConsumerThreads);
+    const uint64_t b1 = b0 + (uint64_t)len * 12ull;
+    const uint64_t m0 = (b0 + 15ull) & ~15ull, m1 = b1 & ~15ull;
+    const bool mid = m1 > m0;
+    const unsigned char* sbase = reinterpret_cast<const unsigned char*>(xs) - (b0 & 15ull);
+    if (tid == 0) {
+      if (ok && !*abort_flag && mid) bulk_copy_s2g(obase + m0, sbase + (m0 - (b0 & ~15ull)), (uint32_t)(m1 - m0));
+      bulk_commit();
+      bulk_wait_read<1>();
+      if (issued < n_items) issue();
+    } else if (ok && tid >= 32 && tid < 38) {
+      const int q = tid - 32;
+      const uint64_t at = mid ? (q < 3 ? b0 + 4ull * q : m1 + 4ull * (q - 3)) : b0 + 4ull * q;
+      const uint64_t lim = mid ? (q < 3 ? m0 : b1) : b1;
+      if (at < lim)
+        *reinterpret_cast<float*>(obase + at) = *reinterpret_cast<const float*>(sbase + (at - (b0 & ~15ull)));
+    }
+    if (*abort_flag) break;
+    if (++s == S) { s = 0; phase ^= 1u; }
+    if (++c == nc) { c = 0; ++f; }
+  }
+  if (tid == 0) {
+    bulk_wait_all<0>();
+    const int64_t first = issued > S ? issued - S : 0;
+    for (int64_t j = first; j < issued; ++j) {
+      const int st = (int)(j % S);
+      const uint32_t ph = (uint32_t)((j / S) & 1);
+      const uint64_t t0 = global_timer_ns();
+      while (!mbar_try_wait(&full[st], ph)) {
+        if (global_timer_ns() - t0 > kWaitLimitNs) {
+          atomicOr(status, kStatusTimeoutDrain);
+          break;
+        }
+      }
+    }
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_superpose_finalize(const FrameLaunch& L, int norotate, double* xf64, float* xf32, cudaStream_t s) {
@@ -117,9 +260,24 @@ cudaError_t launch_superpose_finalize(const FrameLaunch& L, int norotate, double
 }
 
 cudaError_t launch_superpose_apply(const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
-                                   const double* xf64, float* out, int sm_count, cudaStream_t s) {
+                                   const double* xf64, float* out, int sm_count, int* status, cudaStream_t s) {
   if (n_frames == 0 || n_atoms == 0) return cudaSuccess;
   const int64_t items = n_frames * ((n_atoms + 1023) / 1024);
+  if (stride == 3 && ((reinterpret_cast<uintptr_t>(coords) | reinterpret_cast<uintptr_t>(out)) & 15u) == 0) {
+    static bool attr_done[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!attr_done[dev]) {
+      cudaError_t e =
+          cudaFuncSetAttribute(superpose_apply_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, AGeo::kSmemBytes);
+      if (e != cudaSuccess) return e;
+      attr_done[dev] = true;
+    }
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)sm_count * 4));
+    superpose_apply_staged<<<grid, kThreads, AGeo::kSmemBytes, s>>>(coords, n_frames, n_atoms, xf64, out, status);
+    return cudaGetLastError();
+  }
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)sm_count * 8));
   if (stride == 4) superpose_apply_kernel<4><<<grid, 256, 0, s>>>(coords, n_frames, n_atoms, xf64, out);
   else superpose_apply_kernel<3><<<grid, 256, 0, s>>>(coords, n_frames, n_atoms, xf64, out);

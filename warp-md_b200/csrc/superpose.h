@@ -17,7 +17,10 @@ namespace wmd {
 cudaError_t launch_superpose_finalize(const FrameLaunch& L, int norotate, double* xf64, float* xf32, cudaStream_t s);
 
 // out[f][a] = R_f coords[f][a] + t_f for every atom, float32 packed xyz.
+// Packed input with 16-byte aligned coords and out takes the shared-memory
+// staged kernel (bulk copies in and out); anything else the plain one.
+// status: device-visible word the staged kernel reports bounded-wait timeouts into.
 cudaError_t launch_superpose_apply(const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
-                                   const double* xf64, float* out, int sm_count, cudaStream_t s);
+                                   const double* xf64, float* out, int sm_count, int* status, cudaStream_t s);
 
 }  // namespace wmd

@@ -687,7 +687,7 @@ static int superpose_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames
     CU(wmd::launch_superpose_finalize(B, norotate, xf, dxf32 ? dxf32 + f0 * 12 : nullptr, s), "superpose transforms");
     if (dout)
       CU(wmd::launch_superpose_apply(B.coords, nf, n_atoms, stride, xf, dout + (size_t)f0 * n_atoms * 3, ctx->sm_count,
-                                     s),
+                                     ctx->status_dev, s),
          "superpose apply");
   }
   return WMD_OK;
