@@ -194,6 +194,35 @@ int wmd_superpose(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n
                   const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, int norotate, float* out,
                   float* transforms, void* stream);
 
+/* ---- Fluctuations and per-residue RMSD (RmsfPlan, AtomicFluctPlan,
+ *      BfactorsPlan, AtomicAdpPlan, RmsdPerResPlan:
+ *      crates/traj-engine/src/plans/geometry/rms.rs:17-430, 431-686) ---- */
+
+/* Per selected atom, over all frames, without superposition:
+ *   rmsf[i]  = sqrt(var_x + var_y + var_z)            (RmsfPlan, rms.rs:193-218)
+ *   adp[i]   = (uxx, uyy, uzz, uxy, uxz, uyz), the covariance of the position
+ *              with the diagonal clamped at 0         (AtomicAdpPlan, rms.rs:378-411)
+ * Either output may be NULL.  Moments are taken in FP64 about each atom's
+ * position in the first frame.  n_frames == 0 gives RMSF 0 and writes no ADP
+ * rows.  BfactorsPlan is 8 pi^2 / 3 * rmsf^2 and AtomicFluctPlan is rmsf: the
+ * caller derives them.  coords and the outputs may be host or device memory;
+ * with any host pointer the call synchronizes. */
+int wmd_rmsf(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride, const uint32_t* sel,
+             int64_t n_sel, float* rmsf, float* adp, void* stream);
+
+/* RmsdPerResPlan: per frame, the selection is superposed onto `ref` (the
+ * selected reference atoms, unweighted Kabsch) when align != 0, and for every
+ * group g (a residue) out[f][g] = sqrt(mean over the group's atoms a of
+ * |R x_a + t - ref_all[a]|^2); align == 0 compares raw coordinates.  Groups
+ * are given by group_offsets[n_groups + 1] into group_atoms (atom indices into
+ * the frame), both host memory; ref_all [n_atoms][3] is the reference for
+ * every atom (host or device).  An empty group gives 0.  out is float32
+ * [n_frames][n_groups], host or device. */
+int wmd_rmsd_per_group(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                       const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, const float* ref_all,
+                       const uint32_t* group_offsets, const uint32_t* group_atoms, int64_t n_groups, int align,
+                       float* out, void* stream);
+
 /* Per-frame aligned RMSD for callers that cannot allocate memory.  No
  * counterpart in the reference.  Everything else in this header needs a
  * wmd_ctx and a wmd_ref, which allocate device and pinned memory; this call

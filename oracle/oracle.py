@@ -53,6 +53,10 @@ def lib():
         L.wmdo_kabsch_rotation.restype = None
         L.wmdo_superpose.argtypes = [_vp, _i64, _i64, _int, _vp, _i64, _vp, _int, _vp, _int, _vp, _vp, _int]
         L.wmdo_superpose.restype = None
+        L.wmdo_rmsf.argtypes = [_vp, _i64, _i64, _int, _vp, _i64, _vp, _vp]
+        L.wmdo_rmsf.restype = None
+        L.wmdo_rmsd_perres.argtypes = [_vp, _i64, _i64, _int, _vp, _i64, _vp, _vp, _vp, _i64, _int, _vp]
+        L.wmdo_rmsd_perres.restype = None
         _lib = L
     return _lib
 
@@ -149,3 +153,32 @@ def superpose(coords, reference, selection=None, weights=None, norotate: bool = 
     lib().wmdo_superpose(_ptr(c), c.shape[0], c.shape[1], stride, _ptr(sel), ref.shape[0], _ptr(ref), ref.shape[1],
                          _ptr(w), int(bool(norotate)), _ptr(xf), _ptr(out), int(threads))
     return xf, out
+
+
+def rmsf(coords, selection=None, n_sel=None):
+    """RmsfPlan (Welford, FP64) and AtomicAdpPlan moments.  Returns (rmsf [n_sel],
+    adp [n_sel][6]) in FP64."""
+    c, stride = _coords(coords)
+    sel = None if selection is None else np.ascontiguousarray(selection, dtype=np.uint32)
+    n = sel.shape[0] if sel is not None else (c.shape[1] if n_sel is None else n_sel)
+    r = np.zeros(n, np.float64)
+    a = np.zeros((n, 6), np.float64)
+    lib().wmdo_rmsf(_ptr(c), c.shape[0], c.shape[1], stride, _ptr(sel), n, _ptr(r), _ptr(a))
+    return r, a
+
+
+def rmsd_perres(coords, ref_all, groups, selection=None, align: bool = True):
+    """RmsdPerResPlan CPU path.  groups: list of atom-index lists.  Returns FP64
+    [frames][groups]."""
+    c, stride = _coords(coords)
+    ref = np.ascontiguousarray(ref_all, dtype=np.float32)
+    sel = None if selection is None else np.ascontiguousarray(selection, dtype=np.uint32)
+    n_sel = sel.shape[0] if sel is not None else c.shape[1]
+    goff = np.zeros(len(groups) + 1, np.uint32)
+    goff[1:] = np.cumsum([len(g) for g in groups])
+    gat = np.ascontiguousarray(np.concatenate([np.asarray(g, np.uint32) for g in groups]) if groups else
+                               np.zeros(1, np.uint32), dtype=np.uint32)
+    out = np.zeros((c.shape[0], len(groups)), np.float64)
+    lib().wmdo_rmsd_perres(_ptr(c), c.shape[0], c.shape[1], stride, _ptr(sel), n_sel, _ptr(ref), _ptr(goff),
+                           _ptr(gat), len(groups), int(bool(align)), _ptr(out))
+    return out

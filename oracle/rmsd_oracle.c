@@ -19,6 +19,8 @@
  *       plan_exec.rs:125-266, 325-459 with kabsch_rotation_weighted and
  *       centroid_weighted (crates/traj-engine/src/plans/geometry/
  *       geometry_math.rs:202-300): weighted Kabsch, t = cy - R cx, R x + t.
+ *   - RmsfPlan / AtomicAdpPlan / RmsdPerResPlan
+ *       crates/traj-engine/src/plans/geometry/rms.rs:110-218, 345-429, 633-671.
  *
  * The SVD in the reference is nalgebra 0.32.6 (Cargo.lock:792-793), which is
  * not vendored.  Here it is a one-sided Jacobi SVD (Hestenes 1958; Demmel &
@@ -475,4 +477,95 @@ WMDO_API void wmdo_superpose(const float* coords, int64_t n_frames, int64_t n_at
     }
   }
   (void)n_threads;
+}
+
+/* ------------------------------------------------------------------ */
+/* Fluctuations and per-residue RMSD                                   */
+/* ------------------------------------------------------------------ */
+
+/* RmsfPlan CPU path (crates/traj-engine/src/plans/geometry/rms.rs:110-140,
+ * 193-218): Welford running mean / M2 per selected atom and axis, FP64;
+ * rmsf = sqrt((M2x + M2y + M2z) / n).  AtomicAdpPlan (rms.rs:345-429): raw
+ * sums of x and of the six products, u_ab = <ab> - <a><b>, diagonal clamped
+ * at 0.  Either output may be NULL. */
+WMDO_API void wmdo_rmsf(const float* coords, int64_t n_frames, int64_t n_atoms, int stride, const uint32_t* sel,
+                        int64_t n_sel, double* rmsf, double* adp) {
+  for (int64_t i = 0; i < n_sel; ++i) {
+    const int64_t a = sel ? (int64_t)sel[i] : i;
+    double mean[3] = {0, 0, 0}, m2[3] = {0, 0, 0}, s[3] = {0, 0, 0}, pr[6] = {0, 0, 0, 0, 0, 0};
+    for (int64_t f = 0; f < n_frames; ++f) {
+      const float* p = coords + (f * n_atoms + a) * stride;
+      const double n = (double)(f + 1);
+      for (int c = 0; c < 3; ++c) {
+        const double x = p[c];
+        const double d = x - mean[c];
+        mean[c] += d / n;
+        m2[c] += d * (x - mean[c]);
+        s[c] += x;
+      }
+      const double x = p[0], y = p[1], z = p[2];
+      pr[0] += x * x; pr[1] += y * y; pr[2] += z * z; pr[3] += x * y; pr[4] += x * z; pr[5] += y * z;
+    }
+    if (rmsf) rmsf[i] = n_frames ? sqrt((m2[0] + m2[1] + m2[2]) / (double)n_frames) : 0.0;
+    if (adp && n_frames) {
+      const double inv = 1.0 / (double)n_frames;
+      const double mx = s[0] * inv, my = s[1] * inv, mz = s[2] * inv;
+      double* o = adp + i * 6;
+      o[0] = fmax(pr[0] * inv - mx * mx, 0.0);
+      o[1] = fmax(pr[1] * inv - my * my, 0.0);
+      o[2] = fmax(pr[2] * inv - mz * mz, 0.0);
+      o[3] = pr[3] * inv - mx * my;
+      o[4] = pr[4] * inv - mx * mz;
+      o[5] = pr[5] * inv - my * mz;
+    }
+  }
+}
+
+/* RmsdPerResPlan CPU path (rms.rs:633-671): per frame the unweighted Kabsch of
+ * the selection onto ref_all[sel] (kabsch_rotation), then per group
+ * sqrt(sum |R (x - cx) - (y - cy)|^2 / max(n, 1)); align = 0 compares raw
+ * coordinates.  out [n_frames][n_groups] in FP64 (the reference rounds to f32). */
+WMDO_API void wmdo_rmsd_perres(const float* coords, int64_t n_frames, int64_t n_atoms, int stride, const uint32_t* sel,
+                               int64_t n_sel, const float* ref_all, const uint32_t* goff, const uint32_t* gatoms,
+                               int64_t n_groups, int align, double* out) {
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 4)
+#endif
+  for (int64_t f = 0; f < n_frames; ++f) {
+    const float* frame = coords + f * n_atoms * stride;
+    double r[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, cx[3] = {0, 0, 0}, cy[3] = {0, 0, 0};
+    if (align && n_sel > 0) {
+      for (int64_t i = 0; i < n_sel; ++i) {
+        const int64_t a = sel ? (int64_t)sel[i] : i;
+        for (int c = 0; c < 3; ++c) { cx[c] += frame[a * stride + c]; cy[c] += ref_all[a * 3 + c]; }
+      }
+      for (int c = 0; c < 3; ++c) { cx[c] /= (double)n_sel; cy[c] /= (double)n_sel; }
+      double h[9] = {0};
+      for (int64_t i = 0; i < n_sel; ++i) {
+        const int64_t a = sel ? (int64_t)sel[i] : i;
+        double px[3], qy[3];
+        for (int c = 0; c < 3; ++c) { px[c] = frame[a * stride + c] - cx[c]; qy[c] = ref_all[a * 3 + c] - cy[c]; }
+        for (int u = 0; u < 3; ++u)
+          for (int v = 0; v < 3; ++v) h[u * 3 + v] += px[u] * qy[v];
+      }
+      kabsch_rotation(h, r, NULL);
+    }
+    for (int64_t g = 0; g < n_groups; ++g) {
+      double sum = 0.0;
+      for (uint32_t k = goff[g]; k < goff[g + 1]; ++k) {
+        const int64_t a = gatoms[k];
+        double p[3], q[3];
+        for (int c = 0; c < 3; ++c) {
+          p[c] = (double)frame[a * stride + c] - (align ? cx[c] : 0.0);
+          q[c] = (double)ref_all[a * 3 + c] - (align ? cy[c] : 0.0);
+        }
+        for (int u = 0; u < 3; ++u) {
+          const double d = (align ? r[u * 3] * p[0] + r[u * 3 + 1] * p[1] + r[u * 3 + 2] * p[2] : p[u]) - q[u];
+          sum += d * d;
+        }
+      }
+      const double n = goff[g + 1] > goff[g] ? (double)(goff[g + 1] - goff[g]) : 1.0;
+      out[f * n_groups + g] = sqrt(sum / n);
+    }
+  }
 }

@@ -1,0 +1,223 @@
+// fluct.cu -- per-atom fluctuations over frames (RmsfPlan, AtomicFluctPlan,
+// BfactorsPlan, AtomicAdpPlan) and per-group RMSD after superposition
+// (RmsdPerResPlan).
+//
+// Fluctuations.  The reference keeps, per selected atom, a Welford running mean
+// and M2 in FP64 on the host (crates/traj-engine/src/plans/geometry/rms.rs:
+// 96-218), or sums x, y, z and |x|^2 (rms.rs:397-429 for the 6 ADP moments).
+// Here every atom's coordinates are shifted by their value in the first frame
+// (differences of two floats are exact in FP64, and so are their squares), and
+// the nine moments sum d, sum d_c^2, sum d_x d_y / d_x d_z / d_y d_z run in FP64:
+//   * fluct_partial_kernel: a thread per selected atom and frame group -- a
+//     CTA covers 256 consecutive selected atoms over one contiguous run of
+//     frames, so a warp's three loads per frame cover 384 contiguous bytes of
+//     a dense selection; partial moments go to [group][atom][9];
+//   * fluct_reduce_kernel adds the groups in order into a running FP64
+//     accumulator (host-resident trajectories arrive chunk by chunk);
+//   * fluct_finalize_kernel turns the moments into RMSF and the ADP tensor.
+//
+// Per-group RMSD.  Per frame, the selection's transform (R, t) comes from the
+// superposition path; per (frame, group) a thread sums |R x + t - y|^2 over the
+// group's atoms against the all-atom reference (rms.rs:633-671) in FP64.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "device_util.cuh"
+#include "fluct.h"
+#include "wmd_internal.h"
+
+namespace wmd {
+namespace {
+
+constexpr int kFluctThreads = 256;
+
+template <int STRIDE>
+__global__ void __launch_bounds__(kFluctThreads) fluct_shift_kernel(const float* __restrict__ coords,
+                                                                    int64_t n_atoms, const uint32_t* __restrict__ sel,
+                                                                    int64_t n_sel, float* __restrict__ shift,
+                                                                    int* status) {
+  const int64_t i = (int64_t)blockIdx.x * kFluctThreads + threadIdx.x;
+  if (i >= n_sel) return;
+  int64_t a = sel ? (int64_t)sel[i] : i;
+  if (a >= n_atoms) {  // bad device-side selection: report, read atom 0
+    atomicOr(status, kStatusBadIndex);
+    a = 0;
+  }
+  for (int c = 0; c < 3; ++c) shift[i * 3 + c] = coords[a * STRIDE + c];
+}
+
+template <int STRIDE>
+__global__ void __launch_bounds__(kFluctThreads) fluct_partial_kernel(const float* __restrict__ coords,
+                                                                      int64_t n_frames, int64_t n_atoms,
+                                                                      const uint32_t* __restrict__ sel, int64_t n_sel,
+                                                                      const float* __restrict__ shift,
+                                                                      double* __restrict__ part) {
+  const int64_t i = (int64_t)blockIdx.x * kFluctThreads + threadIdx.x;
+  const int g = blockIdx.y, G = gridDim.y;
+  if (i >= n_sel) return;
+  const int64_t f0 = n_frames * g / G, f1 = n_frames * (g + 1) / G;
+  int64_t a = sel ? (int64_t)sel[i] : i;
+  if (a >= n_atoms) a = 0;  // reported by fluct_shift_kernel
+  const float s0 = shift[i * 3 + 0], s1 = shift[i * 3 + 1], s2 = shift[i * 3 + 2];
+  double m[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const float* p = coords + (size_t)f0 * n_atoms * STRIDE + a * STRIDE;
+  const size_t step = (size_t)n_atoms * STRIDE;
+  int64_t f = f0;
+  for (; f + 4 <= f1; f += 4) {
+    float x[4][3];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      x[u][0] = __ldg(p + u * step + 0); x[u][1] = __ldg(p + u * step + 1); x[u][2] = __ldg(p + u * step + 2);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double d0 = (double)x[u][0] - s0, d1 = (double)x[u][1] - s1, d2 = (double)x[u][2] - s2;
+      m[0] += d0; m[1] += d1; m[2] += d2;
+      m[3] = fma(d0, d0, m[3]); m[4] = fma(d1, d1, m[4]); m[5] = fma(d2, d2, m[5]);
+      m[6] = fma(d0, d1, m[6]); m[7] = fma(d0, d2, m[7]); m[8] = fma(d1, d2, m[8]);
+    }
+    p += 4 * step;
+  }
+  for (; f < f1; ++f) {
+    const double d0 = (double)__ldg(p) - s0, d1 = (double)__ldg(p + 1) - s1, d2 = (double)__ldg(p + 2) - s2;
+    m[0] += d0; m[1] += d1; m[2] += d2;
+    m[3] = fma(d0, d0, m[3]); m[4] = fma(d1, d1, m[4]); m[5] = fma(d2, d2, m[5]);
+    m[6] = fma(d0, d1, m[6]); m[7] = fma(d0, d2, m[7]); m[8] = fma(d1, d2, m[8]);
+    p += step;
+  }
+  double* o = part + ((size_t)g * n_sel + i) * kFluctMoments;
+#pragma unroll
+  for (int e = 0; e < 9; ++e) o[e] = m[e];
+}
+
+__global__ void __launch_bounds__(kFluctThreads) fluct_reduce_kernel(const double* __restrict__ part, int G,
+                                                                     int64_t n_sel, double* __restrict__ acc) {
+  const int64_t i = (int64_t)blockIdx.x * kFluctThreads + threadIdx.x;
+  if (i >= n_sel) return;
+  double m[9];
+  for (int e = 0; e < 9; ++e) m[e] = acc[i * kFluctMoments + e];
+  for (int g = 0; g < G; ++g)
+    for (int e = 0; e < 9; ++e) m[e] += part[((size_t)g * n_sel + i) * kFluctMoments + e];
+  for (int e = 0; e < 9; ++e) acc[i * kFluctMoments + e] = m[e];
+}
+
+// RMSF = sqrt(max(sum_c var_c, 0)) (rms.rs:199-212); ADP = (uxx, uyy, uzz, uxy,
+// uxz, uyz) with the diagonal clamped at 0 (rms.rs:384-406).  Both are
+// invariant under the per-atom shift.
+__global__ void __launch_bounds__(kFluctThreads) fluct_finalize_kernel(const double* __restrict__ acc, int64_t n_sel,
+                                                                       int64_t n_frames, float* __restrict__ rmsf,
+                                                                       float* __restrict__ adp) {
+  const int64_t i = (int64_t)blockIdx.x * kFluctThreads + threadIdx.x;
+  if (i >= n_sel) return;
+  const double* m = acc + i * kFluctMoments;
+  const double inv = 1.0 / (double)n_frames;
+  const double mx = m[0] * inv, my = m[1] * inv, mz = m[2] * inv;
+  const double vx = m[3] * inv - mx * mx, vy = m[4] * inv - my * my, vz = m[5] * inv - mz * mz;
+  if (rmsf) {
+    const double var = vx + vy + vz;
+    rmsf[i] = (float)sqrt(var > 0.0 ? var : 0.0);
+  }
+  if (adp) {
+    float* o = adp + i * 6;
+    o[0] = (float)(vx > 0.0 ? vx : 0.0);
+    o[1] = (float)(vy > 0.0 ? vy : 0.0);
+    o[2] = (float)(vz > 0.0 ? vz : 0.0);
+    o[3] = (float)(m[6] * inv - mx * my);
+    o[4] = (float)(m[7] * inv - mx * mz);
+    o[5] = (float)(m[8] * inv - my * mz);
+  }
+}
+
+// One thread per (frame, group), frame-major.  xf: [n_frames][16] FP64 rows
+// (R row-major, t) or null for the identity (align = false).
+template <int STRIDE>
+__global__ void __launch_bounds__(256) group_rmsd_kernel(const float* __restrict__ coords, int64_t n_frames,
+                                                         int64_t n_atoms, const double* __restrict__ xf,
+                                                         const uint32_t* __restrict__ goff,
+                                                         const uint32_t* __restrict__ gatoms, int64_t n_groups,
+                                                         const float* __restrict__ ref_all, float* __restrict__ out) {
+  const int64_t items = n_frames * n_groups;
+  for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < items; it += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t f = it / n_groups, g = it - f * n_groups;
+    double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, t[3] = {0, 0, 0};
+    if (xf) {
+      const double* x = xf + f * kStatDoubles;
+#pragma unroll
+      for (int e = 0; e < 9; ++e) R[e] = __ldg(x + e);
+      t[0] = __ldg(x + 9); t[1] = __ldg(x + 10); t[2] = __ldg(x + 11);
+    }
+    const float* frame = coords + (size_t)f * n_atoms * STRIDE;
+    const uint32_t k0 = goff[g], k1 = goff[g + 1];
+    double s = 0.0;
+    for (uint32_t k = k0; k < k1; ++k) {
+      const int64_t a = gatoms[k];
+      const double p0 = __ldg(frame + a * STRIDE), p1 = __ldg(frame + a * STRIDE + 1), p2 = __ldg(frame + a * STRIDE + 2);
+      const double d0 = R[0] * p0 + R[1] * p1 + R[2] * p2 + t[0] - (double)__ldg(ref_all + a * 3);
+      const double d1 = R[3] * p0 + R[4] * p1 + R[5] * p2 + t[1] - (double)__ldg(ref_all + a * 3 + 1);
+      const double d2 = R[6] * p0 + R[7] * p1 + R[8] * p2 + t[2] - (double)__ldg(ref_all + a * 3 + 2);
+      s += d0 * d0 + d1 * d1 + d2 * d2;
+    }
+    const double n = k1 > k0 ? (double)(k1 - k0) : 1.0;
+    out[f * n_groups + g] = (float)sqrt(s / n);
+  }
+}
+
+}  // namespace
+
+int fluct_groups(int64_t n_sel, int64_t n_frames, int sm_count) {
+  const int64_t blocks = (n_sel + kFluctThreads - 1) / kFluctThreads;
+  const int64_t want = (int64_t)sm_count * 8;
+  int64_t G = blocks > 0 ? (want + blocks - 1) / blocks : 1;
+  G = std::min<int64_t>(G, std::max<int64_t>(1, n_frames / 16));
+  return (int)std::max<int64_t>(1, std::min<int64_t>(G, 1024));
+}
+
+cudaError_t launch_fluct_shift(const float* coords, int64_t n_atoms, int stride, const uint32_t* sel, int64_t n_sel,
+                               float* shift, int* status, cudaStream_t s) {
+  if (n_sel == 0) return cudaSuccess;
+  const unsigned blocks = (unsigned)((n_sel + kFluctThreads - 1) / kFluctThreads);
+  if (stride == 4) fluct_shift_kernel<4><<<blocks, kFluctThreads, 0, s>>>(coords, n_atoms, sel, n_sel, shift, status);
+  else fluct_shift_kernel<3><<<blocks, kFluctThreads, 0, s>>>(coords, n_atoms, sel, n_sel, shift, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fluct_chunk(const float* coords, int64_t n_frames, int64_t n_atoms, int stride, const uint32_t* sel,
+                               int64_t n_sel, const float* shift, int groups, double* part, double* acc,
+                               cudaStream_t s) {
+  if (n_sel == 0 || n_frames == 0) return cudaSuccess;
+  const unsigned blocks = (unsigned)((n_sel + kFluctThreads - 1) / kFluctThreads);
+  const dim3 grid(blocks, (unsigned)groups);
+  if (stride == 4)
+    fluct_partial_kernel<4><<<grid, kFluctThreads, 0, s>>>(coords, n_frames, n_atoms, sel, n_sel, shift, part);
+  else
+    fluct_partial_kernel<3><<<grid, kFluctThreads, 0, s>>>(coords, n_frames, n_atoms, sel, n_sel, shift, part);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  fluct_reduce_kernel<<<blocks, kFluctThreads, 0, s>>>(part, groups, n_sel, acc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fluct_finalize(const double* acc, int64_t n_sel, int64_t n_frames, float* rmsf, float* adp,
+                                  cudaStream_t s) {
+  if (n_sel == 0) return cudaSuccess;
+  const unsigned blocks = (unsigned)((n_sel + kFluctThreads - 1) / kFluctThreads);
+  fluct_finalize_kernel<<<blocks, kFluctThreads, 0, s>>>(acc, n_sel, n_frames, rmsf, adp);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_group_rmsd(const float* coords, int64_t n_frames, int64_t n_atoms, int stride, const double* xf,
+                              const uint32_t* goff, const uint32_t* gatoms, int64_t n_groups, const float* ref_all,
+                              float* out, int sm_count, cudaStream_t s) {
+  if (n_frames == 0 || n_groups == 0) return cudaSuccess;
+  const int64_t items = n_frames * n_groups;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((items + 255) / 256, (int64_t)sm_count * 16));
+  if (stride == 4)
+    group_rmsd_kernel<4><<<grid, 256, 0, s>>>(coords, n_frames, n_atoms, xf, goff, gatoms, n_groups, ref_all, out);
+  else
+    group_rmsd_kernel<3><<<grid, 256, 0, s>>>(coords, n_frames, n_atoms, xf, goff, gatoms, n_groups, ref_all, out);
+  return cudaGetLastError();
+}
+
+}  // namespace wmd

@@ -24,6 +24,7 @@
 
 #include "../../include/warpmd_rmsd.h"
 #include "batched.h"
+#include "fluct.h"
 #include "pairwise.h"
 #include "superpose.h"
 #include "wmd_internal.h"
@@ -80,6 +81,7 @@ struct wmd_ctx {
   int* status_host = nullptr;  // mapped pinned word the kernels report into
   int* status_dev = nullptr;
   DevBuf partial, refine, refine_count, rot, chunk[2], out_tmp, sel_buf, aux, out_chunk;
+  DevBuf fl_part, fl_acc, fl_shift, g_off, g_atoms, g_ref;  // fluctuations, per-group RMSD
   HostBuf stage[2];
   std::string err;
   wmd::PairwiseWorkspace pw;
@@ -403,7 +405,8 @@ WMD_EXPORT int wmd_destroy(wmd_ctx* ctx) {
   DeviceGuard g(ctx->device);
   cudaDeviceSynchronize();
   for (DevBuf* b : {&ctx->partial, &ctx->refine, &ctx->refine_count, &ctx->rot, &ctx->chunk[0], &ctx->chunk[1], &ctx->out_tmp,
-                    &ctx->sel_buf, &ctx->aux, &ctx->out_chunk, &ctx->b_segs, &ctx->b_yc, &ctx->b_partial, &ctx->b_rot,
+                    &ctx->sel_buf, &ctx->aux, &ctx->out_chunk, &ctx->fl_part, &ctx->fl_acc, &ctx->fl_shift, &ctx->g_off,
+                    &ctx->g_atoms, &ctx->g_ref, &ctx->b_segs, &ctx->b_yc, &ctx->b_partial, &ctx->b_rot,
                     &ctx->b_refine, &ctx->b_count})
     if (b->ptr) cudaFree(b->ptr);
   for (HostBuf* b : {&ctx->stage[0], &ctx->stage[1]})
@@ -658,9 +661,18 @@ static int require_device(wmd_ctx* ctx, const void* p, const char* name) {
 
 // Device-resident frames: statistics, per-frame transforms into dxf32 (if not
 // null) and, when dout is not null, every atom moved into dout.
+// Per-group RMSD run after the transforms of each batch (RmsdPerResPlan).
+struct GroupJob {
+  const uint32_t* goff = nullptr;
+  const uint32_t* gatoms = nullptr;
+  int64_t n_groups = 0;
+  const float* ref_all = nullptr;
+  float* out = nullptr;  // [n_frames of this call][n_groups], device
+};
+
 static int superpose_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames, int64_t n_atoms, int stride,
                             const uint32_t* dsel, const wmd_ref* ref, int norotate, float* dxf32, float* dout,
-                            cudaStream_t s) {
+                            cudaStream_t s, const GroupJob* grp = nullptr) {
   if (n_frames == 0) return WMD_OK;
   wmd::FrameLaunch L = base_launch(ctx, ref, n_atoms, stride, dsel);
   L.align = 1;
@@ -689,7 +701,66 @@ static int superpose_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames
       CU(wmd::launch_superpose_apply(B.coords, nf, n_atoms, stride, xf, dout + (size_t)f0 * n_atoms * 3, ctx->sm_count,
                                      ctx->status_dev, s),
          "superpose apply");
+    if (grp)
+      CU(wmd::launch_group_rmsd(B.coords, nf, n_atoms, stride, xf, grp->goff, grp->gatoms, grp->n_groups, grp->ref_all,
+                                grp->out + f0 * grp->n_groups, ctx->sm_count, s),
+         "per-group rmsd");
   }
+  return WMD_OK;
+}
+
+// Calls fn(device_frames, f0, nf) for consecutive runs of frames: in place for
+// device memory; for host memory through the context's two chunk buffers, the
+// H2D copy of the next chunk overlapping the work on this one.
+template <class Fn>
+static int for_each_chunk(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                          cudaStream_t s, Fn fn) {
+  const Mem cm = classify(coords);
+  if (cm == Mem::Device) return fn(coords, (int64_t)0, n_frames);
+  const size_t frame_bytes = (size_t)n_atoms * stride * sizeof(float);
+  const int64_t chunk = std::max<int64_t>(
+      1, std::min<int64_t>(n_frames, (int64_t)(kChunkBytes / std::max<size_t>(frame_bytes, 1))));
+  int rc;
+  for (int b = 0; b < 2; ++b) {
+    if ((rc = ensure(ctx, ctx->chunk[b], (size_t)chunk * frame_bytes + 16))) return rc;
+    if (cm == Mem::PageableHost && (rc = ensure_host(ctx, ctx->stage[b], (size_t)chunk * frame_bytes + 16))) return rc;
+  }
+  CU(cudaEventRecord(ctx->kern_done[0], s), "event");
+  CU(cudaEventRecord(ctx->kern_done[1], s), "event");
+  CU(cudaEventRecord(ctx->h2d_done[0], ctx->copy_stream), "event");
+  CU(cudaEventRecord(ctx->h2d_done[1], ctx->copy_stream), "event");
+  int64_t k = 0;
+  for (int64_t f0 = 0; f0 < n_frames; f0 += chunk, ++k) {
+    const int b = (int)(k & 1);
+    const int64_t nf = std::min(chunk, n_frames - f0);
+    const size_t bytes = (size_t)nf * frame_bytes;
+    const char* src = reinterpret_cast<const char*>(coords) + (size_t)f0 * frame_bytes;
+    if (cm == Mem::PageableHost) {
+      CU(cudaEventSynchronize(ctx->h2d_done[b]), "staging wait");
+      std::memcpy(ctx->stage[b].ptr, src, bytes);
+      src = static_cast<const char*>(ctx->stage[b].ptr);
+    }
+    CU(cudaStreamWaitEvent(ctx->copy_stream, ctx->kern_done[b], 0), "stream wait");
+    CU(cudaMemcpyAsync(ctx->chunk[b].ptr, src, bytes, cudaMemcpyHostToDevice, ctx->copy_stream), "H2D");
+    CU(cudaEventRecord(ctx->h2d_done[b], ctx->copy_stream), "event");
+    CU(cudaStreamWaitEvent(s, ctx->h2d_done[b], 0), "stream wait");
+    if ((rc = fn(static_cast<const float*>(ctx->chunk[b].ptr), f0, nf))) return rc;
+    CU(cudaEventRecord(ctx->kern_done[b], s), "event");
+  }
+  return WMD_OK;
+}
+
+// A device buffer holding `bytes` of `src` (host or device), or src itself
+// when it already is device memory.
+static int device_copy(wmd_ctx* ctx, DevBuf& b, const void* src, size_t bytes, const void** dptr, cudaStream_t s) {
+  if (classify(src) == Mem::Device) {
+    *dptr = src;
+    return WMD_OK;
+  }
+  int rc = ensure(ctx, b, std::max<size_t>(bytes, 16));
+  if (rc) return rc;
+  CU(cudaMemcpyAsync(b.ptr, src, bytes, cudaMemcpyHostToDevice, s), "upload");
+  *dptr = b.ptr;
   return WMD_OK;
 }
 
@@ -782,6 +853,155 @@ WMD_EXPORT int wmd_superpose(wmd_ctx* ctx, const float* coords, int64_t n_frames
   if (ctx && n_frames > 0 && !out) return set_err(ctx, WMD_ERR_INVALID_ARG, "out is null");
   return superpose_common(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, ref, norotate, out, transforms,
                           static_cast<cudaStream_t>(stream));
+}
+
+// ---------------------------------------------------------------------------
+// fluctuations (RmsfPlan / AtomicFluctPlan / BfactorsPlan / AtomicAdpPlan) and
+// per-group RMSD (RmsdPerResPlan)
+// ---------------------------------------------------------------------------
+
+WMD_EXPORT int wmd_rmsf(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                        const uint32_t* sel, int64_t n_sel, float* rmsf, float* adp, void* stream) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  if (stride != 3 && stride != 4) return set_err(ctx, WMD_ERR_INVALID_ARG, "stride must be 3 or 4 (got %d)", stride);
+  if (n_frames < 0 || n_atoms < 0 || n_sel < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "negative size");
+  if (n_frames > 0 && n_sel > 0 && !coords) return set_err(ctx, WMD_ERR_INVALID_ARG, "coords is null");
+  if (!sel && n_sel > n_atoms)
+    return set_err(ctx, WMD_ERR_MISMATCH, "selection of %lld atoms exceeds the frame's %lld atoms", (long long)n_sel,
+                   (long long)n_atoms);
+  if (n_sel > 0 && !rmsf && !adp) return set_err(ctx, WMD_ERR_INVALID_ARG, "rmsf and adp are both null");
+  DeviceGuard g(ctx->device);
+  int rc = check_status(ctx);
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (n_sel == 0) return WMD_OK;
+  const bool rh = rmsf && is_host(classify(rmsf)), ah = adp && is_host(classify(adp));
+  if (n_frames == 0) {
+    // no frames: RMSF 0 (rms.rs:194-196); the ADP tensor has no rows then
+    if (rmsf) {
+      if (rh) std::fill(rmsf, rmsf + n_sel, 0.f);
+      else CU(cudaMemsetAsync(rmsf, 0, (size_t)n_sel * sizeof(float), s), "memset");
+    }
+    return WMD_OK;
+  }
+  const uint32_t* dsel = nullptr;
+  if ((rc = resolve_sel(ctx, sel, n_sel, n_atoms, &dsel, s))) return rc;
+  const int G = wmd::fluct_groups(n_sel, n_frames, ctx->sm_count);
+  const size_t mom = (size_t)n_sel * wmd::kFluctMoments * sizeof(double);
+  if ((rc = ensure(ctx, ctx->fl_part, mom * (size_t)G)) || (rc = ensure(ctx, ctx->fl_acc, mom)) ||
+      (rc = ensure(ctx, ctx->fl_shift, (size_t)n_sel * 3 * sizeof(float))))
+    return rc;
+  double* acc = static_cast<double*>(ctx->fl_acc.ptr);
+  CU(cudaMemsetAsync(acc, 0, mom, s), "memset");
+  rc = for_each_chunk(ctx, coords, n_frames, n_atoms, stride, s, [&](const float* dc, int64_t f0, int64_t nf) -> int {
+    if (f0 == 0)
+      CU(wmd::launch_fluct_shift(dc, n_atoms, stride, dsel, n_sel, static_cast<float*>(ctx->fl_shift.ptr),
+                                 ctx->status_dev, s),
+         "fluctuation shift");
+    const int Gc = wmd::fluct_groups(n_sel, nf, ctx->sm_count);
+    CU(wmd::launch_fluct_chunk(dc, nf, n_atoms, stride, dsel, n_sel, static_cast<const float*>(ctx->fl_shift.ptr),
+                               std::min(Gc, G), static_cast<double*>(ctx->fl_part.ptr), acc, s),
+       "fluctuation moments");
+    return WMD_OK;
+  });
+  if (rc) return rc;
+  float* drmsf = rmsf;
+  float* dadp = adp;
+  if (rh || ah) {
+    if ((rc = ensure(ctx, ctx->out_tmp, (size_t)n_sel * 7 * sizeof(float)))) return rc;
+    float* tmp = static_cast<float*>(ctx->out_tmp.ptr);
+    if (rh) drmsf = tmp;
+    if (ah) dadp = tmp + n_sel;
+  }
+  CU(wmd::launch_fluct_finalize(acc, n_sel, n_frames, drmsf, dadp, s), "fluctuation finalize");
+  if (rh) CU(cudaMemcpyAsync(rmsf, drmsf, (size_t)n_sel * sizeof(float), cudaMemcpyDeviceToHost, s), "D2H");
+  if (ah) CU(cudaMemcpyAsync(adp, dadp, (size_t)n_sel * 6 * sizeof(float), cudaMemcpyDeviceToHost, s), "D2H");
+  if (rh || ah || is_host(classify(coords))) {
+    CU(cudaStreamSynchronize(s), "synchronize");
+    return check_status(ctx);
+  }
+  return WMD_OK;
+}
+
+WMD_EXPORT int wmd_rmsd_per_group(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                                  const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, const float* ref_all,
+                                  const uint32_t* group_offsets, const uint32_t* group_atoms, int64_t n_groups,
+                                  int align, float* out, void* stream) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  if (stride != 3 && stride != 4) return set_err(ctx, WMD_ERR_INVALID_ARG, "stride must be 3 or 4 (got %d)", stride);
+  if (n_frames < 0 || n_atoms < 0 || n_sel < 0 || n_groups < 0)
+    return set_err(ctx, WMD_ERR_INVALID_ARG, "negative size");
+  if (n_frames > 0 && !coords) return set_err(ctx, WMD_ERR_INVALID_ARG, "coords is null");
+  if (align && !ref) return set_err(ctx, WMD_ERR_INVALID_ARG, "reference is null");
+  if (align && ref->info.w)
+    return set_err(ctx, WMD_ERR_INVALID_ARG, "per-group RMSD superposes without weights; pass an unweighted reference");
+  if (align && n_sel != ref->info.n_sel)
+    return set_err(ctx, WMD_ERR_MISMATCH, "reference has %lld atoms but the selection has %lld",
+                   (long long)ref->info.n_sel, (long long)n_sel);
+  if (!sel && n_sel > n_atoms)
+    return set_err(ctx, WMD_ERR_MISMATCH, "selection of %lld atoms exceeds the frame's %lld atoms", (long long)n_sel,
+                   (long long)n_atoms);
+  if (n_groups > 0 && (!group_offsets || !group_atoms || !ref_all || (n_frames > 0 && !out)))
+    return set_err(ctx, WMD_ERR_INVALID_ARG, "group_offsets, group_atoms, ref_all and out are required");
+  if (n_groups > 0 && (is_host(classify(group_offsets)) != true || is_host(classify(group_atoms)) != true))
+    return set_err(ctx, WMD_ERR_INVALID_ARG, "group_offsets and group_atoms must be host memory");
+  // the groups are validated here, so the kernel reads no index out of range
+  int64_t n_idx = 0;
+  if (n_groups > 0) {
+    if (group_offsets[0] != 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "group_offsets[0] must be 0");
+    for (int64_t gi = 0; gi < n_groups; ++gi)
+      if (group_offsets[gi + 1] < group_offsets[gi])
+        return set_err(ctx, WMD_ERR_INVALID_ARG, "group_offsets must not decrease");
+    n_idx = group_offsets[n_groups];
+    for (int64_t k = 0; k < n_idx; ++k)
+      if ((int64_t)group_atoms[k] >= n_atoms)
+        return set_err(ctx, WMD_ERR_INVALID_ARG, "group atom index %u out of range for %lld atoms", group_atoms[k],
+                       (long long)n_atoms);
+  }
+  DeviceGuard g(ctx->device);
+  int rc = check_status(ctx);
+  if (rc) return rc;
+  if (n_frames == 0 || n_groups == 0) return WMD_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const uint32_t* dsel = nullptr;
+  if (align && (rc = resolve_sel(ctx, sel, n_sel, n_atoms, &dsel, s))) return rc;
+  GroupJob job;
+  const void* p = nullptr;
+  if ((rc = device_copy(ctx, ctx->g_off, group_offsets, (size_t)(n_groups + 1) * 4, &p, s))) return rc;
+  job.goff = static_cast<const uint32_t*>(p);
+  if ((rc = device_copy(ctx, ctx->g_atoms, group_atoms, (size_t)std::max<int64_t>(n_idx, 1) * 4, &p, s))) return rc;
+  job.gatoms = static_cast<const uint32_t*>(p);
+  if ((rc = device_copy(ctx, ctx->g_ref, ref_all, (size_t)n_atoms * 3 * sizeof(float), &p, s))) return rc;
+  job.ref_all = static_cast<const float*>(p);
+  job.n_groups = n_groups;
+  const bool oh = is_host(classify(out));
+  const size_t row = (size_t)n_groups * sizeof(float);
+  rc = for_each_chunk(ctx, coords, n_frames, n_atoms, stride, s, [&](const float* dc, int64_t f0, int64_t nf) -> int {
+    GroupJob jb = job;
+    if (oh) {
+      int r2 = ensure(ctx, ctx->out_chunk, (size_t)nf * row);
+      if (r2) return r2;
+      jb.out = static_cast<float*>(ctx->out_chunk.ptr);
+    } else {
+      jb.out = out + f0 * n_groups;
+    }
+    if (align) {
+      int r2 = superpose_device(ctx, dc, nf, n_atoms, stride, dsel, ref, 0, nullptr, nullptr, s, &jb);
+      if (r2) return r2;
+    } else {
+      CU(wmd::launch_group_rmsd(dc, nf, n_atoms, stride, nullptr, jb.goff, jb.gatoms, n_groups, jb.ref_all, jb.out,
+                                ctx->sm_count, s),
+         "per-group rmsd");
+    }
+    if (oh) CU(cudaMemcpyAsync(out + f0 * n_groups, jb.out, (size_t)nf * row, cudaMemcpyDeviceToHost, s), "D2H");
+    return WMD_OK;
+  });
+  if (rc) return rc;
+  if (oh || is_host(classify(coords))) {
+    CU(cudaStreamSynchronize(s), "synchronize");
+    return check_status(ctx);
+  }
+  return WMD_OK;
 }
 
 WMD_EXPORT int wmd_rmsd_forward(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,

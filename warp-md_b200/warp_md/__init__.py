@@ -21,8 +21,8 @@ __version__ = "0.4.30"
 
 from ._native import WarpMdError  # noqa: F401
 from .core import Selection, System, Trajectory  # noqa: F401
-from .plans import (AlignPlan, PairwiseRmsdPlan, RmsdPlan, RotationMatrixPlan, SuperposePlan,  # noqa: F401
-                    SuperposeTrajectoryPlan)
+from .plans import (AlignPlan, AtomicAdpPlan, AtomicFluctPlan, BfactorsPlan, PairwiseRmsdPlan,  # noqa: F401
+                    RmsdPerResPlan, RmsdPlan, RmsfPlan, RotationMatrixPlan, SuperposePlan, SuperposeTrajectoryPlan)
 from . import synth  # noqa: F401
 
 __rust_cuda_enabled__ = True
@@ -36,4 +36,5 @@ def native_version() -> str:
 
 
 __all__ = ["System", "Selection", "Trajectory", "RmsdPlan", "PairwiseRmsdPlan", "AlignPlan", "RotationMatrixPlan",
-           "SuperposePlan", "SuperposeTrajectoryPlan", "WarpMdError", "synth"]
+           "SuperposePlan", "SuperposeTrajectoryPlan", "RmsfPlan", "AtomicFluctPlan", "BfactorsPlan", "AtomicAdpPlan",
+           "RmsdPerResPlan", "WarpMdError", "synth"]

@@ -39,7 +39,7 @@ EXPORTED = (
     "wmd_create", "wmd_destroy", "wmd_last_error", "wmd_version", "wmd_reference_upload", "wmd_reference_free",
     "wmd_rmsd_frames", "wmd_rmsd_forward", "wmd_rmsd_backward", "wmd_rmsd_covariance", "wmd_pairwise_rmsd",
     "wmd_batched_prepare", "wmd_batched_rmsd", "wmd_batched_layout", "wmd_rmsd_frames_noalloc",
-    "wmd_reference_upload_weighted", "wmd_superpose_transforms", "wmd_superpose",
+    "wmd_reference_upload_weighted", "wmd_superpose_transforms", "wmd_superpose", "wmd_rmsf", "wmd_rmsd_per_group",
 )
 
 
@@ -97,6 +97,8 @@ def load() -> ctypes.CDLL:
         L.wmd_reference_upload_weighted.argtypes = [vp, vp, i64, i32, vp, ctypes.POINTER(vp)]
         L.wmd_superpose_transforms.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, i32, vp, vp]
         L.wmd_superpose.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, i32, vp, vp, vp]
+        L.wmd_rmsf.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, vp]
+        L.wmd_rmsd_per_group.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, vp, vp, i64, i32, vp, vp]
         L.wmd_rmsd_frames_noalloc.argtypes = [vp, i64, i64, i32, vp, i64, i32, vp, vp]
         for name in EXPORTED:
             getattr(L, name).restype = getattr(L, name).restype if name in ("wmd_last_error", "wmd_version") else i32

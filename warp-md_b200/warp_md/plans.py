@@ -312,3 +312,115 @@ class SuperposeTrajectoryPlan:
         return {"coords": out,
                 "box": None if box is None else np.asarray(box, dtype=np.float32).reshape(n, -1)[:, :3],
                 "time_ps": None if time is None else np.asarray(time, dtype=np.float32).reshape(n)}
+
+
+# ---------------------------------------------------------------------------
+# fluctuations and per-residue RMSD
+# ---------------------------------------------------------------------------
+
+def _fluct_run(plan, traj: Trajectory, system: System, device: str, frame_indices, want_adp: bool):
+    dev = parse_device(device)
+    sel = _check_inputs(traj, system, plan.selection)
+    coords = traj.coords
+    sub = frame_subset(coords.shape[0], frame_indices)
+    if sub is not None:
+        coords = np.ascontiguousarray(coords[sub])
+    n_sel = int(sel.size)
+    rmsf = np.zeros(n_sel, np.float32)
+    adp = np.zeros((n_sel, 6), np.float32) if want_adp else None
+    if n_sel == 0 or coords.shape[0] == 0:
+        return rmsf, (np.empty((0, 6), np.float32) if want_adp else None)
+    ctx = N.context(dev)
+    dense = _dense_prefix(sel)
+    sel_arr = None if dense else np.ascontiguousarray(sel, dtype=np.uint32)
+    ctx.check(ctx.lib.wmd_rmsf(ctx.handle, coords.ctypes.data, coords.shape[0], coords.shape[1], 3, N.ptr(sel_arr),
+                               n_sel, rmsf.ctypes.data, None if adp is None else adp.ctypes.data, None))
+    return rmsf, adp
+
+
+class RmsfPlan:
+    """Per-atom root-mean-square fluctuation over frames, float32 [n_sel]
+    (warp_md.RmsfPlan, crates/traj-py/src/geometry.rs; rms.rs:17-218).  No
+    superposition: align the trajectory first (SuperposePlan) when needed."""
+
+    def __init__(self, selection: Selection):
+        self.selection = selection
+
+    def run(self, traj: Trajectory, system: System, chunk_frames: Optional[int] = None, device: str = "auto",
+            frame_indices: Optional[Sequence[int]] = None) -> np.ndarray:
+        return _fluct_run(self, traj, system, device, frame_indices, False)[0]
+
+
+class AtomicFluctPlan(RmsfPlan):
+    """RMSF under its AtomicFluct name (rms.rs:268-300)."""
+
+
+class BfactorsPlan(RmsfPlan):
+    """Pseudo B-factors 8 pi^2 / 3 * rmsf^2 (rms.rs:221-265), float32 [n_sel]."""
+
+    def run(self, traj: Trajectory, system: System, chunk_frames: Optional[int] = None, device: str = "auto",
+            frame_indices: Optional[Sequence[int]] = None) -> np.ndarray:
+        r = super().run(traj, system, chunk_frames, device, frame_indices).astype(np.float64)
+        return (8.0 * np.pi * np.pi / 3.0 * r * r).astype(np.float32)
+
+
+class AtomicAdpPlan:
+    """Per-atom displacement tensors (uxx, uyy, uzz, uxy, uxz, uyz), float32
+    [n_sel, 6] (rms.rs:303-429); no rows when there are no frames."""
+
+    def __init__(self, selection: Selection):
+        self.selection = selection
+
+    def run(self, traj: Trajectory, system: System, chunk_frames: Optional[int] = None, device: str = "auto",
+            frame_indices: Optional[Sequence[int]] = None) -> np.ndarray:
+        return _fluct_run(self, traj, system, device, frame_indices, True)[1]
+
+
+class RmsdPerResPlan:
+    """Per-frame, per-residue RMSD after superposing the selection onto the
+    reference (warp_md.RmsdPerResPlan, rms.rs:431-686).  run() returns
+    (resids int32 [n_res], float32 [frames, n_res]); residues are the
+    selection's resids in ascending order, each with its atoms in selection
+    order."""
+
+    def __init__(self, selection: Selection, reference: str = "topology", align: bool = True):
+        self.selection = selection
+        self.reference_mode = parse_reference(reference)
+        self.align = bool(align)
+
+    def run(self, traj: Trajectory, system: System, chunk_frames: Optional[int] = None, device: str = "auto"):
+        dev = parse_device(device)
+        sel = _check_inputs(traj, system, self.selection)
+        coords = traj.coords
+        resids = system.resids[sel] if sel.size else np.zeros(0, np.int64)
+        order = np.unique(resids)
+        groups = [sel[resids == r] for r in order]
+        n_groups = len(groups)
+        out = np.zeros((coords.shape[0], n_groups), np.float32)
+        resid_arr = order.astype(np.int32)
+        if self.reference_mode == "topology":
+            if system.positions0 is None:
+                raise RuntimeError("mismatch: no topology reference coords")
+            ref_all = system.positions0
+        else:
+            if coords.shape[0] == 0:
+                return resid_arr, out
+            ref_all = coords[0]
+        if coords.shape[0] == 0 or n_groups == 0:
+            return resid_arr, out
+        ref_all = np.ascontiguousarray(ref_all, dtype=np.float32)
+        goff = np.zeros(n_groups + 1, np.uint32)
+        goff[1:] = np.cumsum([g.size for g in groups])
+        gat = np.ascontiguousarray(np.concatenate(groups), dtype=np.uint32)
+        ctx = N.context(dev)
+        r = N.Reference.from_numpy(ctx, ref_all[sel])
+        try:
+            dense = _dense_prefix(sel)
+            sel_arr = None if dense else np.ascontiguousarray(sel, dtype=np.uint32)
+            ctx.check(ctx.lib.wmd_rmsd_per_group(ctx.handle, coords.ctypes.data, coords.shape[0], coords.shape[1], 3,
+                                                 N.ptr(sel_arr), int(sel.size), r.handle, ref_all.ctypes.data,
+                                                 goff.ctypes.data, gat.ctypes.data, n_groups, int(self.align),
+                                                 out.ctypes.data, None))
+        finally:
+            r.close()
+        return resid_arr, out
