@@ -26,6 +26,8 @@ atom-frames/s.  One step = one pass of the per-frame kernel over all frames.
   vs one forward + backward call per trajectory.
 * superpose: 100,000-atom frames x 2,000 frames, mass-weighted 10,000-atom
   selection, transforms + every atom moved (SuperposePlan).
+* fluct: RMSF + ADP over 100,000 atoms x 2,000 frames, and per-residue RMSD
+  of 10,000 residues after superposing a 10,000-atom selection.
 * --gpus N (torchrun): weak scaling, each rank streams its own 10,000 frames;
   no data-path collective (frames are independent).
 """
@@ -470,6 +472,90 @@ def run_superpose(args, ctx, stream, rank):
     return res
 
 
+def run_fluct(args, ctx, stream, rank):
+    """RmsfPlan and RmsdPerResPlan workloads on 100,000-atom frames x 2,000
+    frames (2.4 GB, device-resident): per-atom RMSF + ADP moments over all
+    atoms; per-residue RMSD of 10,000 ten-atom residues after superposing a
+    10,000-atom selection.  Checked against the oracle on a sample."""
+    import numpy as np
+    import torch
+
+    from warp_md import _native as N
+    from warp_md import synth
+
+    n_atoms, F = 100_000, args.fl_frames
+    x, ref = synth.make_trajectory_torch(n_atoms, F, (0.05, 3.0), seed=60 + rank, device="cuda")
+    r = torch.empty(n_atoms, device="cuda")
+    a = torch.empty(n_atoms, 6, device="cuda")
+    peak, _ = _measured_peaks()
+
+    def timed(fn, steps):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def rmsf_step():
+        ctx.check(ctx.lib.wmd_rmsf(ctx.handle, x.data_ptr(), F, n_atoms, 3, None, n_atoms, r.data_ptr(), a.data_ptr(),
+                                   stream.cuda_stream))
+
+    ms_f = timed(rmsf_step, args.fl_steps)
+    # per-residue RMSD: residues of 10 consecutive atoms, every 10th atom selected
+    sel = np.arange(0, n_atoms, 10, dtype=np.uint32)
+    goff = np.arange(0, n_atoms + 1, 10, dtype=np.uint32)
+    gat = np.arange(n_atoms, dtype=np.uint32)
+    n_groups = goff.size - 1
+    ref_h = ref.cpu().numpy()
+    rr = N.Reference.from_numpy(ctx, ref_h[sel])
+    dsel = torch.from_numpy(sel.astype(np.int32)).cuda()
+    groups_ref = N.GroupRef(ctx, ref_h, goff, gat)
+    out = torch.empty(F, n_groups, device="cuda")
+
+    def perres_step():
+        ctx.check(ctx.lib.wmd_rmsd_per_group(ctx.handle, x.data_ptr(), F, n_atoms, 3, dsel.data_ptr(), sel.size,
+                                             rr.handle, groups_ref.handle, 1, out.data_ptr(), stream.cuda_stream))
+
+    ms_p = timed(perres_step, args.fl_steps)
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import oracle
+
+    sample = slice(0, min(F, 64))
+    hx = x[sample].cpu().numpy()
+    keep = np.arange(0, n_atoms, 101)
+    orr, _ = oracle.rmsf(x.cpu().numpy()[:, keep])
+    err_rmsf = float(np.abs(r.cpu().numpy()[keep] - orr).max())
+    groups = [np.arange(g * 10, g * 10 + 10) for g in range(0, n_groups, 97)]
+    want = oracle.rmsd_perres(hx, ref_h, groups, selection=sel, align=True)
+    got = out[sample].cpu().numpy()[:, ::97]
+    err_pr = float(np.abs(got - want).max())
+    alg_f = 12.0 * n_atoms * F
+    alg_p = F * (12.0 * sel.size + 12.0 * n_atoms + 4.0 * n_groups)
+    res = {"rmsf": {"metric": "RMSF atom-frames/s", "unit": "atom-frames/s", "n_atoms": n_atoms, "n_frames": F,
+                    "ms": ms_f, "value": n_atoms * F / (ms_f / 1e3),
+                    "roofline": {"bound": "hbm", "achieved": alg_f / (ms_f / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                                 "frac": alg_f / (ms_f / 1e3) / 1e9 / peak, "note": "12 B per atom-frame"},
+                    "max_abs_err_vs_oracle_A": err_rmsf, "outputs": "RMSF + 6 ADP moments per atom"},
+           "rmsd_perres": {"metric": "per-residue RMSD atom-frames/s", "unit": "atom-frames/s", "n_atoms": n_atoms,
+                           "n_frames": F, "n_residues": n_groups, "n_sel": int(sel.size), "ms": ms_p,
+                           "value": n_atoms * F / (ms_p / 1e3),
+                           "roofline": {"bound": "hbm", "achieved": alg_p / (ms_p / 1e3) / 1e9, "peak": peak,
+                                        "unit": "GB/s", "frac": alg_p / (ms_p / 1e3) / 1e9 / peak,
+                                        "note": "12 B per selected atom-frame + 12 B per atom-frame + 4 B per "
+                                                "residue-frame"},
+                           "max_abs_err_vs_oracle_A": err_pr}}
+    rr.close()
+    groups_ref.close()
+    del x, r, a, out, dsel
+    torch.cuda.empty_cache()
+    return res
+
+
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
@@ -634,6 +720,9 @@ def run_ours(args):
     superpose = None
     if not args.skip_superpose:
         superpose = run_superpose(args, ctx, stream, rank)
+    fluct = None
+    if not args.skip_fluct:
+        fluct = run_fluct(args, ctx, stream, rank)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -656,6 +745,7 @@ def run_ours(args):
             "differentiable": differentiable,
             "batched_uneven": batched,
             "superpose": superpose,
+            "fluct": fluct,
         }
         print(json.dumps(line), flush=True)
     r.close()
@@ -691,6 +781,9 @@ def main():
     ap.add_argument("--sp-frames", type=int, default=2000)
     ap.add_argument("--sp-steps", type=int, default=5)
     ap.add_argument("--sp-e2e-frames", type=int, default=500)
+    ap.add_argument("--skip-fluct", action="store_true")
+    ap.add_argument("--fl-frames", type=int, default=2000)
+    ap.add_argument("--fl-steps", type=int, default=5)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

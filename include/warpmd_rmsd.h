@@ -210,17 +210,25 @@ int wmd_superpose(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n
 int wmd_rmsf(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride, const uint32_t* sel,
              int64_t n_sel, float* rmsf, float* adp, void* stream);
 
+/* Groups of atoms (RmsdPerResPlan's residues) with the reference coordinates
+ * of every atom, uploaded once: group g is group_atoms[group_offsets[g] ..
+ * group_offsets[g + 1]) (atom indices into the frame), ref_all is
+ * [n_atoms][stride] (3 or 4).  All may be host or device memory; the indices
+ * are validated here.  Free with wmd_group_ref_free. */
+typedef struct wmd_group_ref wmd_group_ref;
+int wmd_group_ref_upload(wmd_ctx* ctx, const float* ref_all, int64_t n_atoms, int stride,
+                         const uint32_t* group_offsets, const uint32_t* group_atoms, int64_t n_groups,
+                         wmd_group_ref** out);
+int wmd_group_ref_free(wmd_ctx* ctx, wmd_group_ref* groups);
+
 /* RmsdPerResPlan: per frame, the selection is superposed onto `ref` (the
  * selected reference atoms, unweighted Kabsch) when align != 0, and for every
- * group g (a residue) out[f][g] = sqrt(mean over the group's atoms a of
- * |R x_a + t - ref_all[a]|^2); align == 0 compares raw coordinates.  Groups
- * are given by group_offsets[n_groups + 1] into group_atoms (atom indices into
- * the frame), both host memory; ref_all [n_atoms][3] is the reference for
- * every atom (host or device).  An empty group gives 0.  out is float32
- * [n_frames][n_groups], host or device. */
+ * group g out[f][g] = sqrt(mean over the group's atoms a of
+ * |R x_a + t - ref_all[a]|^2); align == 0 compares raw coordinates (`ref` may
+ * then be NULL).  An empty group gives 0.  out is float32 [n_frames][n_groups],
+ * host or device; coords host or device. */
 int wmd_rmsd_per_group(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
-                       const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, const float* ref_all,
-                       const uint32_t* group_offsets, const uint32_t* group_atoms, int64_t n_groups, int align,
+                       const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, const wmd_group_ref* groups, int align,
                        float* out, void* stream);
 
 /* Per-frame aligned RMSD for callers that cannot allocate memory.  No

@@ -148,16 +148,14 @@ def test_rmsd_per_residue_matches_oracle():
                 np.testing.assert_allclose(got, want, rtol=0, atol=1e-5, err_msg=f"{expr} {mode} {align}")
 
 
-def test_rmsd_per_group_validates_groups():
+def test_group_ref_validates_groups():
     from warp_md import _native as N
 
     ctx = N.context(0)
-    fr, ref = synth.make_trajectory(20, 2, 0.5, 3)
-    r = N.Reference.from_numpy(ctx, ref)
-    out = np.empty((2, 2), np.float32)
+    _, ref = synth.make_trajectory(20, 2, 0.5, 3)
     goff = np.array([0, 3, 5], np.uint32)
     bad = np.array([0, 1, 2, 3, 20], np.uint32)  # 20 is out of range
-    rc = ctx.lib.wmd_rmsd_per_group(ctx.handle, fr.ctypes.data, 2, 20, 3, None, 20, r.handle, ref.ctypes.data,
-                                    goff.ctypes.data, bad.ctypes.data, 2, 1, out.ctypes.data, None)
-    assert rc == N.WMD_ERR_INVALID_ARG
-    r.close()
+    with pytest.raises(N.WarpMdError):
+        N.GroupRef(ctx, ref, goff, bad)
+    with pytest.raises(N.WarpMdError):
+        N.GroupRef(ctx, ref, np.array([0, 3, 2], np.uint32), bad[:3])

@@ -17,8 +17,8 @@
 //   * fluct_finalize_kernel turns the moments into RMSF and the ADP tensor.
 //
 // Per-group RMSD.  Per frame, the selection's transform (R, t) comes from the
-// superposition path; per (frame, group) a thread sums |R x + t - y|^2 over the
-// group's atoms against the all-atom reference (rms.rs:633-671) in FP64.
+// superposition path; |R x + t - y|^2 against the all-atom reference is summed
+// per group in FP64 (rms.rs:633-671), see group_rmsd_kernel.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -130,37 +130,93 @@ __global__ void __launch_bounds__(kFluctThreads) fluct_finalize_kernel(const dou
   }
 }
 
-// One thread per (frame, group), frame-major.  xf: [n_frames][16] FP64 rows
-// (R row-major, t) or null for the identity (align = false).
-template <int STRIDE>
-__global__ void __launch_bounds__(256) group_rmsd_kernel(const float* __restrict__ coords, int64_t n_frames,
+// Per-group RMSD.  Groups are contiguous ranges of the concatenated atom list
+// and are packed, in order, into blocks of at most kGroupTile list positions
+// (a larger group gets a block of its own, walked in tiles).  A CTA takes a
+// (frame, block) item: its threads compute |R x + t - y|^2 for consecutive list
+// positions -- coalesced loads when a residue's atoms are consecutive -- into
+// shared memory, then one thread per group adds its range in list order (the
+// order of the reference's loop), so results are deterministic.
+constexpr int kGroupTile = 2048;
+
+// CONTIG: the concatenated atom list is a run of consecutive atoms (list
+// position q is atom contig_base + q), so no index load precedes the
+// coordinate loads.
+template <int STRIDE, bool CONTIG>
+__global__ void __launch_bounds__(256, 4) group_rmsd_kernel(const float* __restrict__ coords, int64_t n_frames,
                                                          int64_t n_atoms, const double* __restrict__ xf,
                                                          const uint32_t* __restrict__ goff,
-                                                         const uint32_t* __restrict__ gatoms, int64_t n_groups,
-                                                         const float* __restrict__ ref_all, float* __restrict__ out) {
-  const int64_t items = n_frames * n_groups;
-  for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < items; it += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t f = it / n_groups, g = it - f * n_groups;
-    double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, t[3] = {0, 0, 0};
-    if (xf) {
-      const double* x = xf + f * kStatDoubles;
-#pragma unroll
-      for (int e = 0; e < 9; ++e) R[e] = __ldg(x + e);
-      t[0] = __ldg(x + 9); t[1] = __ldg(x + 10); t[2] = __ldg(x + 11);
-    }
+                                                         const uint32_t* __restrict__ gatoms, int64_t contig_base,
+                                                         const uint32_t* __restrict__ blocks, int64_t n_blocks,
+                                                         int64_t n_groups, const float* __restrict__ ref_all,
+                                                         float* __restrict__ out) {
+  __shared__ double sq[kGroupTile];
+  __shared__ double rt[12];
+  const int tid = threadIdx.x;
+  const int64_t items = n_frames * n_blocks;
+  for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
+    const int64_t f = it / n_blocks, b = it - f * n_blocks;
+    const uint32_t g0 = blocks[b], g1 = blocks[b + 1];
+    const uint32_t p0 = goff[g0], p1 = goff[g1];
+    if (tid < 12) rt[tid] = xf ? __ldg(xf + f * kStatDoubles + tid) : ((tid == 0 || tid == 4 || tid == 8) ? 1.0 : 0.0);
+    __syncthreads();
     const float* frame = coords + (size_t)f * n_atoms * STRIDE;
-    const uint32_t k0 = goff[g], k1 = goff[g + 1];
-    double s = 0.0;
-    for (uint32_t k = k0; k < k1; ++k) {
-      const int64_t a = gatoms[k];
-      const double p0 = __ldg(frame + a * STRIDE), p1 = __ldg(frame + a * STRIDE + 1), p2 = __ldg(frame + a * STRIDE + 2);
-      const double d0 = R[0] * p0 + R[1] * p1 + R[2] * p2 + t[0] - (double)__ldg(ref_all + a * 3);
-      const double d1 = R[3] * p0 + R[4] * p1 + R[5] * p2 + t[1] - (double)__ldg(ref_all + a * 3 + 1);
-      const double d2 = R[6] * p0 + R[7] * p1 + R[8] * p2 + t[2] - (double)__ldg(ref_all + a * 3 + 2);
-      s += d0 * d0 + d1 * d1 + d2 * d2;
+    // a block spans several tiles only when it is one group larger than a tile
+    double big = 0.0;
+    for (uint32_t q0 = p0; q0 < p1; q0 += kGroupTile) {
+      const uint32_t q1 = min(p1, q0 + (uint32_t)kGroupTile);
+      {
+        double R[9], t[3];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) R[e] = rt[e];
+        t[0] = rt[9]; t[1] = rt[10]; t[2] = rt[11];
+        // 4 positions per thread per pass: all loads issued before any use
+        for (uint32_t qb = q0; qb < q1; qb += 4 * 256) {
+          float xv[4][3], yv[4][3];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const uint32_t q = qb + tid + u * 256;
+            if (q < q1) {
+              const int64_t a = CONTIG ? contig_base + q : (int64_t)__ldg(gatoms + q);
+              xv[u][0] = __ldg(frame + a * STRIDE); xv[u][1] = __ldg(frame + a * STRIDE + 1);
+              xv[u][2] = __ldg(frame + a * STRIDE + 2);
+              yv[u][0] = __ldg(ref_all + a * 3); yv[u][1] = __ldg(ref_all + a * 3 + 1);
+              yv[u][2] = __ldg(ref_all + a * 3 + 2);
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const uint32_t q = qb + tid + u * 256;
+            if (q < q1) {
+              const double x0 = xv[u][0], x1 = xv[u][1], x2 = xv[u][2];
+              const double d0 = R[0] * x0 + R[1] * x1 + R[2] * x2 + t[0] - (double)yv[u][0];
+              const double d1 = R[3] * x0 + R[4] * x1 + R[5] * x2 + t[1] - (double)yv[u][1];
+              const double d2 = R[6] * x0 + R[7] * x1 + R[8] * x2 + t[2] - (double)yv[u][2];
+              sq[q - q0] = d0 * d0 + d1 * d1 + d2 * d2;
+            }
+          }
+        }
+      }
+      __syncthreads();
+      if (g1 - g0 == 1 && p1 - p0 > (uint32_t)kGroupTile) {
+        // one large group: thread 0 adds the tile in list order
+        if (tid == 0)
+          for (uint32_t q = q0; q < q1; ++q) big += sq[q - q0];
+      } else {
+        for (uint32_t g = g0 + tid; g < g1; g += 256) {
+          const uint32_t a0 = goff[g], a1 = goff[g + 1];
+          double acc = 0.0;
+          for (uint32_t q = a0; q < a1; ++q) acc += sq[q - q0];
+          out[f * n_groups + g] = (float)sqrt(acc / (a1 > a0 ? (double)(a1 - a0) : 1.0));
+        }
+      }
+      __syncthreads();
     }
-    const double n = k1 > k0 ? (double)(k1 - k0) : 1.0;
-    out[f * n_groups + g] = (float)sqrt(s / n);
+    if (g1 - g0 == 1 && p1 - p0 > (uint32_t)kGroupTile && tid == 0)
+      out[f * n_groups + g0] = (float)sqrt(big / (double)(p1 - p0));
+    if (p1 == p0)  // blocks of empty groups only
+      for (uint32_t g = g0 + tid; g < g1; g += 256) out[f * n_groups + g] = 0.f;
+    __syncthreads();  // rt is rewritten by the next item
   }
 }
 
@@ -207,16 +263,41 @@ cudaError_t launch_fluct_finalize(const double* acc, int64_t n_sel, int64_t n_fr
   return cudaGetLastError();
 }
 
+int group_blocks(const uint32_t* goff, int64_t n_groups, uint32_t* blocks) {
+  // greedy, in order: a block ends before the group that would take it past
+  // kGroupTile positions or kGroupTile groups
+  int64_t nb = 0;
+  blocks[0] = 0;
+  int64_t g = 0;
+  while (g < n_groups) {
+    const uint32_t start = goff[g];
+    int64_t h = g + 1;
+    while (h < n_groups && goff[h + 1] - start <= (uint32_t)kGroupTile && h - g < kGroupTile) ++h;
+    blocks[++nb] = (uint32_t)h;
+    g = h;
+  }
+  return (int)nb;
+}
+
 cudaError_t launch_group_rmsd(const float* coords, int64_t n_frames, int64_t n_atoms, int stride, const double* xf,
-                              const uint32_t* goff, const uint32_t* gatoms, int64_t n_groups, const float* ref_all,
+                              const uint32_t* goff, const uint32_t* gatoms, int64_t contig_base,
+                              const uint32_t* blocks, int64_t n_blocks, int64_t n_groups, const float* ref_all,
                               float* out, int sm_count, cudaStream_t s) {
   if (n_frames == 0 || n_groups == 0) return cudaSuccess;
-  const int64_t items = n_frames * n_groups;
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((items + 255) / 256, (int64_t)sm_count * 16));
-  if (stride == 4)
-    group_rmsd_kernel<4><<<grid, 256, 0, s>>>(coords, n_frames, n_atoms, xf, goff, gatoms, n_groups, ref_all, out);
-  else
-    group_rmsd_kernel<3><<<grid, 256, 0, s>>>(coords, n_frames, n_atoms, xf, goff, gatoms, n_groups, ref_all, out);
+  const int64_t items = n_frames * n_blocks;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)sm_count * 8));
+#define WMD_GROUP_LAUNCH(ST, CG)                                                                                 \
+  group_rmsd_kernel<ST, CG><<<grid, 256, 0, s>>>(coords, n_frames, n_atoms, xf, goff, gatoms, contig_base, blocks, \
+                                                 n_blocks, n_groups, ref_all, out)
+  const bool contig = contig_base >= 0;
+  if (stride == 4) {
+    if (contig) WMD_GROUP_LAUNCH(4, true);
+    else WMD_GROUP_LAUNCH(4, false);
+  } else {
+    if (contig) WMD_GROUP_LAUNCH(3, true);
+    else WMD_GROUP_LAUNCH(3, false);
+  }
+#undef WMD_GROUP_LAUNCH
   return cudaGetLastError();
 }
 

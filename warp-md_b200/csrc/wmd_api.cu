@@ -72,6 +72,16 @@ struct wmd_ref {
   wmd::RefInfo info;
 };
 
+struct wmd_group_ref {
+  void* mem = nullptr;  // one allocation: offsets, atoms, blocks, reference
+  uint32_t* goff = nullptr;
+  uint32_t* gatoms = nullptr;
+  uint32_t* blocks = nullptr;
+  float* ref_all = nullptr;
+  int64_t n_atoms = 0, n_groups = 0, n_blocks = 0;
+  int64_t contig_base = -1;  // >= 0 when group_atoms[q] == contig_base + q
+};
+
 struct wmd_ctx {
   int device = 0;
   int sm_count = 0;
@@ -81,7 +91,7 @@ struct wmd_ctx {
   int* status_host = nullptr;  // mapped pinned word the kernels report into
   int* status_dev = nullptr;
   DevBuf partial, refine, refine_count, rot, chunk[2], out_tmp, sel_buf, aux, out_chunk;
-  DevBuf fl_part, fl_acc, fl_shift, g_off, g_atoms, g_ref;  // fluctuations, per-group RMSD
+  DevBuf fl_part, fl_acc, fl_shift;  // fluctuations, per-group RMSD
   HostBuf stage[2];
   std::string err;
   wmd::PairwiseWorkspace pw;
@@ -405,8 +415,7 @@ WMD_EXPORT int wmd_destroy(wmd_ctx* ctx) {
   DeviceGuard g(ctx->device);
   cudaDeviceSynchronize();
   for (DevBuf* b : {&ctx->partial, &ctx->refine, &ctx->refine_count, &ctx->rot, &ctx->chunk[0], &ctx->chunk[1], &ctx->out_tmp,
-                    &ctx->sel_buf, &ctx->aux, &ctx->out_chunk, &ctx->fl_part, &ctx->fl_acc, &ctx->fl_shift, &ctx->g_off,
-                    &ctx->g_atoms, &ctx->g_ref, &ctx->b_segs, &ctx->b_yc, &ctx->b_partial, &ctx->b_rot,
+                    &ctx->sel_buf, &ctx->aux, &ctx->out_chunk, &ctx->fl_part, &ctx->fl_acc, &ctx->fl_shift, &ctx->b_segs, &ctx->b_yc, &ctx->b_partial, &ctx->b_rot,
                     &ctx->b_refine, &ctx->b_count})
     if (b->ptr) cudaFree(b->ptr);
   for (HostBuf* b : {&ctx->stage[0], &ctx->stage[1]})
@@ -665,6 +674,9 @@ static int require_device(wmd_ctx* ctx, const void* p, const char* name) {
 struct GroupJob {
   const uint32_t* goff = nullptr;
   const uint32_t* gatoms = nullptr;
+  const uint32_t* blocks = nullptr;
+  int64_t n_blocks = 0;
+  int64_t contig_base = -1;
   int64_t n_groups = 0;
   const float* ref_all = nullptr;
   float* out = nullptr;  // [n_frames of this call][n_groups], device
@@ -702,7 +714,8 @@ static int superpose_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames
                                      ctx->status_dev, s),
          "superpose apply");
     if (grp)
-      CU(wmd::launch_group_rmsd(B.coords, nf, n_atoms, stride, xf, grp->goff, grp->gatoms, grp->n_groups, grp->ref_all,
+      CU(wmd::launch_group_rmsd(B.coords, nf, n_atoms, stride, xf, grp->goff, grp->gatoms, grp->contig_base,
+                                grp->blocks, grp->n_blocks, grp->n_groups, grp->ref_all,
                                 grp->out + f0 * grp->n_groups, ctx->sm_count, s),
          "per-group rmsd");
   }
@@ -750,19 +763,6 @@ static int for_each_chunk(wmd_ctx* ctx, const float* coords, int64_t n_frames, i
   return WMD_OK;
 }
 
-// A device buffer holding `bytes` of `src` (host or device), or src itself
-// when it already is device memory.
-static int device_copy(wmd_ctx* ctx, DevBuf& b, const void* src, size_t bytes, const void** dptr, cudaStream_t s) {
-  if (classify(src) == Mem::Device) {
-    *dptr = src;
-    return WMD_OK;
-  }
-  int rc = ensure(ctx, b, std::max<size_t>(bytes, 16));
-  if (rc) return rc;
-  CU(cudaMemcpyAsync(b.ptr, src, bytes, cudaMemcpyHostToDevice, s), "upload");
-  *dptr = b.ptr;
-  return WMD_OK;
-}
 
 static int superpose_common(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
                             const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, int norotate, float* out,
@@ -923,15 +923,117 @@ WMD_EXPORT int wmd_rmsf(wmd_ctx* ctx, const float* coords, int64_t n_frames, int
   return WMD_OK;
 }
 
+WMD_EXPORT int wmd_group_ref_upload(wmd_ctx* ctx, const float* ref_all, int64_t n_atoms, int stride,
+                                    const uint32_t* group_offsets, const uint32_t* group_atoms, int64_t n_groups,
+                                    wmd_group_ref** out) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  if (!out) return set_err(ctx, WMD_ERR_INVALID_ARG, "out is null");
+  *out = nullptr;
+  if (stride != 3 && stride != 4) return set_err(ctx, WMD_ERR_INVALID_ARG, "stride must be 3 or 4 (got %d)", stride);
+  if (n_atoms < 0 || n_groups < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "negative size");
+  if (n_groups > 0 && (!group_offsets || !group_atoms || (n_atoms > 0 && !ref_all)))
+    return set_err(ctx, WMD_ERR_INVALID_ARG, "ref_all, group_offsets and group_atoms are required");
+  DeviceGuard g(ctx->device);
+  // host copies of everything, validated here once so the kernels read no
+  // index out of range
+  std::vector<uint32_t> off((size_t)n_groups + 1, 0), atoms;
+  std::vector<float> ref((size_t)n_atoms * 3);
+  if (n_groups > 0) {
+    if (classify(group_offsets) == Mem::Device)
+      CU(cudaMemcpy(off.data(), group_offsets, off.size() * 4, cudaMemcpyDeviceToHost), "download");
+    else
+      std::memcpy(off.data(), group_offsets, off.size() * 4);
+    if (off[0] != 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "group_offsets[0] must be 0");
+    for (int64_t gi = 0; gi < n_groups; ++gi)
+      if (off[gi + 1] < off[gi]) return set_err(ctx, WMD_ERR_INVALID_ARG, "group_offsets must not decrease");
+    atoms.resize(off[n_groups]);
+    if (!atoms.empty()) {
+      if (classify(group_atoms) == Mem::Device)
+        CU(cudaMemcpy(atoms.data(), group_atoms, atoms.size() * 4, cudaMemcpyDeviceToHost), "download");
+      else
+        std::memcpy(atoms.data(), group_atoms, atoms.size() * 4);
+    }
+    for (uint32_t a : atoms)
+      if ((int64_t)a >= n_atoms)
+        return set_err(ctx, WMD_ERR_INVALID_ARG, "group atom index %u out of range for %lld atoms", a,
+                       (long long)n_atoms);
+  }
+  if (n_atoms > 0 && ref_all) {
+    std::vector<float> raw((size_t)n_atoms * stride);
+    if (classify(ref_all) == Mem::Device)
+      CU(cudaMemcpy(raw.data(), ref_all, raw.size() * 4, cudaMemcpyDeviceToHost), "download");
+    else
+      std::memcpy(raw.data(), ref_all, raw.size() * 4);
+    for (int64_t a = 0; a < n_atoms; ++a)
+      for (int c = 0; c < 3; ++c) ref[a * 3 + c] = raw[a * stride + c];
+  }
+  std::vector<uint32_t> blocks((size_t)n_groups + 1, 0);
+  const int nb = n_groups > 0 ? wmd::group_blocks(off.data(), n_groups, blocks.data()) : 0;
+  wmd_group_ref* r = new wmd_group_ref();
+  if (!atoms.empty()) {
+    bool contig = true;
+    for (size_t q = 0; q < atoms.size() && contig; ++q) contig = atoms[q] == atoms[0] + q;
+    if (contig) r->contig_base = atoms[0];
+  }
+  r->n_atoms = n_atoms;
+  r->n_groups = n_groups;
+  r->n_blocks = nb;
+  size_t total = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = total;
+    total += (bytes + 255) & ~size_t(255);
+    return at;
+  };
+  const size_t o_off = take(off.size() * 4), o_atoms = take(std::max<size_t>(atoms.size(), 1) * 4),
+               o_blocks = take(((size_t)nb + 1) * 4), o_ref = take(std::max<size_t>(ref.size(), 1) * 4);
+  cudaError_t e = cudaMalloc(&r->mem, total);
+  if (e != cudaSuccess) {
+    delete r;
+    cudaGetLastError();
+    return set_err(ctx, WMD_ERR_OOM, "cuda driver error: group allocation failed: %s", cudaGetErrorString(e));
+  }
+  char* base = static_cast<char*>(r->mem);
+  r->goff = reinterpret_cast<uint32_t*>(base + o_off);
+  r->gatoms = reinterpret_cast<uint32_t*>(base + o_atoms);
+  r->blocks = reinterpret_cast<uint32_t*>(base + o_blocks);
+  r->ref_all = reinterpret_cast<float*>(base + o_ref);
+  e = cudaMemcpy(r->goff, off.data(), off.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !atoms.empty()) e = cudaMemcpy(r->gatoms, atoms.data(), atoms.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(r->blocks, blocks.data(), ((size_t)nb + 1) * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !ref.empty()) e = cudaMemcpy(r->ref_all, ref.data(), ref.size() * 4, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(r->mem);
+    delete r;
+    return cuda_err(ctx, e, "upload groups");
+  }
+  *out = r;
+  return WMD_OK;
+}
+
+WMD_EXPORT int wmd_group_ref_free(wmd_ctx* ctx, wmd_group_ref* groups) {
+  if (!groups) return WMD_OK;
+  if (ctx) {
+    DeviceGuard g(ctx->device);
+    cudaFree(groups->mem);
+  } else {
+    cudaFree(groups->mem);
+  }
+  delete groups;
+  return WMD_OK;
+}
+
 WMD_EXPORT int wmd_rmsd_per_group(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
-                                  const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, const float* ref_all,
-                                  const uint32_t* group_offsets, const uint32_t* group_atoms, int64_t n_groups,
+                                  const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, const wmd_group_ref* groups,
                                   int align, float* out, void* stream) {
   if (!ctx) return WMD_ERR_INVALID_ARG;
   if (stride != 3 && stride != 4) return set_err(ctx, WMD_ERR_INVALID_ARG, "stride must be 3 or 4 (got %d)", stride);
-  if (n_frames < 0 || n_atoms < 0 || n_sel < 0 || n_groups < 0)
-    return set_err(ctx, WMD_ERR_INVALID_ARG, "negative size");
+  if (n_frames < 0 || n_atoms < 0 || n_sel < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "negative size");
+  if (!groups) return set_err(ctx, WMD_ERR_INVALID_ARG, "groups is null");
+  if (groups->n_atoms != n_atoms)
+    return set_err(ctx, WMD_ERR_MISMATCH, "groups were made for %lld atoms but frames have %lld",
+                   (long long)groups->n_atoms, (long long)n_atoms);
   if (n_frames > 0 && !coords) return set_err(ctx, WMD_ERR_INVALID_ARG, "coords is null");
+  if (n_frames > 0 && groups->n_groups > 0 && !out) return set_err(ctx, WMD_ERR_INVALID_ARG, "out is null");
   if (align && !ref) return set_err(ctx, WMD_ERR_INVALID_ARG, "reference is null");
   if (align && ref->info.w)
     return set_err(ctx, WMD_ERR_INVALID_ARG, "per-group RMSD superposes without weights; pass an unweighted reference");
@@ -941,39 +1043,22 @@ WMD_EXPORT int wmd_rmsd_per_group(wmd_ctx* ctx, const float* coords, int64_t n_f
   if (!sel && n_sel > n_atoms)
     return set_err(ctx, WMD_ERR_MISMATCH, "selection of %lld atoms exceeds the frame's %lld atoms", (long long)n_sel,
                    (long long)n_atoms);
-  if (n_groups > 0 && (!group_offsets || !group_atoms || !ref_all || (n_frames > 0 && !out)))
-    return set_err(ctx, WMD_ERR_INVALID_ARG, "group_offsets, group_atoms, ref_all and out are required");
-  if (n_groups > 0 && (is_host(classify(group_offsets)) != true || is_host(classify(group_atoms)) != true))
-    return set_err(ctx, WMD_ERR_INVALID_ARG, "group_offsets and group_atoms must be host memory");
-  // the groups are validated here, so the kernel reads no index out of range
-  int64_t n_idx = 0;
-  if (n_groups > 0) {
-    if (group_offsets[0] != 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "group_offsets[0] must be 0");
-    for (int64_t gi = 0; gi < n_groups; ++gi)
-      if (group_offsets[gi + 1] < group_offsets[gi])
-        return set_err(ctx, WMD_ERR_INVALID_ARG, "group_offsets must not decrease");
-    n_idx = group_offsets[n_groups];
-    for (int64_t k = 0; k < n_idx; ++k)
-      if ((int64_t)group_atoms[k] >= n_atoms)
-        return set_err(ctx, WMD_ERR_INVALID_ARG, "group atom index %u out of range for %lld atoms", group_atoms[k],
-                       (long long)n_atoms);
-  }
   DeviceGuard g(ctx->device);
   int rc = check_status(ctx);
   if (rc) return rc;
+  const int64_t n_groups = groups->n_groups;
   if (n_frames == 0 || n_groups == 0) return WMD_OK;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const uint32_t* dsel = nullptr;
   if (align && (rc = resolve_sel(ctx, sel, n_sel, n_atoms, &dsel, s))) return rc;
   GroupJob job;
-  const void* p = nullptr;
-  if ((rc = device_copy(ctx, ctx->g_off, group_offsets, (size_t)(n_groups + 1) * 4, &p, s))) return rc;
-  job.goff = static_cast<const uint32_t*>(p);
-  if ((rc = device_copy(ctx, ctx->g_atoms, group_atoms, (size_t)std::max<int64_t>(n_idx, 1) * 4, &p, s))) return rc;
-  job.gatoms = static_cast<const uint32_t*>(p);
-  if ((rc = device_copy(ctx, ctx->g_ref, ref_all, (size_t)n_atoms * 3 * sizeof(float), &p, s))) return rc;
-  job.ref_all = static_cast<const float*>(p);
+  job.goff = groups->goff;
+  job.gatoms = groups->gatoms;
+  job.blocks = groups->blocks;
+  job.n_blocks = groups->n_blocks;
+  job.contig_base = groups->contig_base;
   job.n_groups = n_groups;
+  job.ref_all = groups->ref_all;
   const bool oh = is_host(classify(out));
   const size_t row = (size_t)n_groups * sizeof(float);
   rc = for_each_chunk(ctx, coords, n_frames, n_atoms, stride, s, [&](const float* dc, int64_t f0, int64_t nf) -> int {
@@ -989,8 +1074,8 @@ WMD_EXPORT int wmd_rmsd_per_group(wmd_ctx* ctx, const float* coords, int64_t n_f
       int r2 = superpose_device(ctx, dc, nf, n_atoms, stride, dsel, ref, 0, nullptr, nullptr, s, &jb);
       if (r2) return r2;
     } else {
-      CU(wmd::launch_group_rmsd(dc, nf, n_atoms, stride, nullptr, jb.goff, jb.gatoms, n_groups, jb.ref_all, jb.out,
-                                ctx->sm_count, s),
+      CU(wmd::launch_group_rmsd(dc, nf, n_atoms, stride, nullptr, jb.goff, jb.gatoms, jb.contig_base, jb.blocks,
+                                jb.n_blocks, n_groups, jb.ref_all, jb.out, ctx->sm_count, s),
          "per-group rmsd");
     }
     if (oh) CU(cudaMemcpyAsync(out + f0 * n_groups, jb.out, (size_t)nf * row, cudaMemcpyDeviceToHost, s), "D2H");

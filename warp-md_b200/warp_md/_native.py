@@ -40,6 +40,7 @@ EXPORTED = (
     "wmd_rmsd_frames", "wmd_rmsd_forward", "wmd_rmsd_backward", "wmd_rmsd_covariance", "wmd_pairwise_rmsd",
     "wmd_batched_prepare", "wmd_batched_rmsd", "wmd_batched_layout", "wmd_rmsd_frames_noalloc",
     "wmd_reference_upload_weighted", "wmd_superpose_transforms", "wmd_superpose", "wmd_rmsf", "wmd_rmsd_per_group",
+    "wmd_group_ref_upload", "wmd_group_ref_free",
 )
 
 
@@ -98,7 +99,9 @@ def load() -> ctypes.CDLL:
         L.wmd_superpose_transforms.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, i32, vp, vp]
         L.wmd_superpose.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, i32, vp, vp, vp]
         L.wmd_rmsf.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, vp]
-        L.wmd_rmsd_per_group.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, vp, vp, i64, i32, vp, vp]
+        L.wmd_rmsd_per_group.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, i32, vp, vp]
+        L.wmd_group_ref_upload.argtypes = [vp, vp, i64, i32, vp, vp, i64, ctypes.POINTER(vp)]
+        L.wmd_group_ref_free.argtypes = [vp, vp]
         L.wmd_rmsd_frames_noalloc.argtypes = [vp, i64, i64, i32, vp, i64, i32, vp, vp]
         for name in EXPORTED:
             getattr(L, name).restype = getattr(L, name).restype if name in ("wmd_last_error", "wmd_version") else i32
@@ -168,6 +171,32 @@ class Reference:
     def close(self) -> None:
         if getattr(self, "handle", None) and self.ctx.handle:
             self.ctx.lib.wmd_reference_free(self.ctx.handle, self.handle)
+        self.handle = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GroupRef:
+    """Atom groups with the all-atom reference (wmd_group_ref)."""
+
+    def __init__(self, ctx: Context, ref_all: np.ndarray, offsets: np.ndarray, atoms: np.ndarray):
+        self.ctx = ctx
+        r = np.ascontiguousarray(ref_all, dtype=np.float32)
+        off = np.ascontiguousarray(offsets, dtype=np.uint32)
+        at = np.ascontiguousarray(atoms, dtype=np.uint32) if len(atoms) else np.zeros(1, np.uint32)
+        self.n_groups = off.size - 1
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.wmd_group_ref_upload(ctx.handle, r.ctypes.data, r.shape[0], r.shape[1], off.ctypes.data,
+                                               at.ctypes.data, self.n_groups, ctypes.byref(h)))
+        self.handle = h
+
+    def close(self) -> None:
+        if getattr(self, "handle", None) and self.ctx.handle:
+            self.ctx.lib.wmd_group_ref_free(self.ctx.handle, self.handle)
         self.handle = None
 
     def __del__(self):  # pragma: no cover

@@ -414,13 +414,14 @@ class RmsdPerResPlan:
         gat = np.ascontiguousarray(np.concatenate(groups), dtype=np.uint32)
         ctx = N.context(dev)
         r = N.Reference.from_numpy(ctx, ref_all[sel])
+        groups_ref = N.GroupRef(ctx, ref_all, goff, gat)
         try:
             dense = _dense_prefix(sel)
             sel_arr = None if dense else np.ascontiguousarray(sel, dtype=np.uint32)
             ctx.check(ctx.lib.wmd_rmsd_per_group(ctx.handle, coords.ctypes.data, coords.shape[0], coords.shape[1], 3,
-                                                 N.ptr(sel_arr), int(sel.size), r.handle, ref_all.ctypes.data,
-                                                 goff.ctypes.data, gat.ctypes.data, n_groups, int(self.align),
-                                                 out.ctypes.data, None))
+                                                 N.ptr(sel_arr), int(sel.size), r.handle, groups_ref.handle,
+                                                 int(self.align), out.ctypes.data, None))
         finally:
+            groups_ref.close()
             r.close()
         return resid_arr, out
