@@ -231,6 +231,39 @@ int wmd_rmsd_per_group(wmd_ctx* ctx, const float* coords, int64_t n_frames, int6
                        const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, const wmd_group_ref* groups, int align,
                        float* out, void* stream);
 
+/* ---- Clustering (TrajectoryClusterPlan, method "dbscan":
+ *      crates/traj-engine/src/plans/analysis/clustering.rs:160-190, 269-383) ---- */
+
+/* DBSCAN over the all-pairs RMSD matrix of the frames (wmd_pairwise_rmsd with
+ * metric rms and the given mode; WMD_MODE_FP64 reproduces the reference's
+ * matrix to the last float32 bit in practice).  The result is the reference's
+ * sequential DBSCAN:
+ *   labels[f]   cluster id, or -1 for noise (int32 [n_frames]);
+ *   sizes[c], centroids[c]  members per cluster and the member with the
+ *               smallest summed distance to its cluster (ties: lowest index);
+ *               both need room for n_frames entries, *n_clusters are written.
+ * eps <= 0 is WMD_ERR_INVALID_ARG, an empty selection WMD_ERR_MISMATCH; a
+ * min_samples below 1 counts as 1.  The matrix (n_frames^2 float32) lives in
+ * the context.  Outputs may be host or device memory; the call synchronizes. */
+int wmd_cluster_dbscan(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                       const uint32_t* sel, int64_t n_sel, int mode, float eps, int64_t min_samples, int32_t* labels,
+                       uint32_t* centroids, uint32_t* sizes, int64_t* n_clusters, void* stream);
+
+/* k-means (TrajectoryClusterPlan, method "kmeans": clustering.rs:191-205,
+ * 376-548): every frame's selection superposed onto frame 0's (unweighted
+ * Kabsch) gives an FP64 feature vector; centers start at the first n_clusters
+ * of a xorshift64 Fisher-Yates shuffle seeded with `seed` (0 -> a fixed
+ * constant), Lloyd iterations stop after max_iter (at least 1) or once no
+ * center moves more than tol; empty clusters are reseeded from the same
+ * generator.  Outputs: labels int32 [n_frames]; sizes and centroids (the
+ * member nearest its center) for *n_out = min(max(n_clusters, 1), n_frames)
+ * clusters.  Distances and sums follow the reference's order, so labels are
+ * the reference's up to exact FP64 ties.  Synchronizes. */
+int wmd_cluster_kmeans(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                       const uint32_t* sel, int64_t n_sel, int64_t n_clusters, int64_t max_iter, float tol,
+                       uint64_t seed, int32_t* labels, uint32_t* centroids, uint32_t* sizes, int64_t* n_out,
+                       void* stream);
+
 /* Per-frame aligned RMSD for callers that cannot allocate memory.  No
  * counterpart in the reference.  Everything else in this header needs a
  * wmd_ctx and a wmd_ref, which allocate device and pinned memory; this call

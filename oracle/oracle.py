@@ -57,6 +57,11 @@ def lib():
         L.wmdo_rmsf.restype = None
         L.wmdo_rmsd_perres.argtypes = [_vp, _i64, _i64, _int, _vp, _i64, _vp, _vp, _vp, _i64, _int, _vp]
         L.wmdo_rmsd_perres.restype = None
+        L.wmdo_dbscan.argtypes = [_vp, _i64, ctypes.c_double, _i64, _vp, _vp, _vp]
+        L.wmdo_dbscan.restype = _i64
+        L.wmdo_kmeans.argtypes = [_vp, _i64, _i64, _int, _vp, _i64, _i64, _i64, ctypes.c_double, ctypes.c_uint64, _vp,
+                                  _vp, _vp]
+        L.wmdo_kmeans.restype = _i64
         _lib = L
     return _lib
 
@@ -182,3 +187,31 @@ def rmsd_perres(coords, ref_all, groups, selection=None, align: bool = True):
     lib().wmdo_rmsd_perres(_ptr(c), c.shape[0], c.shape[1], stride, _ptr(sel), n_sel, _ptr(ref), _ptr(goff),
                            _ptr(gat), len(groups), int(bool(align)), _ptr(out))
     return out
+
+
+def dbscan(dist, eps: float, min_samples: int):
+    """TrajectoryClusterPlan's DBSCAN over an (n, n) float32 matrix; eps is
+    taken as float32 then widened, as the plan stores it.  Returns (labels
+    int32, centroids uint32, sizes uint32)."""
+    d = np.ascontiguousarray(dist, dtype=np.float32)
+    n = d.shape[0]
+    labels = np.empty(n, np.int32)
+    cent = np.empty(max(n, 1), np.uint32)
+    sizes = np.empty(max(n, 1), np.uint32)
+    k = lib().wmdo_dbscan(_ptr(d), n, float(np.float32(eps)), int(min_samples), _ptr(labels), _ptr(cent), _ptr(sizes))
+    return labels, cent[:k].copy(), sizes[:k].copy()
+
+
+def kmeans(coords, selection=None, n_clusters=8, max_iter=100, tol=1e-4, seed=0):
+    """TrajectoryClusterPlan's k-means.  tol is taken as float32 then widened,
+    as the plan stores it.  Returns (labels, centroids, sizes)."""
+    c, stride = _coords(coords)
+    sel = None if selection is None else np.ascontiguousarray(selection, dtype=np.uint32)
+    n_sel = sel.shape[0] if sel is not None else c.shape[1]
+    n = c.shape[0]
+    labels = np.empty(max(n, 1), np.int32)
+    cent = np.empty(max(n, 1), np.uint32)
+    sizes = np.empty(max(n, 1), np.uint32)
+    k = lib().wmdo_kmeans(_ptr(c), n, c.shape[1], stride, _ptr(sel), n_sel, int(n_clusters), int(max_iter),
+                          float(np.float32(tol)), int(seed), _ptr(labels), _ptr(cent), _ptr(sizes))
+    return labels[:n].copy(), cent[:k].copy(), sizes[:k].copy()

@@ -21,6 +21,8 @@
  *       geometry_math.rs:202-300): weighted Kabsch, t = cy - R cx, R x + t.
  *   - RmsfPlan / AtomicAdpPlan / RmsdPerResPlan
  *       crates/traj-engine/src/plans/geometry/rms.rs:110-218, 345-429, 633-671.
+ *   - TrajectoryClusterPlan (DBSCAN, k-means)
+ *       crates/traj-engine/src/plans/analysis/clustering.rs:269-548.
  *
  * The SVD in the reference is nalgebra 0.32.6 (Cargo.lock:792-793), which is
  * not vendored.  Here it is a one-sided Jacobi SVD (Hestenes 1958; Demmel &
@@ -568,4 +570,198 @@ WMDO_API void wmdo_rmsd_perres(const float* coords, int64_t n_frames, int64_t n_
       out[f * n_groups + g] = sqrt(sum / n);
     }
   }
+}
+
+/* ------------------------------------------------------------------ */
+/* Clustering (TrajectoryClusterPlan)                                  */
+/* ------------------------------------------------------------------ */
+
+/* dbscan_cluster (crates/traj-engine/src/plans/analysis/clustering.rs:
+ * 269-374) over a full n x n float32 distance matrix (tri_get reads the
+ * triangle; d(i,i) = 0): sequential DBSCAN with a FIFO queue, then per cluster
+ * the member with the smallest FP64 sum of distances (first such index).
+ * Returns the number of clusters; centroids/sizes need room for n entries. */
+WMDO_API int64_t wmdo_dbscan(const float* D, int64_t n, double eps, int64_t min_samples, int32_t* labels,
+                             uint32_t* centroids, uint32_t* sizes) {
+  const int32_t UNCLASSIFIED = -2, NOISE = -1;
+  if (min_samples < 1) min_samples = 1;
+  unsigned char* visited = (unsigned char*)calloc((size_t)n, 1);
+  unsigned char* queued = (unsigned char*)malloc((size_t)n);
+  int64_t* neigh = (int64_t*)malloc(sizeof(int64_t) * (size_t)n);
+  int64_t* queue = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n + 1));  /* each point queued once per cluster */
+  for (int64_t i = 0; i < n; ++i) labels[i] = UNCLASSIFIED;
+  int32_t cluster = 0;
+#define WMDO_D(a, b) ((a) == (b) ? 0.0 : (double)D[(a) * n + (b)])
+  for (int64_t i = 0; i < n; ++i) {
+    if (visited[i]) continue;
+    visited[i] = 1;
+    int64_t nn = 0;
+    for (int64_t j = 0; j < n; ++j)
+      if (WMDO_D(i, j) <= eps) neigh[nn++] = j;
+    if (nn < min_samples) {
+      labels[i] = NOISE;
+      continue;
+    }
+    labels[i] = cluster;
+    memset(queued, 0, (size_t)n);
+    int64_t qh = 0, qt = 0;
+    for (int64_t k = 0; k < nn; ++k)
+      if (neigh[k] != i && !queued[neigh[k]]) {
+        queue[qt++] = neigh[k];
+        queued[neigh[k]] = 1;
+      }
+    while (qh < qt) {
+      const int64_t p = queue[qh++];
+      if (!visited[p]) {
+        visited[p] = 1;
+        int64_t m = 0;
+        for (int64_t j = 0; j < n; ++j)
+          if (WMDO_D(p, j) <= eps) neigh[m++] = j;
+        if (m >= min_samples)
+          for (int64_t k = 0; k < m; ++k)
+            if (!queued[neigh[k]]) {
+              queue[qt++] = neigh[k];
+              queued[neigh[k]] = 1;
+            }
+      }
+      if (labels[p] == UNCLASSIFIED || labels[p] == NOISE) labels[p] = cluster;
+    }
+    ++cluster;
+  }
+  for (int32_t c = 0; c < cluster; ++c) {
+    uint32_t size = 0, best = 0;
+    double best_sum = INFINITY;
+    int first = 1;
+    for (int64_t a = 0; a < n; ++a) {
+      if (labels[a] != c) continue;
+      ++size;
+      if (first) { best = (uint32_t)a; first = 0; }
+      double s = 0.0;
+      for (int64_t b = 0; b < n; ++b)
+        if (labels[b] == c) s += WMDO_D(a, b);
+      if (s < best_sum) { best_sum = s; best = (uint32_t)a; }
+    }
+    sizes[c] = size;
+    centroids[c] = best;
+  }
+#undef WMDO_D
+  free(visited); free(queued); free(neigh); free(queue);
+  return cluster;
+}
+
+static uint64_t xorshift64_step(uint64_t* state) {
+  uint64_t x = *state;
+  if (x == 0) x = 0x9E3779B97F4A7C15ull;
+  x ^= x << 13;
+  x ^= x >> 7;
+  x ^= x << 17;
+  *state = x;
+  return x;
+}
+
+static double sq_dist(const double* a, const double* b, int64_t m) {
+  double s = 0.0;
+  for (int64_t i = 0; i < m; ++i) {
+    const double d = a[i] - b[i];
+    s += d * d;
+  }
+  return s;
+}
+
+/* build_aligned_features + kmeans_cluster (clustering.rs:376-548): features
+ * are the selection's coordinates after the unweighted Kabsch onto frame 0's,
+ * R (x - cx) + cy, in FP64; Lloyd iterations with the xorshift64 shuffle and
+ * reseeding.  Returns the number of clusters K. */
+WMDO_API int64_t wmdo_kmeans(const float* coords, int64_t n_frames, int64_t n_atoms, int stride, const uint32_t* sel,
+                             int64_t n_sel, int64_t n_clusters, int64_t max_iter, double tol, uint64_t seed,
+                             int32_t* labels, uint32_t* centroids, uint32_t* sizes) {
+  const int64_t N = n_frames, nf = n_sel * 3;
+  if (N == 0) return 0;
+  int64_t K = n_clusters < 1 ? 1 : (n_clusters > N ? N : n_clusters);
+  if (max_iter < 1) max_iter = 1;
+  if (tol < 0) tol = 0;
+  double* feat = (double*)malloc(sizeof(double) * (size_t)(N * nf));
+  const float* ref = coords;  /* frame 0 */
+  for (int64_t f = 0; f < N; ++f) {
+    const float* fr = coords + f * n_atoms * stride;
+    double cx[3] = {0, 0, 0}, cy[3] = {0, 0, 0};
+    for (int64_t i = 0; i < n_sel; ++i) {
+      const int64_t a = sel ? (int64_t)sel[i] : i;
+      for (int c = 0; c < 3; ++c) { cx[c] += fr[a * stride + c]; cy[c] += ref[a * stride + c]; }
+    }
+    for (int c = 0; c < 3; ++c) { cx[c] /= (double)n_sel; cy[c] /= (double)n_sel; }
+    double h[9] = {0}, r[9];
+    for (int64_t i = 0; i < n_sel; ++i) {
+      const int64_t a = sel ? (int64_t)sel[i] : i;
+      double p[3], q[3];
+      for (int c = 0; c < 3; ++c) { p[c] = fr[a * stride + c] - cx[c]; q[c] = ref[a * stride + c] - cy[c]; }
+      for (int u = 0; u < 3; ++u)
+        for (int v = 0; v < 3; ++v) h[u * 3 + v] += p[u] * q[v];
+    }
+    kabsch_rotation(h, r, NULL);
+    for (int64_t i = 0; i < n_sel; ++i) {
+      const int64_t a = sel ? (int64_t)sel[i] : i;
+      double p[3];
+      for (int c = 0; c < 3; ++c) p[c] = fr[a * stride + c] - cx[c];
+      for (int u = 0; u < 3; ++u)
+        feat[(f * n_sel + i) * 3 + u] = r[u * 3] * p[0] + r[u * 3 + 1] * p[1] + r[u * 3 + 2] * p[2] + cy[u];
+    }
+  }
+  uint64_t state = seed == 0 ? 0x9E3779B97F4A7C15ull : seed;
+  int64_t* order = (int64_t*)malloc(sizeof(int64_t) * (size_t)N);
+  for (int64_t i = 0; i < N; ++i) order[i] = i;
+  for (int64_t i = N - 1; i >= 1; --i) {
+    const int64_t j = (int64_t)(xorshift64_step(&state) % (uint64_t)(i + 1));
+    const int64_t t = order[i]; order[i] = order[j]; order[j] = t;
+  }
+  double* centers = (double*)malloc(sizeof(double) * (size_t)(K * nf));
+  double* sums = (double*)malloc(sizeof(double) * (size_t)(K * nf));
+  double* nc = (double*)malloc(sizeof(double) * (size_t)nf);
+  int64_t* counts = (int64_t*)malloc(sizeof(int64_t) * (size_t)K);
+  for (int64_t c = 0; c < K; ++c) memcpy(centers + c * nf, feat + order[c] * nf, sizeof(double) * (size_t)nf);
+  for (int64_t it = 0; it < max_iter; ++it) {
+    memset(counts, 0, sizeof(int64_t) * (size_t)K);
+    memset(sums, 0, sizeof(double) * (size_t)(K * nf));
+    for (int64_t i = 0; i < N; ++i) {
+      int64_t best = 0;
+      double bd = INFINITY;
+      for (int64_t c = 0; c < K; ++c) {
+        const double d = sq_dist(feat + i * nf, centers + c * nf, nf);
+        if (d < bd) { bd = d; best = c; }
+      }
+      labels[i] = (int32_t)best;
+      counts[best] += 1;
+      for (int64_t k = 0; k < nf; ++k) sums[best * nf + k] += feat[i * nf + k];
+    }
+    double max_shift = 0.0;
+    for (int64_t c = 0; c < K; ++c) {
+      if (counts[c] == 0) {
+        const int64_t idx = (int64_t)(xorshift64_step(&state) % (uint64_t)N);
+        const double sh = sqrt(sq_dist(centers + c * nf, feat + idx * nf, nf));
+        if (sh > max_shift) max_shift = sh;
+        memcpy(centers + c * nf, feat + idx * nf, sizeof(double) * (size_t)nf);
+        continue;
+      }
+      const double inv = 1.0 / (double)counts[c];
+      for (int64_t k = 0; k < nf; ++k) nc[k] = sums[c * nf + k] * inv;
+      const double sh = sqrt(sq_dist(centers + c * nf, nc, nf));
+      if (sh > max_shift) max_shift = sh;
+      memcpy(centers + c * nf, nc, sizeof(double) * (size_t)nf);
+    }
+    if (max_shift <= tol) break;
+  }
+  for (int64_t c = 0; c < K; ++c) {
+    uint32_t cnt = 0, best_idx = 0;
+    double bd = INFINITY;
+    for (int64_t i = 0; i < N; ++i) {
+      if (labels[i] != c) continue;
+      ++cnt;
+      const double d = sq_dist(feat + i * nf, centers + c * nf, nf);
+      if (d < bd) { bd = d; best_idx = (uint32_t)i; }
+    }
+    sizes[c] = cnt;
+    centroids[c] = best_idx;
+  }
+  free(feat); free(order); free(centers); free(sums); free(nc); free(counts);
+  return K;
 }

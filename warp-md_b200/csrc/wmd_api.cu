@@ -24,6 +24,7 @@
 
 #include "../../include/warpmd_rmsd.h"
 #include "batched.h"
+#include "cluster.h"
 #include "fluct.h"
 #include "pairwise.h"
 #include "superpose.h"
@@ -91,7 +92,8 @@ struct wmd_ctx {
   int* status_host = nullptr;  // mapped pinned word the kernels report into
   int* status_dev = nullptr;
   DevBuf partial, refine, refine_count, rot, chunk[2], out_tmp, sel_buf, aux, out_chunk;
-  DevBuf fl_part, fl_acc, fl_shift;  // fluctuations, per-group RMSD
+  DevBuf fl_part, fl_acc, fl_shift;
+  DevBuf cl_mat, cl_scratch, cl_out, km_feat, km_xf, km_work;  // clustering  // fluctuations, per-group RMSD
   HostBuf stage[2];
   std::string err;
   wmd::PairwiseWorkspace pw;
@@ -415,7 +417,8 @@ WMD_EXPORT int wmd_destroy(wmd_ctx* ctx) {
   DeviceGuard g(ctx->device);
   cudaDeviceSynchronize();
   for (DevBuf* b : {&ctx->partial, &ctx->refine, &ctx->refine_count, &ctx->rot, &ctx->chunk[0], &ctx->chunk[1], &ctx->out_tmp,
-                    &ctx->sel_buf, &ctx->aux, &ctx->out_chunk, &ctx->fl_part, &ctx->fl_acc, &ctx->fl_shift, &ctx->b_segs, &ctx->b_yc, &ctx->b_partial, &ctx->b_rot,
+                    &ctx->sel_buf, &ctx->aux, &ctx->out_chunk, &ctx->fl_part, &ctx->fl_acc, &ctx->fl_shift, &ctx->cl_mat, &ctx->cl_scratch,
+                    &ctx->cl_out, &ctx->km_feat, &ctx->km_xf, &ctx->km_work, &ctx->b_segs, &ctx->b_yc, &ctx->b_partial, &ctx->b_rot,
                     &ctx->b_refine, &ctx->b_count})
     if (b->ptr) cudaFree(b->ptr);
   for (HostBuf* b : {&ctx->stage[0], &ctx->stage[1]})
@@ -684,7 +687,7 @@ struct GroupJob {
 
 static int superpose_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames, int64_t n_atoms, int stride,
                             const uint32_t* dsel, const wmd_ref* ref, int norotate, float* dxf32, float* dout,
-                            cudaStream_t s, const GroupJob* grp = nullptr) {
+                            cudaStream_t s, const GroupJob* grp = nullptr, double* xf64_out = nullptr) {
   if (n_frames == 0) return WMD_OK;
   wmd::FrameLaunch L = base_launch(ctx, ref, n_atoms, stride, dsel);
   L.align = 1;
@@ -709,6 +712,10 @@ static int superpose_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames
     }
     double* xf = static_cast<double*>(ctx->rot.ptr);
     CU(wmd::launch_superpose_finalize(B, norotate, xf, dxf32 ? dxf32 + f0 * 12 : nullptr, s), "superpose transforms");
+    if (xf64_out)
+      CU(cudaMemcpyAsync(xf64_out + f0 * wmd::kStatDoubles, xf, (size_t)nf * wmd::kStatDoubles * sizeof(double),
+                         cudaMemcpyDeviceToDevice, s),
+         "copy transforms");
     if (dout)
       CU(wmd::launch_superpose_apply(B.coords, nf, n_atoms, stride, xf, dout + (size_t)f0 * n_atoms * 3, ctx->sm_count,
                                      ctx->status_dev, s),
@@ -1182,6 +1189,203 @@ WMD_EXPORT int wmd_pairwise_rmsd(wmd_ctx* ctx, const float* coords, int64_t n_fr
     return check_status(ctx);
   }
   return WMD_OK;
+}
+
+WMD_EXPORT int wmd_cluster_dbscan(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                                  const uint32_t* sel, int64_t n_sel, int mode, float eps, int64_t min_samples,
+                                  int32_t* labels, uint32_t* centroids, uint32_t* sizes, int64_t* n_clusters,
+                                  void* stream) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  if (!n_clusters) return set_err(ctx, WMD_ERR_INVALID_ARG, "n_clusters is null");
+  *n_clusters = 0;
+  if (!(eps > 0.0f)) return set_err(ctx, WMD_ERR_INVALID_ARG, "parse error: trajectory_cluster DBSCAN eps must be > 0");
+  if (n_sel == 0) return set_err(ctx, WMD_ERR_MISMATCH, "mismatch: trajectory_cluster requires a non-empty selection");
+  if (n_frames < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "negative size");
+  if (n_frames > (int64_t)0x7fffffff) return set_err(ctx, WMD_ERR_UNSUPPORTED, "too many frames for clustering");
+  if (n_frames > 0 && (!labels || !centroids || !sizes))
+    return set_err(ctx, WMD_ERR_INVALID_ARG, "labels, centroids and sizes are required");
+  if (n_frames == 0) return WMD_OK;
+  DeviceGuard g(ctx->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc;
+  const size_t mat = (size_t)n_frames * n_frames * sizeof(float);
+  if ((rc = ensure(ctx, ctx->cl_mat, mat))) return rc;
+  rc = wmd_pairwise_rmsd(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, WMD_PAIR_RMS, mode,
+                         static_cast<float*>(ctx->cl_mat.ptr), stream);
+  if (rc) return rc;
+  const size_t n = (size_t)n_frames;
+  // device outputs: labels [n], sizes [n], centroids [n], cluster count, best sums [n]
+  if ((rc = ensure(ctx, ctx->cl_scratch, wmd::dbscan_scratch_bytes(n_frames))) ||
+      (rc = ensure(ctx, ctx->cl_out, n * (4 + 4 + 4 + 8) + 16)))
+    return rc;
+  char* o = static_cast<char*>(ctx->cl_out.ptr);
+  int* dlabels = reinterpret_cast<int*>(o);
+  unsigned* dsizes = reinterpret_cast<unsigned*>(o + n * 4);
+  unsigned* dcent = reinterpret_cast<unsigned*>(o + n * 8);
+  int* dcount = reinterpret_cast<int*>(o + n * 12);
+  unsigned long long* dbest = reinterpret_cast<unsigned long long*>(o + ((n * 12 + 4 + 7) & ~size_t(7)));
+  const float* D = static_cast<const float*>(ctx->cl_mat.ptr);
+  CU(wmd::dbscan_run(D, n_frames, (double)eps, std::max<int64_t>(1, min_samples), ctx->cl_scratch.ptr, dlabels, dcount,
+                     ctx->status_dev, ctx->sm_count, s),
+     "dbscan");
+  int count = 0;
+  CU(cudaMemcpyAsync(&count, dcount, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
+  CU(cudaStreamSynchronize(s), "synchronize");
+  if ((rc = check_status(ctx))) return rc;
+  CU(wmd::dbscan_summary(D, n_frames, dlabels, count, ctx->cl_scratch.ptr, dsizes, dcent, dbest, s), "dbscan summary");
+  auto put = [&](void* dst, const void* src, size_t bytes) -> int {
+    if (!bytes) return WMD_OK;
+    CU(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s), "copy out");
+    return WMD_OK;
+  };
+  if ((rc = put(labels, dlabels, n * 4)) || (rc = put(sizes, dsizes, (size_t)count * 4)) ||
+      (rc = put(centroids, dcent, (size_t)count * 4)))
+    return rc;
+  CU(cudaStreamSynchronize(s), "synchronize");
+  *n_clusters = count;
+  return check_status(ctx);
+}
+
+static uint64_t km_xorshift64(uint64_t* state) {
+  // xorshift64 as clustering.rs:536-547 writes it (zero state replaced)
+  uint64_t x = *state;
+  if (x == 0) x = 0x9E3779B97F4A7C15ull;
+  x ^= x << 13;
+  x ^= x >> 7;
+  x ^= x << 17;
+  *state = x;
+  return x;
+}
+
+WMD_EXPORT int wmd_cluster_kmeans(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                                  const uint32_t* sel, int64_t n_sel, int64_t n_clusters, int64_t max_iter, float tol,
+                                  uint64_t seed, int32_t* labels, uint32_t* centroids, uint32_t* sizes,
+                                  int64_t* n_out, void* stream) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  if (!n_out) return set_err(ctx, WMD_ERR_INVALID_ARG, "n_out is null");
+  *n_out = 0;
+  if (n_sel == 0) return set_err(ctx, WMD_ERR_MISMATCH, "mismatch: trajectory_cluster requires a non-empty selection");
+  if (stride != 3 && stride != 4) return set_err(ctx, WMD_ERR_INVALID_ARG, "stride must be 3 or 4 (got %d)", stride);
+  if (n_frames < 0 || n_atoms < 0 || n_sel < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "negative size");
+  if (n_frames > (int64_t)0x7fffffff) return set_err(ctx, WMD_ERR_UNSUPPORTED, "too many frames for clustering");
+  if (!sel && n_sel > n_atoms)
+    return set_err(ctx, WMD_ERR_MISMATCH, "selection of %lld atoms exceeds the frame's %lld atoms", (long long)n_sel,
+                   (long long)n_atoms);
+  if (n_frames > 0 && (!coords || !labels || !centroids || !sizes))
+    return set_err(ctx, WMD_ERR_INVALID_ARG, "coords, labels, centroids and sizes are required");
+  if (n_frames == 0) return WMD_OK;
+  DeviceGuard g(ctx->device);
+  int rc = check_status(ctx);
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int64_t N = n_frames, K = std::min<int64_t>(std::max<int64_t>(n_clusters, 1), N);
+  const int64_t iters = std::max<int64_t>(max_iter, 1);
+  const double tolerance = std::max(0.0, (double)tol);
+  const int64_t nf = n_sel * 3;
+  // frame 0's selected atoms are the reference (build_aligned_features,
+  // clustering.rs:376-386)
+  std::vector<float> f0((size_t)n_atoms * stride), ref((size_t)n_sel * 3);
+  CU(cudaMemcpy(f0.data(), coords, f0.size() * sizeof(float), cudaMemcpyDefault), "read frame 0");
+  std::vector<uint32_t> hsel;
+  if (sel) {
+    hsel.resize((size_t)n_sel);
+    CU(cudaMemcpy(hsel.data(), sel, hsel.size() * 4, cudaMemcpyDefault), "read selection");
+    for (uint32_t a : hsel)
+      if ((int64_t)a >= n_atoms)
+        return set_err(ctx, WMD_ERR_INVALID_ARG, "selection index %u out of range for %lld atoms", a, (long long)n_atoms);
+  }
+  for (int64_t a = 0; a < n_sel; ++a) {
+    const int64_t atom = sel ? hsel[a] : a;
+    for (int c = 0; c < 3; ++c) ref[a * 3 + c] = f0[atom * stride + c];
+  }
+  wmd_ref* r = nullptr;
+  if ((rc = reference_upload(ctx, ref.data(), n_sel, 3, nullptr, &r))) return rc;
+  struct RefFree {
+    wmd_ctx* c;
+    wmd_ref* r;
+    ~RefFree() { wmd_reference_free(c, r); }
+  } ref_guard{ctx, r};
+  const uint32_t* dsel = nullptr;
+  if ((rc = resolve_sel(ctx, sel, n_sel, n_atoms, &dsel, s))) return rc;
+  const size_t feat_bytes = (size_t)N * nf * sizeof(double);
+  if ((rc = ensure(ctx, ctx->km_feat, feat_bytes)) ||
+      (rc = ensure(ctx, ctx->km_xf, (size_t)N * wmd::kStatDoubles * sizeof(double))))
+    return rc;
+  double* feat = static_cast<double*>(ctx->km_feat.ptr);
+  double* xf_all = static_cast<double*>(ctx->km_xf.ptr);
+  rc = for_each_chunk(ctx, coords, n_frames, n_atoms, stride, s, [&](const float* dc, int64_t fb, int64_t nfr) -> int {
+    int r2 = superpose_device(ctx, dc, nfr, n_atoms, stride, dsel, r, 0, nullptr, nullptr, s, nullptr,
+                              xf_all + fb * wmd::kStatDoubles);
+    if (r2) return r2;
+    CU(wmd::kmeans_features(dc, nfr, n_atoms, stride, dsel, n_sel, xf_all + fb * wmd::kStatDoubles,
+                            feat + (size_t)fb * nf, ctx->sm_count, s),
+       "kmeans features");
+    return WMD_OK;
+  });
+  if (rc) return rc;
+  // work: centers x2, sums [K][nf]; labels [N]; counts [K]; reseed [K]; shift [K];
+  // dist [N]; best [K]; sizes, centroids [K]
+  auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+  const size_t cbytes = al((size_t)K * nf * 8);
+  const size_t total = 3 * cbytes + al(N * 4) + al(K * 4) + al(K * 8) + al(K * 8) + al(N * 8) + al(K * 8) +
+                       2 * al(K * 4);
+  if ((rc = ensure(ctx, ctx->km_work, total))) return rc;
+  char* w = static_cast<char*>(ctx->km_work.ptr);
+  double* cen_a = reinterpret_cast<double*>(w);
+  double* cen_b = reinterpret_cast<double*>(w + cbytes);
+  double* sums = reinterpret_cast<double*>(w + 2 * cbytes);
+  size_t off = 3 * cbytes;
+  auto take = [&](size_t b) { char* p = w + off; off += al(b); return p; };
+  int* dlabels = reinterpret_cast<int*>(take(N * 4));
+  int* dcounts = reinterpret_cast<int*>(take(K * 4));
+  int64_t* dreseed = reinterpret_cast<int64_t*>(take(K * 8));
+  double* dshift = reinterpret_cast<double*>(take(K * 8));
+  double* ddist = reinterpret_cast<double*>(take(N * 8));
+  unsigned long long* dbest = reinterpret_cast<unsigned long long*>(take(K * 8));
+  unsigned* dsizes = reinterpret_cast<unsigned*>(take(K * 4));
+  unsigned* dcent = reinterpret_cast<unsigned*>(take(K * 4));
+  // initial centers: the first K of a Fisher-Yates shuffle (clustering.rs:433-445, 527-534)
+  uint64_t state = seed == 0 ? 0x9E3779B97F4A7C15ull : seed;
+  std::vector<int64_t> order((size_t)N);
+  for (int64_t i = 0; i < N; ++i) order[i] = i;
+  for (int64_t i = N - 1; i >= 1; --i) {
+    const int64_t j = (int64_t)(km_xorshift64(&state) % (uint64_t)(i + 1));
+    std::swap(order[i], order[j]);
+  }
+  std::vector<int64_t> idx(order.begin(), order.begin() + K);
+  CU(cudaMemcpyAsync(dreseed, idx.data(), (size_t)K * 8, cudaMemcpyHostToDevice, s), "upload");
+  CU(wmd::kmeans_gather(feat, nf, dreseed, (int)K, cen_a, s), "kmeans init");
+  std::vector<int> counts((size_t)K);
+  std::vector<int64_t> reseed((size_t)K);
+  std::vector<double> shift((size_t)K);
+  for (int64_t it = 0; it < iters; ++it) {
+    CU(wmd::kmeans_assign(feat, N, nf, cen_a, (int)K, dlabels, nullptr, s), "kmeans assign");
+    CU(wmd::kmeans_sums(feat, N, nf, dlabels, (int)K, sums, dcounts, s), "kmeans sums");
+    CU(cudaMemcpyAsync(counts.data(), dcounts, (size_t)K * 4, cudaMemcpyDeviceToHost, s), "D2H");
+    CU(cudaStreamSynchronize(s), "synchronize");
+    for (int64_t c = 0; c < K; ++c)
+      reseed[c] = counts[c] == 0 ? (int64_t)(km_xorshift64(&state) % (uint64_t)N) : -1;
+    CU(cudaMemcpyAsync(dreseed, reseed.data(), (size_t)K * 8, cudaMemcpyHostToDevice, s), "upload");
+    CU(wmd::kmeans_centers(feat, nf, sums, dcounts, dreseed, (int)K, cen_a, cen_b, dshift, s), "kmeans centers");
+    CU(cudaMemcpyAsync(shift.data(), dshift, (size_t)K * 8, cudaMemcpyDeviceToHost, s), "D2H");
+    CU(cudaStreamSynchronize(s), "synchronize");
+    std::swap(cen_a, cen_b);
+    double max_shift = 0.0;
+    for (double v : shift) max_shift = std::max(max_shift, v);
+    if (max_shift <= tolerance) break;
+  }
+  CU(wmd::kmeans_finish(feat, N, nf, cen_a, dlabels, (int)K, ddist, dbest, dsizes, dcent, s), "kmeans finish");
+  std::vector<unsigned> hs((size_t)K), hc((size_t)K);
+  CU(cudaMemcpyAsync(hs.data(), dsizes, (size_t)K * 4, cudaMemcpyDeviceToHost, s), "D2H");
+  CU(cudaMemcpyAsync(hc.data(), dcent, (size_t)K * 4, cudaMemcpyDeviceToHost, s), "D2H");
+  CU(cudaMemcpyAsync(labels, dlabels, (size_t)N * 4, cudaMemcpyDefault, s), "copy out");
+  CU(cudaStreamSynchronize(s), "synchronize");
+  for (int64_t c = 0; c < K; ++c)
+    if (hs[c] == 0) hc[c] = 0;  // the reference's best_idx default
+  CU(cudaMemcpy(sizes, hs.data(), (size_t)K * 4, cudaMemcpyDefault), "copy out");
+  CU(cudaMemcpy(centroids, hc.data(), (size_t)K * 4, cudaMemcpyDefault), "copy out");
+  *n_out = K;
+  return check_status(ctx);
 }
 
 // Builds the device trajectory table for a tile shape; returns total items

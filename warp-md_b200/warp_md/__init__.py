@@ -22,7 +22,8 @@ __version__ = "0.4.30"
 from ._native import WarpMdError  # noqa: F401
 from .core import Selection, System, Trajectory  # noqa: F401
 from .plans import (AlignPlan, AtomicAdpPlan, AtomicFluctPlan, BfactorsPlan, PairwiseRmsdPlan,  # noqa: F401
-                    RmsdPerResPlan, RmsdPlan, RmsfPlan, RotationMatrixPlan, SuperposePlan, SuperposeTrajectoryPlan)
+                    RmsdPerResPlan, RmsdPlan, RmsfPlan, RotationMatrixPlan, SuperposePlan, SuperposeTrajectoryPlan,
+                    TrajectoryClusterPlan)
 from . import synth  # noqa: F401
 
 __rust_cuda_enabled__ = True
@@ -37,4 +38,4 @@ def native_version() -> str:
 
 __all__ = ["System", "Selection", "Trajectory", "RmsdPlan", "PairwiseRmsdPlan", "AlignPlan", "RotationMatrixPlan",
            "SuperposePlan", "SuperposeTrajectoryPlan", "RmsfPlan", "AtomicFluctPlan", "BfactorsPlan", "AtomicAdpPlan",
-           "RmsdPerResPlan", "WarpMdError", "synth"]
+           "RmsdPerResPlan", "TrajectoryClusterPlan", "WarpMdError", "synth"]

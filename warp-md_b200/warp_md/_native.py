@@ -40,7 +40,7 @@ EXPORTED = (
     "wmd_rmsd_frames", "wmd_rmsd_forward", "wmd_rmsd_backward", "wmd_rmsd_covariance", "wmd_pairwise_rmsd",
     "wmd_batched_prepare", "wmd_batched_rmsd", "wmd_batched_layout", "wmd_rmsd_frames_noalloc",
     "wmd_reference_upload_weighted", "wmd_superpose_transforms", "wmd_superpose", "wmd_rmsf", "wmd_rmsd_per_group",
-    "wmd_group_ref_upload", "wmd_group_ref_free",
+    "wmd_group_ref_upload", "wmd_group_ref_free", "wmd_cluster_dbscan", "wmd_cluster_kmeans",
 )
 
 
@@ -102,6 +102,10 @@ def load() -> ctypes.CDLL:
         L.wmd_rmsd_per_group.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, i32, vp, vp]
         L.wmd_group_ref_upload.argtypes = [vp, vp, i64, i32, vp, vp, i64, ctypes.POINTER(vp)]
         L.wmd_group_ref_free.argtypes = [vp, vp]
+        L.wmd_cluster_dbscan.argtypes = [vp, vp, i64, i64, i32, vp, i64, i32, ctypes.c_float, i64, vp, vp, vp,
+                                         ctypes.POINTER(i64), vp]
+        L.wmd_cluster_kmeans.argtypes = [vp, vp, i64, i64, i32, vp, i64, i64, i64, ctypes.c_float, ctypes.c_uint64,
+                                         vp, vp, vp, ctypes.POINTER(i64), vp]
         L.wmd_rmsd_frames_noalloc.argtypes = [vp, i64, i64, i32, vp, i64, i32, vp, vp]
         for name in EXPORTED:
             getattr(L, name).restype = getattr(L, name).restype if name in ("wmd_last_error", "wmd_version") else i32

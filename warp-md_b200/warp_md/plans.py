@@ -11,6 +11,7 @@ runs the fused per-frame kernel.  Results are float32 like the reference
 """
 from __future__ import annotations
 
+import ctypes
 from typing import Optional, Sequence
 
 import numpy as np
@@ -425,3 +426,77 @@ class RmsdPerResPlan:
             groups_ref.close()
             r.close()
         return resid_arr, out
+
+
+# ---------------------------------------------------------------------------
+# clustering
+# ---------------------------------------------------------------------------
+
+class TrajectoryClusterPlan:
+    """Frame clustering (warp_md.TrajectoryClusterPlan, crates/traj-py/src/io.rs:
+    2805-2881; clustering.rs): DBSCAN over the all-pairs RMSD matrix (computed
+    on the tensor-core or SIMT pairwise path, ``pairwise_mode``; "fp64"
+    reproduces the reference's matrix) or k-means on frames superposed onto
+    frame 0.  run() returns {"labels", "centroids", "sizes", "method",
+    "n_frames"}."""
+
+    def __init__(self, selection: Selection, method: str = "dbscan", eps: float = 2.0, min_samples: int = 5,
+                 n_clusters: int = 8, max_iter: int = 100, tol: float = 1.0e-4, seed: int = 0,
+                 memory_budget_bytes: Optional[int] = None, pairwise_mode: str = "fp64"):
+        m = str(method).strip().lower()
+        if m not in ("dbscan", "kmeans"):
+            raise RuntimeError("method must be 'dbscan' or 'kmeans'")
+        if pairwise_mode not in _PAIR_MODES:
+            raise RuntimeError(f"pairwise_mode must be one of {sorted(_PAIR_MODES)}")
+        self.selection = selection
+        self.method = m
+        self.eps = float(np.float32(eps))
+        self.min_samples = int(min_samples)
+        self.n_clusters = int(n_clusters)
+        self.max_iter = int(max_iter)
+        self.tol = float(np.float32(tol))
+        self.seed = int(seed)
+        self.memory_budget_bytes = memory_budget_bytes
+        self.pairwise_mode = pairwise_mode
+
+    def run(self, traj: Trajectory, system: System, chunk_frames: Optional[int] = None, device: str = "auto",
+            frame_indices: Optional[Sequence[int]] = None) -> dict:
+        dev = parse_device(device)
+        if len(self.selection) == 0:
+            raise RuntimeError("mismatch: trajectory_cluster requires a non-empty selection")
+        sel = _check_inputs(traj, system, self.selection)
+        coords = traj.coords
+        sub = frame_subset(coords.shape[0], frame_indices)
+        if sub is not None:
+            coords = np.ascontiguousarray(coords[sub])
+        n = coords.shape[0]
+        empty = {"labels": np.zeros(0, np.int32), "centroids": np.zeros(0, np.uint32),
+                 "sizes": np.zeros(0, np.uint32), "method": self.method, "n_frames": 0}
+        if n == 0:
+            return empty
+        labels = np.empty(n, np.int32)
+        cent = np.empty(n, np.uint32)
+        sizes = np.empty(n, np.uint32)
+        k = ctypes.c_int64(0)
+        ctx = N.context(dev)
+        dense = _dense_prefix(sel)
+        sel_arr = None if dense else np.ascontiguousarray(sel, dtype=np.uint32)
+        if self.method == "dbscan":
+            if self.eps <= 0.0:
+                raise RuntimeError("parse error: trajectory_cluster DBSCAN eps must be > 0")
+            need = n * (n - 1) // 2 * 4
+            if self.memory_budget_bytes is not None and need > self.memory_budget_bytes:
+                raise RuntimeError(f"unsupported: trajectory_cluster distance matrix requires {need} bytes but "
+                                   f"memory_budget_bytes={self.memory_budget_bytes}")
+            ctx.check(ctx.lib.wmd_cluster_dbscan(ctx.handle, coords.ctypes.data, n, coords.shape[1], 3, N.ptr(sel_arr),
+                                                 int(sel.size), _PAIR_MODES[self.pairwise_mode], self.eps,
+                                                 max(1, self.min_samples), labels.ctypes.data, cent.ctypes.data,
+                                                 sizes.ctypes.data, k, None))
+        else:
+            ctx.check(ctx.lib.wmd_cluster_kmeans(ctx.handle, coords.ctypes.data, n, coords.shape[1], 3, N.ptr(sel_arr),
+                                                 int(sel.size), self.n_clusters, self.max_iter, self.tol,
+                                                 self.seed & 0xFFFFFFFFFFFFFFFF, labels.ctypes.data, cent.ctypes.data,
+                                                 sizes.ctypes.data, k, None))
+        kk = int(k.value)
+        return {"labels": labels, "centroids": cent[:kk].copy(), "sizes": sizes[:kk].copy(), "method": self.method,
+                "n_frames": n}
