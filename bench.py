@@ -28,6 +28,8 @@ atom-frames/s.  One step = one pass of the per-frame kernel over all frames.
   selection, transforms + every atom moved (SuperposePlan).
 * fluct: RMSF + ADP over 100,000 atoms x 2,000 frames, and per-residue RMSD
   of 10,000 residues after superposing a 10,000-atom selection.
+* cluster: DBSCAN over the 20,000-frame all-pairs matrix (tensor-core and
+  FP64 forms) and k-means on the superposed frames (TrajectoryClusterPlan).
 * --gpus N (torchrun): weak scaling, each rank streams its own 10,000 frames;
   no data-path collective (frames are independent).
 """
@@ -556,6 +558,76 @@ def run_fluct(args, ctx, stream, rank):
     return res
 
 
+def run_cluster(args, ctx, stream, rank):
+    """TrajectoryClusterPlan workloads on the all-pairs trajectory (20,000
+    frames x 1,000 atoms): DBSCAN over the tensor-core (i8x3) matrix and over
+    the FP64 matrix, and k-means (8 clusters, 20 iterations) on the frames
+    superposed onto frame 0.  Device-resident inputs; checked against the
+    oracle on a 1,000-frame prefix."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from warp_md import _native as N
+    from warp_md import synth
+    from warp_md.plans import _PAIR_MODES
+
+    F, n = args.cl_frames, PAIR_ATOMS
+    coords = synth.make_drift_trajectory_torch(n, F, 0.1, seed=3 + rank, device="cuda")
+    labels = torch.empty(F, dtype=torch.int32, device="cuda")
+    cent = torch.empty(F, dtype=torch.int32, device="cuda")
+    sizes = torch.empty(F, dtype=torch.int32, device="cuda")
+    k = ctypes.c_int64(0)
+    eps = 1.0
+
+    def dbscan(mode):
+        ctx.check(ctx.lib.wmd_cluster_dbscan(ctx.handle, coords.data_ptr(), F, n, 3, None, n, _PAIR_MODES[mode], eps,
+                                             5, labels.data_ptr(), cent.data_ptr(), sizes.data_ptr(),
+                                             ctypes.byref(k), stream.cuda_stream))
+
+    def kmeans():
+        ctx.check(ctx.lib.wmd_cluster_kmeans(ctx.handle, coords.data_ptr(), F, n, 3, None, n, 8, 20, 0.0, 7,
+                                             labels.data_ptr(), cent.data_ptr(), sizes.data_ptr(), ctypes.byref(k),
+                                             stream.cuda_stream))
+
+    res = {"n_frames": F, "n_atoms": n, "workload": PAIR_WORKLOAD}
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / reps * 1e3
+
+    for mode in ("i8x3", "fp64"):
+        ms = timed(lambda: dbscan(mode), 1 if mode == "fp64" else 3)
+        res[f"dbscan_{mode}"] = {"ms": ms, "n_clusters": int(k.value), "eps": eps, "min_samples": 5,
+                                 "noise": int((labels == -1).sum().item()),
+                                 "timing": "host wall clock around the synchronous call (matrix + DBSCAN)"}
+    ms = timed(kmeans, 1)
+    res["kmeans"] = {"ms": ms, "n_clusters": 8, "iterations": 20, "sizes": sizes[: int(k.value)].cpu().tolist()}
+    # parity on a prefix
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import oracle
+
+    m = min(F, 1000)
+    host = coords[:m].cpu().numpy()
+    d32, _ = oracle.pairwise(host)
+    ol, oc, osz = oracle.dbscan(d32, eps, 5)
+    sub = coords[:m].contiguous()
+    ctx.check(ctx.lib.wmd_cluster_dbscan(ctx.handle, sub.data_ptr(), m, n, 3, None, n, _PAIR_MODES["fp64"], eps, 5,
+                                         labels.data_ptr(), cent.data_ptr(), sizes.data_ptr(), ctypes.byref(k),
+                                         stream.cuda_stream))
+    res["dbscan_parity_1000"] = bool(np.array_equal(labels[:m].cpu().numpy(), ol) and
+                                     np.array_equal(cent[: int(k.value)].cpu().numpy().astype(np.uint32), oc))
+    del coords, labels, cent, sizes
+    torch.cuda.empty_cache()
+    return res
+
+
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
@@ -723,6 +795,9 @@ def run_ours(args):
     fluct = None
     if not args.skip_fluct:
         fluct = run_fluct(args, ctx, stream, rank)
+    cluster = None
+    if not args.skip_cluster:
+        cluster = run_cluster(args, ctx, stream, rank)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -746,6 +821,7 @@ def run_ours(args):
             "batched_uneven": batched,
             "superpose": superpose,
             "fluct": fluct,
+            "cluster": cluster,
         }
         print(json.dumps(line), flush=True)
     r.close()
@@ -784,6 +860,8 @@ def main():
     ap.add_argument("--skip-fluct", action="store_true")
     ap.add_argument("--fl-frames", type=int, default=2000)
     ap.add_argument("--fl-steps", type=int, default=5)
+    ap.add_argument("--skip-cluster", action="store_true")
+    ap.add_argument("--cl-frames", type=int, default=20_000)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
