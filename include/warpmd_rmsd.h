@@ -43,6 +43,9 @@ extern "C" {
 #define WMD_ERR_UNSUPPORTED (-5) /* mode/metric not provided on this build   */
 #define WMD_ERR_TIMEOUT (-6)     /* a bounded device-side wait ran out       */
 #define WMD_ERR_NO_DEVICE (-7)   /* no CUDA device / not an sm_100 device     */
+#define WMD_ERR_IO (-8)          /* file missing or shorter than its records  */
+                                 /* say (TrajError::Io)                       */
+#define WMD_ERR_PARSE (-9)       /* malformed trajectory file (TrajError::Parse) */
 
 #define WMD_PAIR_RMS 0   /* optimal-superposition RMSD (metric "rms")  */
 #define WMD_PAIR_NOFIT 1 /* plain coordinate RMSD (metric "nofit")     */
@@ -263,6 +266,38 @@ int wmd_cluster_kmeans(wmd_ctx* ctx, const float* coords, int64_t n_frames, int6
                        const uint32_t* sel, int64_t n_sel, int64_t n_clusters, int64_t max_iter, float tol,
                        uint64_t seed, int32_t* labels, uint32_t* centroids, uint32_t* sizes, int64_t* n_out,
                        void* stream);
+
+/* ---- DCD trajectories (DcdReader, crates/traj-io/src/dcd.rs:45-570;
+ *      PyTrajectory.open_dcd / read_chunk, crates/traj-py/src/io.rs:687-708,
+ *      1335-1560) ----
+ * The file is parsed on the host at open; frames are read as raw bytes
+ * (threaded pread into pinned buffers), copied to the device asynchronously
+ * and decoded there (record markers checked, byte order, selection, length
+ * scale), overlapping the read of the next batch.  Errors follow the
+ * reference's: WMD_ERR_IO, WMD_ERR_PARSE, WMD_ERR_UNSUPPORTED (unknown record
+ * marker), WMD_ERR_MISMATCH (selection index out of bounds). */
+typedef struct wmd_dcd wmd_dcd;
+int wmd_dcd_open(wmd_ctx* ctx, const char* path, float length_scale, wmd_dcd** out);
+int wmd_dcd_close(wmd_ctx* ctx, wmd_dcd* dcd);
+/* n_atoms; n_frames = whole frames the file holds; header_frames = the
+ * header's count when positive, else 0 (n_frames_hint). */
+int wmd_dcd_info(const wmd_dcd* dcd, int64_t* n_atoms, int64_t* n_frames, int64_t* header_frames);
+/* read_chunk / read_chunk_selected from frame `first`: up to max_frames
+ * frames into coords [n][n_out][3] float32 (host or device), n_out = n_sel
+ * when sel is not NULL (atoms in selection order, repeats allowed) else
+ * n_atoms.  box_kind [n] (0 none, 1 orthorhombic, 2 triclinic) and box [n][9]
+ * (box vectors a, b, c as rows), host, may be NULL.  *n_read = frames read
+ * (fewer than max_frames at the end of the file).  A read that reaches a
+ * damaged end of file fails as the reference's chunk does and reads nothing. */
+int wmd_dcd_read(wmd_ctx* ctx, wmd_dcd* dcd, int64_t first, int64_t max_frames, const uint32_t* sel, int64_t n_sel,
+                 float* coords, int32_t* box_kind, float* box, int64_t* n_read, void* stream);
+/* RmsdPlan over frames [first, first + max_frames) of the file: the selected
+ * atoms of every frame against `ref` (align as in wmd_rmsd_frames); out [n]
+ * doubles, host or device; *n_read as in wmd_dcd_read.  The file read, the
+ * host->device copy, the decode and the RMSD kernels of successive batches
+ * overlap. */
+int wmd_dcd_rmsd(wmd_ctx* ctx, wmd_dcd* dcd, int64_t first, int64_t max_frames, const uint32_t* sel, int64_t n_sel,
+                 const wmd_ref* ref, int align, double* out, int64_t* n_read, void* stream);
 
 /* Per-frame aligned RMSD for callers that cannot allocate memory.  No
  * counterpart in the reference.  Everything else in this header needs a

@@ -18,6 +18,7 @@ enum DeviceStatus : int {
   kStatusTimeoutDrain = 4,  // exit-time wait for copies in flight ran out
   kStatusTimeoutPeer = 8,   // wait on another CTA's flag ran out
   kStatusBadIndex = 16,     // a selection index was >= n_atoms
+  kStatusBadRecord = 64,    // a DCD record marker differs from the layout assumed for the file
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {

@@ -20,11 +20,14 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/warpmd_rmsd.h"
 #include "batched.h"
 #include "cluster.h"
+#include "dcd.h"
+#include "device_util.cuh"
 #include "fluct.h"
 #include "pairwise.h"
 #include "superpose.h"
@@ -1577,4 +1580,329 @@ WMD_EXPORT int wmd_batched_layout(const wmd_ctx* ctx, int* tile_atoms, int* fram
   if (tile_atoms) *tile_atoms = wmd::batched_tile_atoms(ctx->b_plan.apt);
   if (frame_major) *frame_major = ctx->b_plan.variant == wmd::kBatchFrames ? 1 : 0;
   return WMD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// DCD trajectories (DcdReader, crates/traj-io/src/dcd.rs; PyTrajectory
+// open_dcd / read_chunk, crates/traj-py/src/io.rs:687-708, 1335-1560)
+// ---------------------------------------------------------------------------
+
+struct wmd_dcd {
+  wmd::DcdFile f;
+  int device = 0;
+  int threads = 8;  // parallel preads per batch
+  HostBuf pin[2];   // raw file bytes of a batch (+ the X-offset table of an indexed file)
+  DevBuf raw[2], coords;
+  cudaEvent_t h2d_done[2] = {nullptr, nullptr};
+  cudaEvent_t consumed[2] = {nullptr, nullptr};
+};
+
+namespace {
+
+// Raw bytes per batch: large enough to keep the copy engine and the pread
+// threads streaming, small enough that two pinned slots stay cheap.
+constexpr int64_t kDcdBatchBytes = int64_t(64) << 20;
+
+int dcd_err(wmd_ctx* ctx, const wmd::DcdError& e) {
+  const int code = e.kind == wmd::kDcdIo ? WMD_ERR_IO : e.kind == wmd::kDcdParse ? WMD_ERR_PARSE : WMD_ERR_UNSUPPORTED;
+  const char* cls = e.kind == wmd::kDcdIo ? "io error" : e.kind == wmd::kDcdParse ? "parse error" : "unsupported";
+  return set_err(ctx, code, "%s: %s", cls, e.msg.c_str());
+}
+
+// Status of the decode launches: a record marker that broke the layout
+// assumed for the file is returned in *bad_record, anything else as an error.
+int dcd_status(wmd_ctx* ctx, bool* bad_record) {
+  const int st = __atomic_exchange_n(ctx->status_host, 0, __ATOMIC_ACQ_REL);
+  *bad_record = (st & wmd::kStatusBadRecord) != 0;
+  const int rest = st & ~wmd::kStatusBadRecord;
+  if (!rest) return WMD_OK;
+  if (rest & wmd::kStatusBadIndex)
+    return set_err(ctx, WMD_ERR_MISMATCH, "mismatch: selection index out of bounds (device selection)");
+  return set_err(ctx, WMD_ERR_TIMEOUT, "a device-side wait exceeded its limit (status 0x%x)", rest);
+}
+
+// Host selection indices checked as validate_selection does
+// (crates/traj-io/src/selection_support.rs:3-13).
+int dcd_check_sel(wmd_ctx* ctx, const wmd::DcdFile& F, const uint32_t* sel, int64_t n_sel) {
+  if (!sel || classify(sel) == Mem::Device) return WMD_OK;
+  for (int64_t i = 0; i < n_sel; ++i)
+    if ((int64_t)sel[i] >= F.n_atoms)
+      return set_err(ctx, WMD_ERR_MISMATCH, "mismatch: selection index %u out of bounds for trajectory with %lld atoms",
+                     sel[i], (long long)F.n_atoms);
+  return WMD_OK;
+}
+
+// Streams frames [first, first + n) through the two pinned and device slots.
+// Per batch: pread (host threads) -> on_host(pinned bytes, their file offset,
+// frames [fa, fb)) -> host->device copy (copy stream) -> decode (stream s)
+// into dout at the batch's frames, or into scratch when dout is null ->
+// on_dev(decoded frames, fa - first, fb - fa).  The pread of batch k + 1 runs
+// while batch k is copied and decoded.
+template <class HostFn, class DevFn>
+int dcd_stream(wmd_ctx* ctx, wmd_dcd* d, int64_t first, int64_t n, const uint32_t* dsel, int64_t n_out, float* dout,
+               cudaStream_t s, HostFn on_host, DevFn on_dev) {
+  const wmd::DcdFile& F = d->f;
+  if (n == 0) return WMD_OK;
+  std::vector<int64_t> cuts{first};
+  size_t max_bytes = 0;
+  int64_t max_frames = 0;
+  for (int64_t a = first; a < first + n;) {
+    int64_t b;
+    if (!F.indexed) {
+      b = std::min(first + n, a + std::max<int64_t>(1, kDcdBatchBytes / F.stride));
+    } else {
+      b = a + 1;
+      while (b < first + n && F.frame_begin(b + 1) - F.frame_begin(a) <= kDcdBatchBytes) ++b;
+    }
+    const int64_t base = F.frame_begin(a) & ~int64_t(15);
+    const size_t padded = ((size_t)(F.frame_begin(b) - base) + 15) & ~size_t(15);
+    max_bytes = std::max(max_bytes, padded + (F.indexed ? (size_t)(b - a) * 8 : 0));
+    max_frames = std::max(max_frames, b - a);
+    cuts.push_back(b);
+    a = b;
+  }
+  int rc;
+  for (int k = 0; k < 2; ++k) {
+    if ((rc = ensure_host(ctx, d->pin[k], max_bytes))) return rc;
+    if ((rc = ensure(ctx, d->raw[k], max_bytes))) return rc;
+  }
+  float* scratch = nullptr;
+  if (!dout) {
+    if ((rc = ensure(ctx, d->coords, (size_t)max_frames * (size_t)n_out * 3 * sizeof(float)))) return rc;
+    scratch = static_cast<float*>(d->coords.ptr);
+  }
+  for (int k = 0; k < 2; ++k) {
+    CU(cudaEventRecord(d->consumed[k], s), "event");
+    CU(cudaEventRecord(d->h2d_done[k], ctx->copy_stream), "event");
+  }
+  for (size_t k = 0; k + 1 < cuts.size(); ++k) {
+    const int b = (int)(k & 1);
+    const int64_t fa = cuts[k], fb = cuts[k + 1], nf = fb - fa;
+    const int64_t base = F.frame_begin(fa) & ~int64_t(15);
+    const int64_t bytes = F.frame_begin(fb) - base;
+    const size_t padded = ((size_t)bytes + 15) & ~size_t(15);
+    CU(cudaEventSynchronize(d->h2d_done[b]), "pinned slot wait");
+    uint8_t* hp = static_cast<uint8_t*>(d->pin[b].ptr);
+    if (wmd::DcdError e = wmd::dcd_pread(F, hp, base, bytes, d->threads)) return dcd_err(ctx, e);
+    size_t copy = padded;
+    if (F.indexed) {
+      int64_t* tab = reinterpret_cast<int64_t*>(hp + padded);
+      for (int64_t f = 0; f < nf; ++f) tab[f] = F.frame_x(fa + f);
+      copy += (size_t)nf * 8;
+    }
+    on_host(static_cast<const uint8_t*>(hp), base, fa, fb);
+    CU(cudaStreamWaitEvent(ctx->copy_stream, d->consumed[b], 0), "stream wait");
+    CU(cudaMemcpyAsync(d->raw[b].ptr, hp, copy, cudaMemcpyHostToDevice, ctx->copy_stream), "H2D");
+    CU(cudaEventRecord(d->h2d_done[b], ctx->copy_stream), "event");
+    CU(cudaStreamWaitEvent(s, d->h2d_done[b], 0), "stream wait");
+    wmd::DcdDecode D;
+    D.raw = static_cast<const uint8_t*>(d->raw[b].ptr);
+    D.raw_off = base;
+    D.first = fa;
+    D.n_frames = nf;
+    D.xoff = F.indexed ? reinterpret_cast<const int64_t*>(static_cast<const uint8_t*>(d->raw[b].ptr) + padded) : nullptr;
+    D.data_start = F.data_start;
+    D.stride = F.stride;
+    D.cell = F.cell;
+    D.n_atoms = F.n_atoms;
+    D.marker = F.marker;
+    D.big = F.big;
+    D.aligned = (F.data_start & 3) == 0;
+    D.scale = F.length_scale;
+    D.sel = dsel;
+    D.n_out = n_out;
+    D.out = dout ? dout + (size_t)(fa - first) * (size_t)n_out * 3 : scratch;
+    D.status = ctx->status_dev;
+    CU(wmd::launch_dcd_decode(D, ctx->sm_count, s), "dcd decode launch");
+    if ((rc = on_dev(D.out, fa - first, nf))) return rc;
+    CU(cudaEventRecord(d->consumed[b], s), "event");
+  }
+  return WMD_OK;
+}
+
+// Frames a read from `first` of up to max_frames returns, or the error of a
+// damaged end of file that the read would reach.
+int dcd_span(wmd_ctx* ctx, const wmd::DcdFile& F, int64_t first, int64_t max_frames, int64_t* n) {
+  const int64_t avail = std::max<int64_t>(0, F.n_frames - first);
+  *n = std::min(max_frames, avail);
+  if (max_frames > avail && F.end) return dcd_err(ctx, F.end);
+  return WMD_OK;
+}
+
+}  // namespace
+
+WMD_EXPORT int wmd_dcd_open(wmd_ctx* ctx, const char* path, float length_scale, wmd_dcd** out) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  if (!out || !path) return set_err(ctx, WMD_ERR_INVALID_ARG, "path or out is null");
+  *out = nullptr;
+  DeviceGuard g(ctx->device);
+  wmd_dcd* d = new wmd_dcd();
+  d->device = ctx->device;
+  if (wmd::DcdError e = wmd::dcd_open(path, length_scale, &d->f)) {
+    wmd::dcd_close(&d->f);
+    delete d;
+    return dcd_err(ctx, e);
+  }
+  const unsigned hw = std::thread::hardware_concurrency();
+  d->threads = (int)std::max(1u, std::min(8u, hw ? hw : 1u));
+  for (int k = 0; k < 2; ++k) {
+    cudaError_t e = cudaEventCreateWithFlags(&d->h2d_done[k], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&d->consumed[k], cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+      wmd_dcd_close(ctx, d);
+      return cuda_err(ctx, e, "event");
+    }
+  }
+  *out = d;
+  return WMD_OK;
+}
+
+WMD_EXPORT int wmd_dcd_close(wmd_ctx* ctx, wmd_dcd* d) {
+  if (!d) return WMD_OK;
+  DeviceGuard g(d->device);
+  for (int k = 0; k < 2; ++k) {
+    if (d->h2d_done[k]) {
+      cudaEventSynchronize(d->h2d_done[k]);
+      cudaEventDestroy(d->h2d_done[k]);
+    }
+    if (d->consumed[k]) {
+      cudaEventSynchronize(d->consumed[k]);
+      cudaEventDestroy(d->consumed[k]);
+    }
+  }
+  for (DevBuf* b : {&d->raw[0], &d->raw[1], &d->coords})
+    if (b->ptr) cudaFree(b->ptr);
+  for (HostBuf* b : {&d->pin[0], &d->pin[1]})
+    if (b->ptr) cudaFreeHost(b->ptr);
+  wmd::dcd_close(&d->f);
+  delete d;
+  (void)ctx;
+  return WMD_OK;
+}
+
+WMD_EXPORT int wmd_dcd_info(const wmd_dcd* d, int64_t* n_atoms, int64_t* n_frames, int64_t* header_frames) {
+  if (!d) return WMD_ERR_INVALID_ARG;
+  if (n_atoms) *n_atoms = d->f.n_atoms;
+  if (n_frames) *n_frames = d->f.n_frames;
+  if (header_frames) *header_frames = d->f.header_frames;
+  return WMD_OK;
+}
+
+WMD_EXPORT int wmd_dcd_read(wmd_ctx* ctx, wmd_dcd* d, int64_t first, int64_t max_frames, const uint32_t* sel,
+                            int64_t n_sel, float* coords, int32_t* box_kind, float* box, int64_t* n_read,
+                            void* stream) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  if (n_read) *n_read = 0;
+  if (!d) return set_err(ctx, WMD_ERR_INVALID_ARG, "dcd is null");
+  if (first < 0 || max_frames < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "negative frame range");
+  if (sel && n_sel <= 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "atom_indices must not be empty");
+  if ((box_kind && classify(box_kind) == Mem::Device) || (box && classify(box) == Mem::Device))
+    return set_err(ctx, WMD_ERR_INVALID_ARG, "box outputs must be host memory");
+  DeviceGuard g(ctx->device);
+  int rc = check_status(ctx);
+  if (rc) return rc;
+  if ((rc = dcd_check_sel(ctx, d->f, sel, n_sel))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const wmd::DcdFile& F = d->f;
+  const int64_t n_out = sel ? n_sel : F.n_atoms;
+  const Mem cm = classify(coords);
+  float* dout = cm == Mem::Device ? coords : nullptr;
+  int64_t n_cap = max_frames;  // a retry never writes more frames than the first attempt sized
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    int64_t n = 0;
+    if ((rc = dcd_span(ctx, F, first, max_frames, &n))) return rc;
+    n = std::min(n, n_cap);
+    n_cap = n;
+    if (n == 0) return WMD_OK;
+    if (!coords) return set_err(ctx, WMD_ERR_INVALID_ARG, "coords is null");
+    const uint32_t* dsel = nullptr;
+    if ((rc = resolve_sel(ctx, sel, n_sel, F.n_atoms, &dsel, s))) return rc;
+    auto on_host = [&](const uint8_t* hp, int64_t base, int64_t fa, int64_t fb) {
+      if (!box_kind && !box) return;
+      for (int64_t f = fa; f < fb; ++f) {
+        float m[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        int kind = 0;
+        const int64_t c = F.frame_cell(f);
+        if (c) kind = wmd::dcd_box(F, hp + (F.frame_begin(f) + F.marker - base), c, m);
+        if (box_kind) box_kind[f - first] = kind;
+        if (box) std::memcpy(box + (f - first) * 9, m, sizeof(m));
+      }
+    };
+    auto on_dev = [&](const float* dc, int64_t f0, int64_t nf) -> int {
+      if (dout) return WMD_OK;
+      CU(cudaMemcpyAsync(coords + (size_t)f0 * (size_t)n_out * 3, dc, (size_t)nf * (size_t)n_out * 3 * sizeof(float),
+                         cudaMemcpyDeviceToHost, s),
+         "D2H");
+      return WMD_OK;
+    };
+    if ((rc = dcd_stream(ctx, d, first, n, dsel, n_out, dout, s, on_host, on_dev))) return rc;
+    CU(cudaStreamSynchronize(s), "synchronize");
+    bool bad = false;
+    if ((rc = dcd_status(ctx, &bad))) return rc;
+    if (!bad) {
+      if (n_read) *n_read = n;
+      return WMD_OK;
+    }
+    if (F.indexed) break;
+    wmd::dcd_index(&d->f);  // frames differ from the first one: read them by their own layout
+  }
+  return set_err(ctx, WMD_ERR_PARSE, "parse error: record markers disagree with the frame index");
+}
+
+WMD_EXPORT int wmd_dcd_rmsd(wmd_ctx* ctx, wmd_dcd* d, int64_t first, int64_t max_frames, const uint32_t* sel,
+                            int64_t n_sel, const wmd_ref* ref, int align, double* out, int64_t* n_read,
+                            void* stream) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  if (n_read) *n_read = 0;
+  if (!d) return set_err(ctx, WMD_ERR_INVALID_ARG, "dcd is null");
+  if (!ref) return set_err(ctx, WMD_ERR_INVALID_ARG, "reference is null");
+  if (ref->info.w)
+    return set_err(ctx, WMD_ERR_INVALID_ARG, "a weighted reference serves the superposition entry points only");
+  if (first < 0 || max_frames < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "negative frame range");
+  if (sel && n_sel <= 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "atom_indices must not be empty");
+  const wmd::DcdFile& F = d->f;
+  const int64_t n_out = sel ? n_sel : F.n_atoms;
+  if (n_out != ref->info.n_sel)
+    return set_err(ctx, WMD_ERR_MISMATCH, "reference has %lld atoms but the selection has %lld",
+                   (long long)ref->info.n_sel, (long long)n_out);
+  DeviceGuard g(ctx->device);
+  int rc = check_status(ctx);
+  if (rc) return rc;
+  if ((rc = dcd_check_sel(ctx, F, sel, n_sel))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool oh = is_host(classify(out));
+  int64_t n_cap = max_frames;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    int64_t n = 0;
+    if ((rc = dcd_span(ctx, F, first, max_frames, &n))) return rc;
+    n = std::min(n, n_cap);
+    n_cap = n;
+    if (n == 0) return WMD_OK;
+    if (!out) return set_err(ctx, WMD_ERR_INVALID_ARG, "out is null");
+    const uint32_t* dsel = nullptr;
+    if ((rc = resolve_sel(ctx, sel, n_sel, F.n_atoms, &dsel, s))) return rc;
+    double* o = out;
+    if (oh) {
+      if ((rc = ensure(ctx, ctx->out_tmp, (size_t)n * sizeof(double)))) return rc;
+      o = static_cast<double*>(ctx->out_tmp.ptr);
+    }
+    auto on_host = [](const uint8_t*, int64_t, int64_t, int64_t) {};
+    auto on_dev = [&](const float* dc, int64_t f0, int64_t nf) -> int {
+      wmd::FrameOutputs fo;
+      fo.rmsd = o + f0;
+      return forward_device(ctx, dc, nf, n_out, 3, nullptr, ref, align, fo, s);
+    };
+    if ((rc = dcd_stream(ctx, d, first, n, dsel, n_out, nullptr, s, on_host, on_dev))) return rc;
+    if (oh) CU(cudaMemcpyAsync(out, o, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H");
+    CU(cudaStreamSynchronize(s), "synchronize");
+    bool bad = false;
+    if ((rc = dcd_status(ctx, &bad))) return rc;
+    if (!bad) {
+      if (n_read) *n_read = n;
+      return WMD_OK;
+    }
+    if (F.indexed) break;
+    wmd::dcd_index(&d->f);
+  }
+  return set_err(ctx, WMD_ERR_PARSE, "parse error: record markers disagree with the frame index");
 }

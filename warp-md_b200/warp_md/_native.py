@@ -23,6 +23,8 @@ WMD_ERR_MISMATCH = -4
 WMD_ERR_UNSUPPORTED = -5
 WMD_ERR_TIMEOUT = -6
 WMD_ERR_NO_DEVICE = -7
+WMD_ERR_IO = -8
+WMD_ERR_PARSE = -9
 
 PAIR_RMS = 0
 PAIR_NOFIT = 1
@@ -40,7 +42,8 @@ EXPORTED = (
     "wmd_rmsd_frames", "wmd_rmsd_forward", "wmd_rmsd_backward", "wmd_rmsd_covariance", "wmd_pairwise_rmsd",
     "wmd_batched_prepare", "wmd_batched_rmsd", "wmd_batched_layout", "wmd_rmsd_frames_noalloc",
     "wmd_reference_upload_weighted", "wmd_superpose_transforms", "wmd_superpose", "wmd_rmsf", "wmd_rmsd_per_group",
-    "wmd_group_ref_upload", "wmd_group_ref_free", "wmd_cluster_dbscan", "wmd_cluster_kmeans",
+    "wmd_group_ref_upload", "wmd_group_ref_free", "wmd_cluster_dbscan", "wmd_cluster_kmeans", "wmd_dcd_open",
+    "wmd_dcd_close", "wmd_dcd_info", "wmd_dcd_read", "wmd_dcd_rmsd",
 )
 
 
@@ -107,6 +110,11 @@ def load() -> ctypes.CDLL:
         L.wmd_cluster_kmeans.argtypes = [vp, vp, i64, i64, i32, vp, i64, i64, i64, ctypes.c_float, ctypes.c_uint64,
                                          vp, vp, vp, ctypes.POINTER(i64), vp]
         L.wmd_rmsd_frames_noalloc.argtypes = [vp, i64, i64, i32, vp, i64, i32, vp, vp]
+        L.wmd_dcd_open.argtypes = [vp, ctypes.c_char_p, ctypes.c_float, ctypes.POINTER(vp)]
+        L.wmd_dcd_close.argtypes = [vp, vp]
+        L.wmd_dcd_info.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64)]
+        L.wmd_dcd_read.argtypes = [vp, vp, i64, i64, vp, i64, vp, vp, vp, ctypes.POINTER(i64), vp]
+        L.wmd_dcd_rmsd.argtypes = [vp, vp, i64, i64, vp, i64, vp, i32, vp, ctypes.POINTER(i64), vp]
         for name in EXPORTED:
             getattr(L, name).restype = getattr(L, name).restype if name in ("wmd_last_error", "wmd_version") else i32
         _lib = L

@@ -117,6 +117,19 @@ class Trajectory:
             raise RuntimeError("coords must have final dimension 3")
         return Trajectory(np.ascontiguousarray(a, dtype=np.float32), box, time_ps)
 
+    @staticmethod
+    def open_dcd(path: str, system: "System", length_scale: Optional[float] = None) -> "Trajectory":
+        """A DCD file (PyTrajectory.open_dcd, crates/traj-py/src/io.rs:687-708)
+        read through the GPU decoder; see warp_md.dcd."""
+        from .dcd import DcdTrajectory
+
+        return DcdTrajectory(path, system, length_scale)
+
+    @staticmethod
+    def open_xtc(path: str, system: "System") -> "Trajectory":
+        """XTC needs the xdrfile codec, which this build does not provide."""
+        raise RuntimeError("unsupported: XTC trajectories are not provided by this build (use DCD or from_numpy)")
+
     def n_atoms(self) -> int:
         return int(self.coords.shape[1])
 

@@ -18,6 +18,7 @@ import numpy as np
 
 from . import _native as N
 from .core import Selection, System, Trajectory
+from .dcd import DcdTrajectory
 
 _PAIR_MODES = {"fp32": N.MODE_FP32, "i8x3": N.MODE_I8X3, "i8x2": N.MODE_I8X2, "fp64": N.MODE_FP64}
 
@@ -102,6 +103,8 @@ class RmsdPlan:
             frame_indices: Optional[Sequence[int]] = None, dtype=np.float32) -> np.ndarray:
         dev = parse_device(device)
         sel = _check_inputs(traj, system, self.selection)
+        if isinstance(traj, DcdTrajectory) and frame_indices is None:
+            return self._run_dcd(traj, system, sel, dtype)
         coords = traj.coords
         sub = frame_subset(coords.shape[0], frame_indices)
         if sub is not None:
@@ -130,6 +133,31 @@ class RmsdPlan:
                                               out.ctypes.data, None))
         finally:
             r.close()
+        return out.astype(dtype, copy=False)
+
+    def _run_dcd(self, traj: DcdTrajectory, system: System, sel: np.ndarray, dtype) -> np.ndarray:
+        """Frames from the trajectory's position to the end of the file, read,
+        copied and decoded in batches that overlap the RMSD kernels
+        (wmd_dcd_rmsd); the position moves to the end, as the reference's
+        streaming run leaves its reader."""
+        first = traj._cursor
+        n = max(0, traj.n_frames() - first)
+        dense = _dense_prefix(sel) and sel.size == traj.n_atoms()
+        atoms = None if dense else sel
+        if self.reference_mode == "topology":
+            if system.positions0 is None:
+                raise RuntimeError("mismatch: no topology reference coords")
+            ref = system.positions0[sel]
+        else:
+            if n == 0:
+                return np.empty(0, dtype=dtype)
+            chunk = traj._read(first, 1, atoms, False)[0]
+            ref = chunk[0]
+        if sel.size == 0:
+            traj._cursor = first + n
+            return np.zeros(n, dtype=dtype)
+        out = traj.rmsd(ref, atom_indices=atoms, align=self.align, first=first, n=n)
+        traj._cursor = first + out.shape[0]
         return out.astype(dtype, copy=False)
 
 
