@@ -17,7 +17,6 @@
 #include <cerrno>
 #include <cmath>
 #include <cstring>
-#include <thread>
 
 #include "device_util.cuh"
 
@@ -369,23 +368,72 @@ void dcd_close(DcdFile* f) {
   f->fd = -1;
 }
 
-DcdError dcd_pread(const DcdFile& f, void* dst, int64_t off, int64_t len, int threads) {
-  if (off < 0 || off + len > f.file_size) return io_eof();
-  const int64_t min_part = int64_t(4) << 20;
-  const int parts = (int)std::max<int64_t>(1, std::min<int64_t>(threads, len / min_part));
-  if (parts == 1) return pread_full(f.fd, dst, len, off) ? DcdError() : io_eof();
-  std::vector<std::thread> pool;
-  std::vector<char> ok((size_t)parts, 0);
-  const int64_t step = ((len + parts - 1) / parts + 4095) & ~int64_t(4095);
-  for (int p = 0; p < parts; ++p) {
-    const int64_t a = p * step, b = std::min(len, a + step);
-    if (a >= b) {
-      ok[p] = 1;
-      continue;
-    }
-    pool.emplace_back([&, p, a, b] { ok[p] = pread_full(f.fd, static_cast<char*>(dst) + a, b - a, off + a); });
+ReadPool::ReadPool(int threads) {
+  for (int t = 1; t < threads; ++t) workers_.emplace_back([this] { work(); });
+}
+
+ReadPool::~ReadPool() {
+  {
+    std::lock_guard<std::mutex> g(m_);
+    stop_ = true;
   }
-  for (auto& t : pool) t.join();
+  wake_.notify_all();
+  for (auto& t : workers_) t.join();
+}
+
+bool ReadPool::take(int* i) {  // m_ held
+  if (!fn_ || next_ >= parts_) return false;
+  *i = next_++;
+  return true;
+}
+
+void ReadPool::work() {
+  std::unique_lock<std::mutex> lk(m_);
+  for (;;) {
+    int i;
+    wake_.wait(lk, [&] { return stop_ || (fn_ && next_ < parts_); });
+    if (stop_) return;
+    while (take(&i)) {
+      const std::function<void(int)>* fn = fn_;
+      lk.unlock();
+      (*fn)(i);
+      lk.lock();
+      if (--pending_ == 0) done_.notify_all();
+    }
+  }
+}
+
+void ReadPool::run(int parts, const std::function<void(int)>& fn) {
+  if (parts <= 0) return;
+  std::unique_lock<std::mutex> lk(m_);
+  fn_ = &fn;
+  next_ = 0;
+  parts_ = parts;
+  pending_ = parts;
+  wake_.notify_all();
+  int i;
+  while (take(&i)) {
+    lk.unlock();
+    fn(i);
+    lk.lock();
+    --pending_;
+  }
+  done_.wait(lk, [&] { return pending_ == 0; });
+  fn_ = nullptr;
+  parts_ = 0;
+}
+
+DcdError dcd_pread(const DcdFile& f, ReadPool& pool, void* dst, int64_t off, int64_t len) {
+  if (off < 0 || off + len > f.file_size) return io_eof();
+  const int64_t part = int64_t(2) << 20;
+  const int parts = (int)std::max<int64_t>(1, std::min<int64_t>((len + part - 1) / part, 4096));
+  if (parts == 1 || pool.size() == 1) return pread_full(f.fd, dst, len, off) ? DcdError() : io_eof();
+  const int64_t step = ((len + parts - 1) / parts + 4095) & ~int64_t(4095);
+  std::vector<char> ok((size_t)parts, 1);
+  pool.run(parts, [&](int p) {
+    const int64_t a = p * step, b = std::min(len, a + step);
+    if (a < b) ok[p] = pread_full(f.fd, static_cast<char*>(dst) + a, b - a, off + a);
+  });
   for (char c : ok)
     if (!c) return io_eof();
   return {};

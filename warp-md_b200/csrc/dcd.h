@@ -10,8 +10,12 @@
 
 #include <cuda_runtime.h>
 
+#include <condition_variable>
 #include <cstdint>
+#include <functional>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace wmd {
@@ -54,6 +58,27 @@ struct DcdFile {
   }
 };
 
+// Persistent threads for the parallel preads of a batch; the calling thread
+// takes parts too.
+class ReadPool {
+ public:
+  explicit ReadPool(int threads);
+  ~ReadPool();
+  int size() const { return (int)workers_.size() + 1; }
+  // fn(i) for every i in [0, parts), spread over the pool; returns when all are done
+  void run(int parts, const std::function<void(int)>& fn);
+
+ private:
+  void work();
+  bool take(int* i);
+  std::vector<std::thread> workers_;
+  std::mutex m_;
+  std::condition_variable wake_, done_;
+  const std::function<void(int)>* fn_ = nullptr;
+  int next_ = 0, parts_ = 0, pending_ = 0;
+  bool stop_ = false;
+};
+
 // Opens and parses the header (dcd.rs:45-95) and the frame layout.
 DcdError dcd_open(const char* path, float length_scale, DcdFile* f);
 void dcd_close(DcdFile* f);
@@ -61,8 +86,8 @@ void dcd_close(DcdFile* f);
 // sequential reader does (dcd.rs:207-291) and switches to the indexed layout;
 // the first damaged frame ends the readable range and becomes `end`.
 DcdError dcd_index(DcdFile* f);
-// pread of [off, off + len) into dst, split over `threads` threads.
-DcdError dcd_pread(const DcdFile& f, void* dst, int64_t off, int64_t len, int threads);
+// pread of [off, off + len) into dst in parts of a few MiB spread over the pool.
+DcdError dcd_pread(const DcdFile& f, ReadPool& pool, void* dst, int64_t off, int64_t len);
 // Box of one frame from its unit-cell payload (read_unitcell_with_len +
 // box_from_values, dcd.rs:978-1093): returns 0 none, 1 orthorhombic,
 // 2 triclinic; m = the box vectors a, b, c as rows.

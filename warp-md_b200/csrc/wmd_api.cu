@@ -20,6 +20,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <memory>
 #include <thread>
 #include <vector>
 
@@ -1590,7 +1591,7 @@ WMD_EXPORT int wmd_batched_layout(const wmd_ctx* ctx, int* tile_atoms, int* fram
 struct wmd_dcd {
   wmd::DcdFile f;
   int device = 0;
-  int threads = 8;  // parallel preads per batch
+  std::unique_ptr<wmd::ReadPool> pool;  // parallel preads per batch
   HostBuf pin[2];   // raw file bytes of a batch (+ the X-offset table of an indexed file)
   DevBuf raw[2], coords;
   cudaEvent_t h2d_done[2] = {nullptr, nullptr};
@@ -1683,7 +1684,7 @@ int dcd_stream(wmd_ctx* ctx, wmd_dcd* d, int64_t first, int64_t n, const uint32_
     const size_t padded = ((size_t)bytes + 15) & ~size_t(15);
     CU(cudaEventSynchronize(d->h2d_done[b]), "pinned slot wait");
     uint8_t* hp = static_cast<uint8_t*>(d->pin[b].ptr);
-    if (wmd::DcdError e = wmd::dcd_pread(F, hp, base, bytes, d->threads)) return dcd_err(ctx, e);
+    if (wmd::DcdError e = wmd::dcd_pread(F, *d->pool, hp, base, bytes)) return dcd_err(ctx, e);
     size_t copy = padded;
     if (F.indexed) {
       int64_t* tab = reinterpret_cast<int64_t*>(hp + padded);
@@ -1744,7 +1745,12 @@ WMD_EXPORT int wmd_dcd_open(wmd_ctx* ctx, const char* path, float length_scale, 
     return dcd_err(ctx, e);
   }
   const unsigned hw = std::thread::hardware_concurrency();
-  d->threads = (int)std::max(1u, std::min(8u, hw ? hw : 1u));
+  int threads = (int)std::max(1u, std::min(16u, hw ? hw : 1u));
+  if (const char* v = std::getenv("WMD_DCD_THREADS")) {  // pread threads per batch
+    const int t = std::atoi(v);
+    if (t > 0 && t <= 64) threads = t;
+  }
+  d->pool.reset(new wmd::ReadPool(threads));
   for (int k = 0; k < 2; ++k) {
     cudaError_t e = cudaEventCreateWithFlags(&d->h2d_done[k], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&d->consumed[k], cudaEventDisableTiming);
