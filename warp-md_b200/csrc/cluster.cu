@@ -230,7 +230,6 @@ __global__ void medoid_pick_kernel(int64_t n, const int* labels, const double* s
 // reference's up to exact FP64 ties.
 // ---------------------------------------------------------------------------
 
-constexpr int kKmChunk = 16;  // centers per pass of the assignment kernel
 
 // feat[i][3a + c] = (R_i x_ia + t_i)_c
 template <int STRIDE>
@@ -251,113 +250,171 @@ __global__ void kmeans_features_kernel(const float* __restrict__ coords, int64_t
   }
 }
 
-// labels[i] = argmin_c sum_k (feat[i][k] - centers[c][k])^2, first minimum;
-// dist_own[i] (optional) = the distance to the chosen center.
-__global__ void __launch_bounds__(128) kmeans_assign_kernel(const double* __restrict__ feat, int64_t n, int64_t nf,
-                                                            const double* __restrict__ centers, int k,
-                                                            int* __restrict__ labels, double* __restrict__ dist_own) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double* row = feat + (size_t)i * nf;
-  int best = 0;
+// Assignment tiles: kAsRows samples x kAsCenters centers per block, features
+// staged through shared memory kAsTile at a time (coalesced row loads).  A
+// warp owns kAsCPT centers for its 32 samples (lane = sample); every distance
+// is still the sequential sum over features in order with an unfused multiply
+// then add, as the reference's sq_dist.  Zero padding past nf adds exact
+// zeros.
+constexpr int kAsRows = 32;
+constexpr int kAsWarps = 8;
+constexpr int kAsCPT = 2;
+constexpr int kAsCenters = kAsWarps * kAsCPT;
+constexpr int kAsTile = 64;
+
+// labels[i] = argmin_c |feat[i] - centers[c]|^2 (first minimum), or, when
+// own_labels is given, dist[i] = the distance to centers[own_labels[i]] and
+// the per-cluster minimum as ordered bits in best_bits.
+__global__ void __launch_bounds__(kAsWarps * 32) kmeans_assign_kernel(
+    const double* __restrict__ feat, int64_t n, int64_t nf, const double* __restrict__ centers, int k,
+    int* __restrict__ labels, const int* __restrict__ own_labels, double* __restrict__ dist,
+    unsigned long long* __restrict__ best_bits) {
+  __shared__ double xs[kAsRows][kAsTile + 1];
+  __shared__ double cs[kAsCenters][kAsTile];
+  __shared__ double dsm[kAsCenters][kAsRows];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t row0 = (int64_t)blockIdx.x * kAsRows;
+  const int64_t my_row = row0 + lane;
+  const int own = (own_labels && warp == 0 && my_row < n) ? own_labels[my_row] : -1;
   double best_d = __longlong_as_double(0x7ff0000000000000ll);  // +inf
-  for (int c0 = 0; c0 < k; c0 += kKmChunk) {
-    const int cn = min(kKmChunk, k - c0);
-    double d[kKmChunk];
+  double own_d = 0.0;
+  int best = 0;
+  for (int c0 = 0; c0 < k; c0 += kAsCenters) {
+    double d[kAsCPT];
 #pragma unroll
-    for (int c = 0; c < kKmChunk; ++c) d[c] = 0.0;
-    for (int64_t j = 0; j < nf; ++j) {
-      const double v = row[j];
+    for (int p = 0; p < kAsCPT; ++p) d[p] = 0.0;
+    for (int64_t j0 = 0; j0 < nf; j0 += kAsTile) {
+      const int tw = (int)min((int64_t)kAsTile, nf - j0);
+      for (int e = tid; e < kAsRows * kAsTile; e += kAsWarps * 32) {
+        const int r = e / kAsTile, q = e - r * kAsTile;
+        const int64_t row = row0 + r;
+        xs[r][q] = (row < n && q < tw) ? __ldg(feat + (size_t)row * nf + j0 + q) : 0.0;
+      }
+      for (int e = tid; e < kAsCenters * kAsTile; e += kAsWarps * 32) {
+        const int cc = e / kAsTile, q = e - cc * kAsTile;
+        const int c = c0 + cc;
+        cs[cc][q] = (c < k && q < tw) ? __ldg(centers + (size_t)c * nf + j0 + q) : 0.0;
+      }
+      __syncthreads();
+#pragma unroll 16
+      for (int q = 0; q < kAsTile; ++q) {
+        const double x = xs[lane][q];
 #pragma unroll
-      for (int c = 0; c < kKmChunk; ++c)
-        if (c < cn) {
-          const double e = v - __ldg(centers + (size_t)(c0 + c) * nf + j);
-          d[c] = __dadd_rn(d[c], __dmul_rn(e, e));  // d*d then +, unfused, as sq_dist
+        for (int p = 0; p < kAsCPT; ++p) {
+          const double e = x - cs[warp * kAsCPT + p][q];
+          d[p] = __dadd_rn(d[p], __dmul_rn(e, e));
         }
+      }
+      __syncthreads();
     }
 #pragma unroll
-    for (int c = 0; c < kKmChunk; ++c)
-      if (c < cn && d[c] < best_d) {
-        best_d = d[c];
-        best = c0 + c;
+    for (int p = 0; p < kAsCPT; ++p) dsm[warp * kAsCPT + p][lane] = d[p];
+    __syncthreads();
+    if (warp == 0) {
+      for (int cc = 0; cc < kAsCenters && c0 + cc < k; ++cc) {
+        const double v = dsm[cc][lane];
+        if (v < best_d) {
+          best_d = v;
+          best = c0 + cc;
+        }
+        if (c0 + cc == own) own_d = v;
       }
+    }
+    __syncthreads();
   }
-  labels[i] = best;
-  if (dist_own) dist_own[i] = best_d;
+  if (warp != 0 || my_row >= n) return;
+  if (!own_labels) {
+    labels[my_row] = best;
+  } else {
+    dist[my_row] = own_d;
+    if (own >= 0) atomicMin(best_bits + own, (unsigned long long)__double_as_longlong(own_d));
+  }
 }
 
-// Per feature column j: sums[c][j] over the samples of cluster c, in index
-// order (threads own columns, so loads are coalesced), and counts.
-__global__ void __launch_bounds__(128) kmeans_sums_kernel(const double* __restrict__ feat, int64_t n, int64_t nf,
-                                                          const int* __restrict__ labels, int k,
-                                                          double* __restrict__ sums, int* __restrict__ counts) {
-  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int c0 = blockIdx.y * kKmChunk;
-  const int cn = min(kKmChunk, k - c0);
-  if (j >= nf) return;
-  double acc[kKmChunk];
-  int cnt[kKmChunk];
+// Per-cluster sums in sample order.  Block = (256 feature columns, one
+// cluster); each warp scans the labels 32 at a time, queues the members'
+// indices in shared memory in index order (ballot + prefix count) and adds
+// their rows kSumBatch at a time, so kSumBatch coalesced row loads per lane
+// are in flight while the sum itself stays sequential.
+constexpr int kSumWarps = 8;
+constexpr int kSumBatch = 16;
+
+__global__ void __launch_bounds__(kSumWarps * 32) kmeans_sums_kernel(const double* __restrict__ feat, int64_t n,
+                                                                     int64_t nf, const int* __restrict__ labels,
+                                                                     int k, double* __restrict__ sums,
+                                                                     int* __restrict__ counts) {
+  __shared__ int queue[kSumWarps][kSumBatch + 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = blockIdx.y;
+  const int64_t col0 = ((int64_t)blockIdx.x * kSumWarps + warp) * 32;
+  if (col0 >= nf) return;  // warp-uniform
+  const int64_t col = col0 + lane;
+  const bool live = col < nf;
+  int* q = queue[warp];
+  double acc = 0.0;
+  int m = 0, cnt = 0;
+  auto flush = [&](int take) {
+    double v[kSumBatch];
 #pragma unroll
-  for (int c = 0; c < kKmChunk; ++c) { acc[c] = 0.0; cnt[c] = 0; }
-  for (int64_t i = 0; i < n; ++i) {
-    const int c = labels[i] - c0;
-    if (c < 0 || c >= cn) continue;
-    const double v = feat[(size_t)i * nf + j];
+    for (int p = 0; p < kSumBatch; ++p) v[p] = (p < take && live) ? __ldg(feat + (size_t)q[p] * nf + col) : 0.0;
 #pragma unroll
-    for (int q = 0; q < kKmChunk; ++q)
-      if (q == c) {
-        acc[q] += v;
-        ++cnt[q];
-      }
+    for (int p = 0; p < kSumBatch; ++p)
+      if (p < take) acc += v[p];
+  };
+  for (int64_t i0 = 0; i0 < n; i0 += 32) {
+    const int64_t i = i0 + lane;
+    const bool mine = i < n && __ldg(labels + i) == c;
+    const unsigned mask = __ballot_sync(0xffffffffu, mine);
+    if (mine) q[m + __popc(mask & ((1u << lane) - 1u))] = (int)i;
+    m += __popc(mask);
+    cnt += __popc(mask);
+    __syncwarp();
+    while (m >= kSumBatch) {
+      flush(kSumBatch);
+      const int rest = m - kSumBatch;  // < 32
+      const int t = lane < rest ? q[kSumBatch + lane] : 0;
+      __syncwarp();
+      if (lane < rest) q[lane] = t;
+      m = rest;
+      __syncwarp();
+    }
   }
-  for (int q = 0; q < cn; ++q) sums[(size_t)(c0 + q) * nf + j] = acc[q];
-  if (j == 0)
-    for (int q = 0; q < cn; ++q) counts[c0 + q] = cnt[q];
+  if (m > 0) flush(m);
+  if (live) sums[(size_t)c * nf + col] = acc;
+  if (col == 0) counts[c] = cnt;
 }
 
 // New centers: sums / count, or the sample reseed[c] for an empty cluster;
-// shift[c] = |old - new| (features in order).  A block per cluster, thread 0
-// keeps the sequential shift sum.
+// shift[c] = |old - new| with the squares added in feature order (thread 0
+// over a shared-memory tile).  A block per cluster.
+constexpr int kCtrTile = 2048;
+
 __global__ void __launch_bounds__(256) kmeans_centers_kernel(const double* __restrict__ feat, int64_t nf,
                                                              const double* __restrict__ sums,
                                                              const int* __restrict__ counts,
                                                              const int64_t* __restrict__ reseed,
                                                              const double* __restrict__ old_c,
                                                              double* __restrict__ new_c, double* __restrict__ shift) {
+  __shared__ double sq[kCtrTile];
   const int c = blockIdx.x;
   const int64_t src = reseed[c];
   const double inv = counts[c] > 0 ? 1.0 / (double)counts[c] : 0.0;
-  for (int64_t j = threadIdx.x; j < nf; j += blockDim.x)
-    new_c[(size_t)c * nf + j] = src >= 0 ? feat[(size_t)src * nf + j] : sums[(size_t)c * nf + j] * inv;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int64_t j = 0; j < nf; ++j) {
-      const double e = old_c[(size_t)c * nf + j] - new_c[(size_t)c * nf + j];
-      s = __dadd_rn(s, __dmul_rn(e, e));
-    }
-    shift[c] = sqrt(s);
-  }
-}
-
-// Distance of each sample to its own cluster's center (features in order) and
-// the per-cluster minimum as ordered bits (non-negative doubles).
-__global__ void __launch_bounds__(128) kmeans_own_dist_kernel(const double* __restrict__ feat, int64_t n, int64_t nf,
-                                                              const double* __restrict__ centers,
-                                                              const int* __restrict__ labels, double* __restrict__ d,
-                                                              unsigned long long* __restrict__ best_bits) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int c = labels[i];
-  const double* row = feat + (size_t)i * nf;
-  const double* ctr = centers + (size_t)c * nf;
   double s = 0.0;
-  for (int64_t j = 0; j < nf; ++j) {
-    const double e = row[j] - ctr[j];
-    s = __dadd_rn(s, __dmul_rn(e, e));
+  for (int64_t j0 = 0; j0 < nf; j0 += kCtrTile) {
+    const int tw = (int)min((int64_t)kCtrTile, nf - j0);
+    for (int j = threadIdx.x; j < tw; j += blockDim.x) {
+      const size_t at = (size_t)c * nf + j0 + j;
+      const double v = src >= 0 ? feat[(size_t)src * nf + j0 + j] : sums[at] * inv;
+      new_c[at] = v;
+      const double e = old_c[at] - v;
+      sq[j] = __dmul_rn(e, e);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int j = 0; j < tw; ++j) s = __dadd_rn(s, sq[j]);
+    __syncthreads();
   }
-  d[i] = s;
-  atomicMin(best_bits + c, (unsigned long long)__double_as_longlong(s));
+  if (threadIdx.x == 0) shift[c] = sqrt(s);
 }
 
 __global__ void kmeans_gather_kernel(const double* __restrict__ feat, int64_t nf, const int64_t* __restrict__ idx,
@@ -420,14 +477,17 @@ cudaError_t kmeans_gather(const double* feat, int64_t nf, const int64_t* idx, in
 
 cudaError_t kmeans_assign(const double* feat, int64_t n, int64_t nf, const double* centers, int k, int* labels,
                           double* dist_own, cudaStream_t s) {
-  kmeans_assign_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(feat, n, nf, centers, k, labels, dist_own);
+  (void)dist_own;
+  kmeans_assign_kernel<<<(unsigned)((n + kAsRows - 1) / kAsRows), kAsWarps * 32, 0, s>>>(feat, n, nf, centers, k,
+                                                                                       labels, nullptr, nullptr,
+                                                                                       nullptr);
   return cudaGetLastError();
 }
 
 cudaError_t kmeans_sums(const double* feat, int64_t n, int64_t nf, const int* labels, int k, double* sums, int* counts,
                         cudaStream_t s) {
-  const dim3 grid((unsigned)((nf + 127) / 128), (unsigned)((k + kKmChunk - 1) / kKmChunk));
-  kmeans_sums_kernel<<<grid, 128, 0, s>>>(feat, n, nf, labels, k, sums, counts);
+  const dim3 grid((unsigned)((nf + kSumWarps * 32 - 1) / (kSumWarps * 32)), (unsigned)k);
+  kmeans_sums_kernel<<<grid, kSumWarps * 32, 0, s>>>(feat, n, nf, labels, k, sums, counts);
   return cudaGetLastError();
 }
 
@@ -446,7 +506,9 @@ cudaError_t kmeans_finish(const double* feat, int64_t n, int64_t nf, const doubl
   if ((e = cudaMemsetAsync(best_bits, 0xff, (size_t)k * sizeof(unsigned long long), s)) != cudaSuccess) return e;
   const unsigned lin = (unsigned)((n + 127) / 128);
   sizes_kernel<<<lin, 128, 0, s>>>(labels, n, sizes);
-  kmeans_own_dist_kernel<<<lin, 128, 0, s>>>(feat, n, nf, centers, labels, dist, best_bits);
+  kmeans_assign_kernel<<<(unsigned)((n + kAsRows - 1) / kAsRows), kAsWarps * 32, 0, s>>>(feat, n, nf, centers, k,
+                                                                                       nullptr, labels, dist,
+                                                                                       best_bits);
   medoid_pick_kernel<<<lin, 128, 0, s>>>(n, labels, dist, best_bits, centroids);
   return cudaGetLastError();
 }
