@@ -522,7 +522,13 @@ size_t frame_smem_bytes(int stride, int tile_atoms) {
   return stride == 4 ? Geo<4, kApt>::kSmemBytes : Geo<3, kApt>::kSmemBytes;
 }
 
+void frame_plan(FrameLaunch& L) {
+  L.lanes = lanes_eligible(L);
+  L.tile_atoms = L.lanes ? kLaneTile : kConsumerThreads * kApt;
+}
+
 int frame_grid(const FrameLaunch& L, int sm_count, bool backward) {
+  if (L.lanes && !backward) return lanes_grid(L, sm_count);
   static int cache[2][2][2] = {};  // [bwd][stride4][gather]
   int& occ = cache[backward ? 1 : 0][L.stride == 4][L.gather ? 1 : 0];
   if (occ == 0) occ = backward ? occupancy<kBwd>(L) : occupancy<kFwdFit>(L);
@@ -534,7 +540,7 @@ int frame_grid(const FrameLaunch& L, int sm_count, bool backward) {
 cudaError_t launch_rmsd_forward(const FrameLaunch& L, cudaStream_t s) {
   if (L.n_frames == 0) return cudaSuccess;
   if (!L.align) {
-    cudaError_t e = dispatch<kFwdRaw>(L, s);
+    cudaError_t e = L.lanes ? launch_lanes_forward(L, true, s) : dispatch<kFwdRaw>(L, s);
     if (e != cudaSuccess) return e;
     rmsd_finalize_kernel<kFwdRaw><<<(unsigned)((L.n_frames + 7) / 8), 256, 0, s>>>(L, frame_tiles(L));
     return cudaGetLastError();
@@ -543,7 +549,7 @@ cudaError_t launch_rmsd_forward(const FrameLaunch& L, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(L.refine_count, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
   }
-  cudaError_t e = dispatch<kFwdFit>(L, s);
+  cudaError_t e = L.lanes ? launch_lanes_forward(L, false, s) : dispatch<kFwdFit>(L, s);
   if (e != cudaSuccess) return e;
   rmsd_finalize_kernel<kFwdFit><<<(unsigned)((L.n_frames + 7) / 8), 256, 0, s>>>(L, frame_tiles(L));
   if ((e = cudaGetLastError()) != cudaSuccess || !L.refine) return e;

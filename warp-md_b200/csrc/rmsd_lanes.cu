@@ -1,0 +1,326 @@
+// rmsd_lanes.cu -- per-frame RMSD statistics with frames across lanes.
+//
+// The atom-major streaming kernel (rmsd_frames.cu) gives every thread a few
+// atoms of one frame, so each (tile, frame) item ends in a 15-value
+// cross-lane reduction and a CTA barrier; those cost about as many
+// instructions as the FP64 arithmetic itself.  Here the roles are swapped:
+//
+//   * A warp owns a run of stages; a stage is 32 frames x 32 atoms (lane l =
+//     frame 32g + l).  The frames' coordinates arrive by 2-D TMA (boxes of 32
+//     rows x 128 bytes, 128-byte swizzle, so that every lane reading "its"
+//     row hits a different bank group), the 32 reference atoms (centred,
+//     FP64) by a 1-D bulk copy next to them.  Two stages per warp, refilled
+//     by lane 0 as soon as the warp is done with one.
+//   * Each lane adds, in FP64 and in atom order, the 15 sums of its own frame
+//     (sum x, sum x_a^2, sum x y_c^T): no shuffles, no barriers.
+//   * Atoms are grouped into 2,048-atom tiles; a unit is (tile, 32-frame
+//     group) and belongs to one warp, which stores each lane's 16 sums into
+//     the same [frame][tile][16] partials the finalize kernel reads.  Every
+//     warp gets the same number of whole units, so results do not depend on
+//     the launch shape and are bitwise reproducible.
+//
+// Requirements (else the atom-major kernel runs): dense selection (the first
+// n_sel atoms), a 16-byte aligned base and a frame stride that is a multiple
+// of 16 bytes (n_atoms % 4 == 0 for packed xyz).  The reference centred
+// coordinates must be padded with 32 zero atoms (the bulk copy of the last
+// stage reads past n_sel).
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+
+#include "device_util.cuh"
+#include "wmd_internal.h"
+
+namespace wmd {
+
+namespace {
+
+constexpr int kLaneWarps = 4;   // warps per CTA
+constexpr int kLaneStages = 2;  // stage ring per warp
+constexpr int kLaneAtoms = 32;  // atoms per stage
+
+template <int STRIDE>
+struct LaneGeo {
+  static constexpr int kBoxes = kLaneAtoms * STRIDE / 32;  // [32 frames][32 floats] boxes per stage
+  static constexpr int kXBytes = kBoxes * 32 * 32 * 4;
+  static constexpr int kYBytes = kLaneAtoms * 3 * 8;
+  static constexpr int kStageBytes = (kXBytes + kYBytes + 1023) / 1024 * 1024;
+  static constexpr int kBarOffset = kLaneWarps * kLaneStages * kStageBytes;
+  static constexpr int kAbortOffset = kBarOffset + kLaneWarps * kLaneStages * 8;
+  static constexpr int kSmemBytes = kAbortOffset + 16 + 1024;  // + slack to align the base to 1024
+};
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// One lane's sums over the valid atoms of a stage (valid is warp-uniform).
+// Packed xyz: 4 atoms = 3 swizzled 16-byte chunks; xyzw: 1 atom = 1 chunk.
+template <int STRIDE, bool RAW>
+__device__ __forceinline__ void stage_sums(double (&acc)[15], const unsigned char* st, int lane, int valid,
+                                           const FrameLaunch& L) {
+  const unsigned char* row = st + lane * 128;
+  const int sw = lane & 7;
+  auto chunk = [&](int c) -> float4 {
+    return *reinterpret_cast<const float4*>(row + (c >> 3) * 4096 + (((c & 7) ^ sw) << 4));
+  };
+  const double2* yb = reinterpret_cast<const double2*>(st + LaneGeo<STRIDE>::kXBytes);
+  auto add_atom = [&](float fx, float fy, float fz, double y0, double y1, double y2, bool in) {
+    const double x0 = fx, x1 = fy, x2 = fz;
+    if (RAW) {
+      const double d0 = x0 - (y0 + L.ref.mean[0]);
+      const double d1 = x1 - (y1 + L.ref.mean[1]);
+      const double d2 = x2 - (y2 + L.ref.mean[2]);
+      acc[0] = fma(d0, in ? d0 : 0.0, acc[0]);
+      acc[1] = fma(d1, in ? d1 : 0.0, acc[1]);
+      acc[2] = fma(d2, in ? d2 : 0.0, acc[2]);
+    } else {
+      acc[0] += x0; acc[1] += x1; acc[2] += x2;
+      acc[3] = fma(x0, x0, acc[3]); acc[4] = fma(x1, x1, acc[4]); acc[5] = fma(x2, x2, acc[5]);
+      acc[6] = fma(x0, y0, acc[6]);  acc[7] = fma(x0, y1, acc[7]);  acc[8] = fma(x0, y2, acc[8]);
+      acc[9] = fma(x1, y0, acc[9]);  acc[10] = fma(x1, y1, acc[10]); acc[11] = fma(x1, y2, acc[11]);
+      acc[12] = fma(x2, y0, acc[12]); acc[13] = fma(x2, y1, acc[13]); acc[14] = fma(x2, y2, acc[14]);
+    }
+  };
+  if (STRIDE == 3) {
+#pragma unroll
+    for (int m = 0; m < kLaneAtoms / 4; ++m) {
+      if (4 * m >= valid) break;
+      const float4 a = chunk(3 * m), b = chunk(3 * m + 1), c = chunk(3 * m + 2);
+      const double2 y01 = yb[6 * m + 0], y23 = yb[6 * m + 1], y45 = yb[6 * m + 2];
+      const double2 y67 = yb[6 * m + 3], y89 = yb[6 * m + 4], yab = yb[6 * m + 5];
+      add_atom(a.x, a.y, a.z, y01.x, y01.y, y23.x, 4 * m + 0 < valid);
+      add_atom(a.w, b.x, b.y, y23.y, y45.x, y45.y, 4 * m + 1 < valid);
+      add_atom(b.z, b.w, c.x, y67.x, y67.y, y89.x, 4 * m + 2 < valid);
+      add_atom(c.y, c.z, c.w, y89.y, yab.x, yab.y, 4 * m + 3 < valid);
+    }
+  } else {
+#pragma unroll
+    for (int m = 0; m < kLaneAtoms / 2; ++m) {
+      if (2 * m >= valid) break;
+      const float4 a = chunk(2 * m), b = chunk(2 * m + 1);
+      const double2 y01 = yb[3 * m + 0], y23 = yb[3 * m + 1], y45 = yb[3 * m + 2];
+      add_atom(a.x, a.y, a.z, y01.x, y01.y, y23.x, 2 * m + 0 < valid);
+      add_atom(b.x, b.y, b.z, y23.y, y45.x, y45.y, 2 * m + 1 < valid);
+    }
+  }
+}
+
+template <int STRIDE, bool RAW>
+__global__ void __launch_bounds__(kLaneWarps * 32) rmsd_lanes_kernel(const __grid_constant__ CUtensorMap map,
+                                                                     const FrameLaunch L) {
+  using G = LaneGeo<STRIDE>;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem = smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + G::kBarOffset);
+  uint64_t* full = bars + warp * kLaneStages;
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + G::kAbortOffset);
+  unsigned char* ring = smem + warp * kLaneStages * G::kStageBytes;
+
+  const int64_t F = L.n_frames, n_sel = L.ref.n_sel;
+  const int64_t groups = (F + 31) / 32;
+  const int n_tiles = (int)((n_sel + kLaneTile - 1) / kLaneTile);
+  const int64_t units = groups * n_tiles;  // (tile, frame group), tile-major
+  const int64_t nw = L.lane_warps, gw = (int64_t)blockIdx.x * kLaneWarps + warp;
+  const int64_t u0 = units * gw / nw, u1 = units * (gw + 1) / nw;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kLaneWarps * kLaneStages; ++i) mbar_init(&bars[i], 1);
+    *abort_flag = 0;
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (gw >= nw || u0 >= u1) return;
+
+  auto unit_stages = [&](int64_t u) {
+    const int64_t t = u / groups;
+    return (int)((min((int64_t)kLaneTile, n_sel - t * kLaneTile) + kLaneAtoms - 1) / kLaneAtoms);
+  };
+  // producer cursor (lane 0): unit pu, stage pk; n_issued stages so far
+  int64_t pu = u0;
+  int pk = 0, p_kst = unit_stages(u0);
+  int64_t n_issued = 0;
+  auto issue_next = [&]() {  // lane 0
+    const int64_t t = pu / groups, g = pu - t * groups;
+    const int slot = (int)(n_issued % kLaneStages);
+    unsigned char* dst = ring + slot * G::kStageBytes;
+    const int64_t a0 = t * kLaneTile + (int64_t)pk * kLaneAtoms;
+    // the warp's earlier generic reads of this slot before the async writes
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_arrive_expect_tx(&full[slot], G::kXBytes + G::kYBytes);
+#pragma unroll
+    for (int b = 0; b < G::kBoxes; ++b)
+      tma_load_2d(dst + b * 4096, &map, (int)(a0 * STRIDE + 32 * b), (int)(g * 32), &full[slot]);
+    bulk_copy_g2s(dst + G::kXBytes, L.ref.yc + a0 * 3, G::kYBytes, &full[slot]);
+    ++n_issued;
+    if (++pk == p_kst && ++pu < u1) {
+      pk = 0;
+      p_kst = unit_stages(pu);
+    }
+  };
+  if (lane == 0)
+    while (n_issued < kLaneStages && pu < u1) issue_next();
+
+  int64_t n_done = 0;
+  bool aborted = false;
+  for (int64_t u = u0; u < u1 && !aborted; ++u) {
+    const int64_t t = u / groups, g = u - t * groups;
+    const int kst = unit_stages(u);
+    double acc[15];
+#pragma unroll
+    for (int e = 0; e < 15; ++e) acc[e] = 0.0;
+    for (int k = 0; k < kst; ++k) {
+      const int slot = (int)(n_done % kLaneStages);
+      const uint32_t parity = (uint32_t)((n_done / kLaneStages) & 1);
+      if (!mbar_wait(&full[slot], parity, L.status, kStatusTimeoutFull, abort_flag)) {
+        aborted = true;
+        break;
+      }
+      const int64_t a0 = t * kLaneTile + (int64_t)k * kLaneAtoms;
+      const int valid = (int)min((int64_t)kLaneAtoms, n_sel - a0);
+      stage_sums<STRIDE, RAW>(acc, ring + slot * G::kStageBytes, lane, valid, L);
+      ++n_done;
+      __syncwarp();
+      if (lane == 0 && pu < u1) issue_next();
+    }
+    if (aborted) break;
+    if (RAW) {  // the no-fit record holds sum |x - y|^2 in its first word
+      acc[0] += acc[1] + acc[2];
+      acc[1] = acc[2] = 0.0;
+    }
+    const int64_t f = g * 32 + lane;
+    if (f < F) {
+      double* rec = L.partial + ((size_t)f * n_tiles + t) * kStatDoubles;
+#pragma unroll
+      for (int e = 0; e < 15; ++e) rec[e] = acc[e];
+      rec[15] = 0.0;
+    }
+  }
+
+  // after an abort, copies this warp issued may still be landing
+  if (aborted && lane == 0) {
+    for (int64_t j = n_done; j < n_issued; ++j) {
+      const int slot = (int)(j % kLaneStages);
+      const uint32_t ph = (uint32_t)((j / kLaneStages) & 1);
+      const uint64_t t0 = global_timer_ns();
+      while (!mbar_try_wait(&full[slot], ph)) {
+        if (global_timer_ns() - t0 > kWaitLimitNs) {
+          atomicOr(L.status, kStatusTimeoutDrain);
+          break;
+        }
+      }
+    }
+  }
+}
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn() {
+  static EncodeTiled fn = nullptr;
+  if (fn) return fn;
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult qr;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &qr) != cudaSuccess ||
+      qr != cudaDriverEntryPointSuccess || !p) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  fn = reinterpret_cast<EncodeTiled>(p);
+  return fn;
+}
+
+int64_t lane_units(const FrameLaunch& L) {
+  return ((L.n_frames + 31) / 32) * ((L.ref.n_sel + kLaneTile - 1) / kLaneTile);
+}
+
+template <int STRIDE, bool RAW>
+int lanes_occupancy() {
+  auto kern = rmsd_lanes_kernel<STRIDE, RAW>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, LaneGeo<STRIDE>::kSmemBytes);
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kLaneWarps * 32, LaneGeo<STRIDE>::kSmemBytes) !=
+      cudaSuccess)
+    b = 1;
+  return std::max(b, 1);
+}
+
+template <int STRIDE, bool RAW>
+cudaError_t launch_lanes(const FrameLaunch& L, cudaStream_t s) {
+  EncodeTiled enc = encode_fn();
+  if (!enc) return cudaErrorNotSupported;
+  CUtensorMap map;
+  const cuuint64_t dims[2] = {(cuuint64_t)(L.ref.n_sel * STRIDE), (cuuint64_t)L.n_frames};
+  const cuuint64_t strides[1] = {(cuuint64_t)(L.n_atoms * STRIDE * 4)};
+  const cuuint32_t box[2] = {32, 32};
+  const cuuint32_t estr[2] = {1, 1};
+  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(L.coords), dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return cudaErrorInvalidValue;
+  auto kern = rmsd_lanes_kernel<STRIDE, RAW>;
+  static bool attr_done[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!attr_done[dev]) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, LaneGeo<STRIDE>::kSmemBytes);
+    if (e != cudaSuccess) return e;
+    attr_done[dev] = true;
+  }
+  kern<<<L.grid, kLaneWarps * 32, LaneGeo<STRIDE>::kSmemBytes, s>>>(map, L);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+bool lanes_eligible(const FrameLaunch& L) {
+  static int mode = -1;
+  if (mode < 0) {
+    const char* e = std::getenv("WMD_FRAMES_KERNEL");
+    mode = (e && std::strcmp(e, "atoms") == 0) ? 0 : 1;
+  }
+  if (!mode || L.gather || L.ref.n_sel <= 0 || L.n_frames <= 0) return false;
+  if (L.stride != 4 && (L.n_atoms & 3) != 0) return false;
+  if ((reinterpret_cast<uintptr_t>(L.coords) & 15u) != 0) return false;
+  if (L.ref.n_sel * L.stride >= (int64_t(1) << 31) || L.n_frames >= (int64_t(1) << 31)) return false;
+  return true;
+}
+
+// Active warps: every warp gets the same number of whole units (the last one
+// possibly fewer), as many warps as the SMs hold at most.
+static int64_t lane_warps(const FrameLaunch& L, int sm_count) {
+  static int occ[2] = {0, 0};
+  int& o = occ[L.stride == 4 ? 1 : 0];
+  if (o == 0) o = L.stride == 4 ? lanes_occupancy<4, false>() : lanes_occupancy<3, false>();
+  const int64_t units = lane_units(L);
+  const int64_t slots = (int64_t)sm_count * o * kLaneWarps;
+  const int64_t per = (units + slots - 1) / slots;
+  return std::max<int64_t>(1, (units + per - 1) / per);
+}
+
+int lanes_grid(const FrameLaunch& L, int sm_count) {
+  return (int)((lane_warps(L, sm_count) + kLaneWarps - 1) / kLaneWarps);
+}
+
+cudaError_t launch_lanes_forward(const FrameLaunch& L, bool raw, cudaStream_t s) {
+  FrameLaunch K = L;
+  const int64_t units = lane_units(L);
+  const int64_t slots = (int64_t)L.grid * kLaneWarps;
+  const int64_t per = (units + slots - 1) / slots;
+  K.lane_warps = (int)std::max<int64_t>(1, (units + per - 1) / per);
+  if (L.stride == 4) return raw ? launch_lanes<4, true>(K, s) : launch_lanes<4, false>(K, s);
+  return raw ? launch_lanes<3, true>(K, s) : launch_lanes<3, false>(K, s);
+}
+
+}  // namespace wmd

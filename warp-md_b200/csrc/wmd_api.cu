@@ -276,6 +276,9 @@ int forward_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames, int64_t
   wmd::FrameLaunch L = base_launch(ctx, ref, n_atoms, stride, dsel);
   L.align = align;
   L.gather = dsel != nullptr || (reinterpret_cast<uintptr_t>(dcoords) & 15u) != 0;
+  L.coords = dcoords;
+  L.n_frames = n_frames;
+  wmd::frame_plan(L);
   const int tiles = wmd::frame_tiles(L);
   const size_t per_frame = (size_t)tiles * wmd::kStatDoubles * sizeof(double);
   int64_t batch = std::max<int64_t>(1, (int64_t)(kPartialBytesMax / per_frame));
@@ -523,7 +526,11 @@ static int reference_upload(wmd_ctx* ctx, const float* ref, int64_t n_sel, int s
       }
     I.gy = gy.value();
   }
-  cudaError_t e = cudaMalloc(&r->yc, yc.size() * sizeof(double));
+  // 32 zero atoms after the reference: the frames-across-lanes kernel copies
+  // whole 32-atom blocks of it
+  const size_t yc_pad = 32 * 3;
+  cudaError_t e = cudaMalloc(&r->yc, (yc.size() + yc_pad) * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemset(r->yc + yc.size(), 0, yc_pad * sizeof(double));
   if (e == cudaSuccess && weights && n_sel > 0) e = cudaMalloc(&r->w, (size_t)n_sel * sizeof(float));
   if (e != cudaSuccess) {
     cudaFree(r->yc);

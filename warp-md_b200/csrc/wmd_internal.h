@@ -42,7 +42,9 @@ struct FrameLaunch {
   int stride = 3;                 // floats per atom (3 or 4)
   const uint32_t* sel = nullptr;  // device indices, or null (dense 0..n_sel-1)
   bool gather = false;            // plain loads (selection or unaligned base)
-  int tile_atoms = 2048;          // atoms per tile (kConsumerThreads * atoms/thread)
+  int tile_atoms = 2048;          // atoms per tile (kConsumerThreads * atoms/thread, or kLaneTile)
+  bool lanes = false;             // frames-across-lanes forward kernel (rmsd_lanes.cu)
+  int lane_warps = 0;             // its active warps (set at launch)
   int align = 1;
   RefInfo ref;
   FrameOutputs out;
@@ -66,6 +68,15 @@ constexpr double kRefineScale = 1e-7;
 void set_thread_error(const char* msg);
 
 int frame_tiles(const FrameLaunch& L);
+// Picks the forward kernel for a launch (sets lanes and tile_atoms); call
+// before sizing the partials with frame_tiles.
+void frame_plan(FrameLaunch& L);
+// frames-across-lanes forward (rmsd_lanes.cu): tile of 2,048 atoms per
+// partial record
+constexpr int kLaneTile = 2048;
+bool lanes_eligible(const FrameLaunch& L);
+int lanes_grid(const FrameLaunch& L, int sm_count);
+cudaError_t launch_lanes_forward(const FrameLaunch& L, bool raw, cudaStream_t s);
 size_t frame_smem_bytes(int stride, int tile_atoms);
 // Forward: zeroes L.refine_count, runs the fused kernel, then the residual pass
 // over the frames it flagged.
