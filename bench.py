@@ -956,7 +956,8 @@ def run_ours(args):
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6650 GB/s",
-                         "kernel": "wmd::rmsd_frames_kernel (fused forward)", "kernel_ms": kern_ms,
+                         "kernel": "wmd::rmsd_lanes_kernel (frames across lanes) + rmsd_finalize_kernel (QCP)",
+                         "kernel_ms": kern_ms,
                          "algorithmic_bytes_per_launch": alg_bytes},
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -76,6 +76,27 @@ def test_odd_shapes(gpu_ctx, n_atoms, n_frames):
     np.testing.assert_allclose(got, exp, rtol=0, atol=TOL)
 
 
+@pytest.mark.parametrize("n_atoms,n_frames,stride", [
+    (4, 1, 3), (36, 31, 3), (100, 33, 3), (2052, 65, 3), (4100, 3, 3), (8192, 40, 3),
+    (999, 33, 4), (2049, 5, 4), (64, 300, 4)])
+def test_frames_across_lanes_shapes(gpu_ctx, n_atoms, n_frames, stride):
+    """Shapes the frames-across-lanes kernel takes (packed xyz with n_atoms % 4
+    == 0, or xyzw): partial last stages and tiles, frame groups that are not
+    multiples of 32, both metrics."""
+    fr, ref = synth.make_trajectory(n_atoms, n_frames, (0.05, 2.0), seed=n_atoms + 31 * n_frames)
+    got = gpu_rmsd(gpu_ctx, fr, ref, stride=stride, device_io=True)
+    _, exp = oracle.rmsd_frames(fr, ref)
+    np.testing.assert_allclose(got, exp, rtol=0, atol=TOL)
+    raw = gpu_rmsd(gpu_ctx, fr, ref, stride=stride, align=False, device_io=True)
+    _, expr = oracle.rmsd_frames(fr, ref, align=False)
+    np.testing.assert_allclose(raw, expr, rtol=0, atol=TOL)
+    # a dense prefix of the frame (n_sel < n_atoms)
+    k = max(1, n_atoms // 2)
+    got = gpu_rmsd(gpu_ctx, fr, ref[:k], stride=stride, device_io=True)
+    _, exp = oracle.rmsd_frames(fr, ref[:k], selection=np.arange(k))
+    np.testing.assert_allclose(got, exp, rtol=0, atol=TOL)
+
+
 @pytest.mark.parametrize("stride", [3, 4])
 @pytest.mark.parametrize("device_io", [False, True])
 def test_layouts_and_memory_kinds(gpu_ctx, stride, device_io):

@@ -522,9 +522,9 @@ size_t frame_smem_bytes(int stride, int tile_atoms) {
   return stride == 4 ? Geo<4, kApt>::kSmemBytes : Geo<3, kApt>::kSmemBytes;
 }
 
-void frame_plan(FrameLaunch& L) {
+void frame_plan(FrameLaunch& L, int sm_count) {
   L.lanes = lanes_eligible(L);
-  L.tile_atoms = L.lanes ? kLaneTile : kConsumerThreads * kApt;
+  L.tile_atoms = L.lanes ? lanes_tile(L, sm_count) : kConsumerThreads * kApt;
 }
 
 int frame_grid(const FrameLaunch& L, int sm_count, bool backward) {

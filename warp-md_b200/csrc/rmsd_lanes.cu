@@ -13,8 +13,9 @@
 //     by lane 0 as soon as the warp is done with one.
 //   * Each lane adds, in FP64 and in atom order, the 15 sums of its own frame
 //     (sum x, sum x_a^2, sum x y_c^T): no shuffles, no barriers.
-//   * Atoms are grouped into 2,048-atom tiles; a unit is (tile, 32-frame
-//     group) and belongs to one warp, which stores each lane's 16 sums into
+//   * Atoms are grouped into tiles (256 to 2,048 atoms, chosen per launch so
+//     that whole units balance over the warp slots); a unit is (tile,
+//     32-frame group) and belongs to one warp, which stores each lane's 16 sums into
 //     the same [frame][tile][16] partials the finalize kernel reads.  Every
 //     warp gets the same number of whole units, so results do not depend on
 //     the launch shape and are bitwise reproducible.
@@ -128,7 +129,8 @@ __global__ void __launch_bounds__(kLaneWarps * 32) rmsd_lanes_kernel(const __gri
 
   const int64_t F = L.n_frames, n_sel = L.ref.n_sel;
   const int64_t groups = (F + 31) / 32;
-  const int n_tiles = (int)((n_sel + kLaneTile - 1) / kLaneTile);
+  const int64_t tile = L.tile_atoms;  // a multiple of kLaneAtoms
+  const int n_tiles = (int)((n_sel + tile - 1) / tile);
   const int64_t units = groups * n_tiles;  // (tile, frame group), tile-major
   const int64_t nw = L.lane_warps, gw = (int64_t)blockIdx.x * kLaneWarps + warp;
   const int64_t u0 = units * gw / nw, u1 = units * (gw + 1) / nw;
@@ -143,7 +145,7 @@ __global__ void __launch_bounds__(kLaneWarps * 32) rmsd_lanes_kernel(const __gri
 
   auto unit_stages = [&](int64_t u) {
     const int64_t t = u / groups;
-    return (int)((min((int64_t)kLaneTile, n_sel - t * kLaneTile) + kLaneAtoms - 1) / kLaneAtoms);
+    return (int)((min(tile, n_sel - t * tile) + kLaneAtoms - 1) / kLaneAtoms);
   };
   // producer cursor (lane 0): unit pu, stage pk; n_issued stages so far
   int64_t pu = u0;
@@ -153,7 +155,7 @@ __global__ void __launch_bounds__(kLaneWarps * 32) rmsd_lanes_kernel(const __gri
     const int64_t t = pu / groups, g = pu - t * groups;
     const int slot = (int)(n_issued % kLaneStages);
     unsigned char* dst = ring + slot * G::kStageBytes;
-    const int64_t a0 = t * kLaneTile + (int64_t)pk * kLaneAtoms;
+    const int64_t a0 = t * tile + (int64_t)pk * kLaneAtoms;
     // the warp's earlier generic reads of this slot before the async writes
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_arrive_expect_tx(&full[slot], G::kXBytes + G::kYBytes);
@@ -185,7 +187,7 @@ __global__ void __launch_bounds__(kLaneWarps * 32) rmsd_lanes_kernel(const __gri
         aborted = true;
         break;
       }
-      const int64_t a0 = t * kLaneTile + (int64_t)k * kLaneAtoms;
+      const int64_t a0 = t * tile + (int64_t)k * kLaneAtoms;
       const int valid = (int)min((int64_t)kLaneAtoms, n_sel - a0);
       stage_sums<STRIDE, RAW>(acc, ring + slot * G::kStageBytes, lane, valid, L);
       ++n_done;
@@ -199,10 +201,10 @@ __global__ void __launch_bounds__(kLaneWarps * 32) rmsd_lanes_kernel(const __gri
     }
     const int64_t f = g * 32 + lane;
     if (f < F) {
-      double* rec = L.partial + ((size_t)f * n_tiles + t) * kStatDoubles;
+      double2* rec = reinterpret_cast<double2*>(L.partial + ((size_t)f * n_tiles + t) * kStatDoubles);
 #pragma unroll
-      for (int e = 0; e < 15; ++e) rec[e] = acc[e];
-      rec[15] = 0.0;
+      for (int e = 0; e < 7; ++e) rec[e] = make_double2(acc[2 * e], acc[2 * e + 1]);
+      rec[7] = make_double2(acc[14], 0.0);
     }
   }
 
@@ -240,8 +242,8 @@ EncodeTiled encode_fn() {
   return fn;
 }
 
-int64_t lane_units(const FrameLaunch& L) {
-  return ((L.n_frames + 31) / 32) * ((L.ref.n_sel + kLaneTile - 1) / kLaneTile);
+int64_t lane_units(const FrameLaunch& L, int64_t tile) {
+  return ((L.n_frames + 31) / 32) * ((L.ref.n_sel + tile - 1) / tile);
 }
 
 template <int STRIDE, bool RAW>
@@ -297,28 +299,46 @@ bool lanes_eligible(const FrameLaunch& L) {
   return true;
 }
 
-// Active warps: every warp gets the same number of whole units (the last one
-// possibly fewer), as many warps as the SMs hold at most.
-static int64_t lane_warps(const FrameLaunch& L, int sm_count) {
+static int lanes_slots(int stride, int sm_count) {
   static int occ[2] = {0, 0};
-  int& o = occ[L.stride == 4 ? 1 : 0];
-  if (o == 0) o = L.stride == 4 ? lanes_occupancy<4, false>() : lanes_occupancy<3, false>();
-  const int64_t units = lane_units(L);
-  const int64_t slots = (int64_t)sm_count * o * kLaneWarps;
+  int& o = occ[stride == 4 ? 1 : 0];
+  if (o == 0) o = stride == 4 ? lanes_occupancy<4, false>() : lanes_occupancy<3, false>();
+  return sm_count * o * kLaneWarps;
+}
+
+// Active warps for `slots` warp slots: every warp gets the same number of
+// whole units (the last one possibly fewer).
+static int64_t lane_warps(const FrameLaunch& L, int64_t slots) {
+  const int64_t units = lane_units(L, L.tile_atoms);
   const int64_t per = (units + slots - 1) / slots;
   return std::max<int64_t>(1, (units + per - 1) / per);
 }
 
+int lanes_tile(const FrameLaunch& L, int sm_count) {
+  // Tile size from 2,048 down to 256 atoms minimising the busiest warp's
+  // bytes: (units per warp) x (tile bytes + its 128-byte partial, written
+  // and read back).  Large tiles mean few records; small ones balance short
+  // runs (few frames or few atoms) over all warp slots.
+  const int64_t slots = lanes_slots(L.stride, sm_count);
+  int64_t best = kLaneTile, best_cost = -1;
+  for (int64_t tile = kLaneTile; tile >= 256; tile /= 2) {
+    const int64_t per = (lane_units(L, tile) + slots - 1) / slots;
+    const int64_t cost = per * (tile * L.stride * 4 + 256);
+    if (best_cost < 0 || cost < best_cost) {
+      best = tile;
+      best_cost = cost;
+    }
+  }
+  return (int)best;
+}
+
 int lanes_grid(const FrameLaunch& L, int sm_count) {
-  return (int)((lane_warps(L, sm_count) + kLaneWarps - 1) / kLaneWarps);
+  return (int)((lane_warps(L, lanes_slots(L.stride, sm_count)) + kLaneWarps - 1) / kLaneWarps);
 }
 
 cudaError_t launch_lanes_forward(const FrameLaunch& L, bool raw, cudaStream_t s) {
   FrameLaunch K = L;
-  const int64_t units = lane_units(L);
-  const int64_t slots = (int64_t)L.grid * kLaneWarps;
-  const int64_t per = (units + slots - 1) / slots;
-  K.lane_warps = (int)std::max<int64_t>(1, (units + per - 1) / per);
+  K.lane_warps = (int)lane_warps(L, (int64_t)L.grid * kLaneWarps);
   if (L.stride == 4) return raw ? launch_lanes<4, true>(K, s) : launch_lanes<4, false>(K, s);
   return raw ? launch_lanes<3, true>(K, s) : launch_lanes<3, false>(K, s);
 }

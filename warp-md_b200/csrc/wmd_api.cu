@@ -278,7 +278,7 @@ int forward_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames, int64_t
   L.gather = dsel != nullptr || (reinterpret_cast<uintptr_t>(dcoords) & 15u) != 0;
   L.coords = dcoords;
   L.n_frames = n_frames;
-  wmd::frame_plan(L);
+  wmd::frame_plan(L, ctx->sm_count);
   const int tiles = wmd::frame_tiles(L);
   const size_t per_frame = (size_t)tiles * wmd::kStatDoubles * sizeof(double);
   int64_t batch = std::max<int64_t>(1, (int64_t)(kPartialBytesMax / per_frame));

@@ -70,11 +70,12 @@ void set_thread_error(const char* msg);
 int frame_tiles(const FrameLaunch& L);
 // Picks the forward kernel for a launch (sets lanes and tile_atoms); call
 // before sizing the partials with frame_tiles.
-void frame_plan(FrameLaunch& L);
-// frames-across-lanes forward (rmsd_lanes.cu): tile of 2,048 atoms per
+void frame_plan(FrameLaunch& L, int sm_count);
+// frames-across-lanes forward (rmsd_lanes.cu): at most 2,048 atoms per
 // partial record
 constexpr int kLaneTile = 2048;
 bool lanes_eligible(const FrameLaunch& L);
+int lanes_tile(const FrameLaunch& L, int sm_count);
 int lanes_grid(const FrameLaunch& L, int sm_count);
 cudaError_t launch_lanes_forward(const FrameLaunch& L, bool raw, cudaStream_t s);
 size_t frame_smem_bytes(int stride, int tile_atoms);
