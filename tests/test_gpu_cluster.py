@@ -83,6 +83,30 @@ def test_dbscan_chain_and_frame_subset():
     np.testing.assert_array_equal(out["labels"], labels)
 
 
+def test_dbscan_medoid_with_near_duplicate_frames():
+    """Near-duplicate frames give distances of ~1e-7 A next to ~1 A ones, so
+    the medoid sums take the sequential path (the lanes' partial sums could
+    round); labels, sizes and medoids still match the oracle exactly."""
+    import warp_md
+
+    rng = np.random.default_rng(4)
+    _, ref = synth.make_trajectory(40, 1, 0.0, 2)
+    base = ref[None] + rng.normal(0, 0.4, (60, 40, 3)).astype(np.float32)
+    dup = base[:20] + np.float32(1e-6) * rng.standard_normal((20, 40, 3)).astype(np.float32)
+    fr = np.concatenate([base, dup]).astype(np.float32)
+    system = _system(40)
+    traj = warp_md.Trajectory.from_numpy(fr)
+    sel = system.select("all")
+    d32, _ = oracle.pairwise(fr)
+    assert d32[d32 > 0].min() < 1e-5
+    for eps, ms in ((1.2, 3), (0.8, 2)):
+        out = warp_md.TrajectoryClusterPlan(sel, eps=eps, min_samples=ms).run(traj, system)
+        labels, cent, sizes = oracle.dbscan(d32, eps, ms)
+        np.testing.assert_array_equal(out["labels"], labels)
+        np.testing.assert_array_equal(out["centroids"], cent)
+        np.testing.assert_array_equal(out["sizes"], sizes)
+
+
 def test_kmeans_plan_matches_oracle():
     import warp_md
 

@@ -196,21 +196,50 @@ __global__ void sizes_kernel(const int* labels, int64_t n, unsigned* sizes) {
 }
 
 // sum[i] = sum over members j of i's cluster, in index order, of d(i, j), FP64
-// (a thread per point, sequential like the reference's loop).
+// (the reference's sequential loop).  A warp per point reads its row
+// coalesced.  The lanes' strided partial sums equal the sequential sum
+// whenever no addition in either order rounds: every term is a multiple of
+// 2^low (low = the smallest term's last mantissa bit) and the total is below
+// 2^(53 + low), so every partial sum of any subset is representable.  Rows
+// that miss that bound (tiny distances next to large ones) take the
+// sequential loop on lane 0.
 __global__ void __launch_bounds__(256) medoid_sum_kernel(const float* __restrict__ D, int64_t n,
                                                          const int* __restrict__ labels, double* __restrict__ sum,
                                                          unsigned long long* __restrict__ best_bits) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int c = labels[i];
-  if (c < 0) return;
-  const float* row = D + (size_t)i * n;
-  double s = 0.0;
-  for (int64_t j = 0; j < n; ++j)
-    if (labels[j] == c) s += j == i ? 0.0 : (double)row[j];
-  sum[i] = s;
-  // non-negative doubles order like their bit patterns
-  atomicMin(best_bits + c, (unsigned long long)__double_as_longlong(s));
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    const int c = labels[i];
+    if (c < 0) continue;  // warp-uniform
+    const float* row = D + (size_t)i * n;
+    double s = 0.0;
+    int low = 1 << 20;  // lowest set-able mantissa bit over the lane's terms
+    for (int64_t j = lane; j < n; j += 32) {
+      if (j == i || __ldg(labels + j) != c) continue;
+      const float v = __ldg(row + j);
+      if (v == 0.0f) continue;
+      const int e = (int)((__float_as_uint(v) >> 23) & 0xffu);
+      low = min(low, (e == 0 ? 1 : e) - 150);  // value = m * 2^(e - 150), subnormals 2^-149
+      s += (double)v;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      s += __shfl_xor_sync(0xffffffffu, s, o);
+      low = min(low, __shfl_xor_sync(0xffffffffu, low, o));
+    }
+    // the same total on every lane; s >= the exact sum's lower neighbour
+    const bool exact = low == (1 << 20) || s < ldexp(1.0, 53 + low) * 0.5;
+    if (lane == 0) {
+      if (!exact) {
+        s = 0.0;
+        for (int64_t j = 0; j < n; ++j)
+          if (labels[j] == c) s += j == i ? 0.0 : (double)row[j];
+      }
+      sum[i] = s;
+      // non-negative doubles order like their bit patterns
+      atomicMin(best_bits + c, (unsigned long long)__double_as_longlong(s));
+    }
+  }
 }
 
 __global__ void medoid_pick_kernel(int64_t n, const int* labels, const double* sum,
@@ -452,7 +481,8 @@ cudaError_t dbscan_summary(const float* D, int64_t n, const int* labels, int64_t
     return e;
   const unsigned lin = (unsigned)((n + 255) / 256);
   sizes_kernel<<<lin, 256, 0, s>>>(labels, n, sizes);
-  medoid_sum_kernel<<<lin, 256, 0, s>>>(D, n, labels, L.sum, best_bits);
+  const unsigned rows = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 7) / 8, 148 * 16));
+  medoid_sum_kernel<<<rows, 256, 0, s>>>(D, n, labels, L.sum, best_bits);
   medoid_pick_kernel<<<lin, 256, 0, s>>>(n, labels, L.sum, best_bits, centroids);
   return cudaGetLastError();
 }
