@@ -24,6 +24,7 @@
 #include <cstdint>
 
 #include "cluster.h"
+#include "device_util.cuh"
 
 namespace wmd {
 namespace {
@@ -279,27 +280,39 @@ __global__ void kmeans_features_kernel(const float* __restrict__ coords, int64_t
   }
 }
 
-// Assignment tiles: kAsRows samples x kAsCenters centers per block, features
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Assignment tiles: kAsRows samples x (8 or 16) centers per block, features
 // staged through shared memory kAsTile at a time (coalesced row loads).  A
-// warp owns kAsCPT centers for its 32 samples (lane = sample); every distance
-// is still the sequential sum over features in order with an unfused multiply
-// then add, as the reference's sq_dist.  Zero padding past nf adds exact
-// zeros.
+// warp owns CPT (1 for k <= 8, else 2) centers for its 32 samples (lane =
+// sample); every distance is the sequential sum over features in order with
+// an unfused multiply then add, as the reference's sq_dist.  Zero padding past
+// nf adds exact zeros.  The next tile is loaded into registers while the
+// current one is used (two shared buffers, one barrier per tile).
 constexpr int kAsRows = 32;
 constexpr int kAsWarps = 8;
-constexpr int kAsCPT = 2;
-constexpr int kAsCenters = kAsWarps * kAsCPT;
-constexpr int kAsTile = 64;
+constexpr int kAsTile = 48;
+constexpr int kAsPerThread = kAsRows * kAsTile / (kAsWarps * 32);  // x values per thread and tile
 
 // labels[i] = argmin_c |feat[i] - centers[c]|^2 (first minimum), or, when
 // own_labels is given, dist[i] = the distance to centers[own_labels[i]] and
 // the per-cluster minimum as ordered bits in best_bits.
+template <int CPT>
 __global__ void __launch_bounds__(kAsWarps * 32) kmeans_assign_kernel(
     const double* __restrict__ feat, int64_t n, int64_t nf, const double* __restrict__ centers, int k,
     int* __restrict__ labels, const int* __restrict__ own_labels, double* __restrict__ dist,
     unsigned long long* __restrict__ best_bits) {
-  __shared__ double xs[kAsRows][kAsTile + 1];
-  __shared__ double cs[kAsCenters][kAsTile];
+  constexpr int kAsCenters = kAsWarps * CPT;
+  constexpr int kAsCPerThread = kAsCenters * kAsTile / (kAsWarps * 32);  // center values per thread and tile
+  __shared__ double xs[2][kAsRows][kAsTile + 1];
+  __shared__ double cs[2][kAsCenters][kAsTile];
   __shared__ double dsm[kAsCenters][kAsRows];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t row0 = (int64_t)blockIdx.x * kAsRows;
@@ -308,36 +321,63 @@ __global__ void __launch_bounds__(kAsWarps * 32) kmeans_assign_kernel(
   double best_d = __longlong_as_double(0x7ff0000000000000ll);  // +inf
   double own_d = 0.0;
   int best = 0;
+  const int64_t n_tiles = (nf + kAsTile - 1) / kAsTile;
   for (int c0 = 0; c0 < k; c0 += kAsCenters) {
-    double d[kAsCPT];
+    double d[CPT];
 #pragma unroll
-    for (int p = 0; p < kAsCPT; ++p) d[p] = 0.0;
-    for (int64_t j0 = 0; j0 < nf; j0 += kAsTile) {
-      const int tw = (int)min((int64_t)kAsTile, nf - j0);
-      for (int e = tid; e < kAsRows * kAsTile; e += kAsWarps * 32) {
+    for (int p = 0; p < CPT; ++p) d[p] = 0.0;
+    double xr[kAsPerThread], cr[kAsCPerThread];
+    auto fetch = [&](int64_t j0) {  // tile j0 into registers (zero past nf / n / k)
+#pragma unroll
+      for (int m = 0; m < kAsPerThread; ++m) {
+        const int e = tid + m * kAsWarps * 32;
         const int r = e / kAsTile, q = e - r * kAsTile;
         const int64_t row = row0 + r;
-        xs[r][q] = (row < n && q < tw) ? __ldg(feat + (size_t)row * nf + j0 + q) : 0.0;
+        xr[m] = (row < n && j0 + q < nf) ? __ldg(feat + (size_t)row * nf + j0 + q) : 0.0;
       }
-      for (int e = tid; e < kAsCenters * kAsTile; e += kAsWarps * 32) {
+#pragma unroll
+      for (int m = 0; m < kAsCPerThread; ++m) {
+        const int e = tid + m * kAsWarps * 32;
         const int cc = e / kAsTile, q = e - cc * kAsTile;
         const int c = c0 + cc;
-        cs[cc][q] = (c < k && q < tw) ? __ldg(centers + (size_t)c * nf + j0 + q) : 0.0;
+        cr[m] = (c < k && j0 + q < nf) ? __ldg(centers + (size_t)c * nf + j0 + q) : 0.0;
       }
-      __syncthreads();
-#pragma unroll 16
-      for (int q = 0; q < kAsTile; ++q) {
-        const double x = xs[lane][q];
+    };
+    auto stash = [&](int buf) {
 #pragma unroll
-        for (int p = 0; p < kAsCPT; ++p) {
-          const double e = x - cs[warp * kAsCPT + p][q];
+      for (int m = 0; m < kAsPerThread; ++m) {
+        const int e = tid + m * kAsWarps * 32;
+        const int r = e / kAsTile, q = e - r * kAsTile;
+        xs[buf][r][q] = xr[m];
+      }
+#pragma unroll
+      for (int m = 0; m < kAsCPerThread; ++m) {
+        const int e = tid + m * kAsWarps * 32;
+        const int cc = e / kAsTile, q = e - cc * kAsTile;
+        cs[buf][cc][q] = cr[m];
+      }
+    };
+    fetch(0);
+    stash(0);
+    __syncthreads();
+    for (int64_t tt = 0; tt < n_tiles; ++tt) {
+      const int buf = (int)(tt & 1);
+      if (tt + 1 < n_tiles) fetch((tt + 1) * kAsTile);
+#pragma unroll 8
+      for (int q = 0; q < kAsTile; ++q) {
+        const double x = xs[buf][lane][q];
+#pragma unroll
+        for (int p = 0; p < CPT; ++p) {
+          const double e = x - cs[buf][warp * CPT + p][q];
           d[p] = __dadd_rn(d[p], __dmul_rn(e, e));
         }
       }
+      // the other buffer was last read before the previous barrier
+      if (tt + 1 < n_tiles) stash(buf ^ 1);
       __syncthreads();
     }
 #pragma unroll
-    for (int p = 0; p < kAsCPT; ++p) dsm[warp * kAsCPT + p][lane] = d[p];
+    for (int p = 0; p < CPT; ++p) dsm[warp * CPT + p][lane] = d[p];
     __syncthreads();
     if (warp == 0) {
       for (int cc = 0; cc < kAsCenters && c0 + cc < k; ++cc) {
@@ -360,19 +400,22 @@ __global__ void __launch_bounds__(kAsWarps * 32) kmeans_assign_kernel(
   }
 }
 
-// Per-cluster sums in sample order.  Block = (256 feature columns, one
-// cluster); each warp scans the labels 32 at a time, queues the members'
-// indices in shared memory in index order (ballot + prefix count) and adds
-// their rows kSumBatch at a time, so kSumBatch coalesced row loads per lane
-// are in flight while the sum itself stays sequential.
-constexpr int kSumWarps = 8;
-constexpr int kSumBatch = 16;
+// Per-cluster sums in sample order.  Block = (128 feature columns, one
+// cluster); each warp scans the labels 32 at a time and queues its members'
+// indices in index order (ballot + prefix count).  Every 32 queued rows each
+// lane prefetches its column of them into shared memory with cp.async (8
+// bytes per row, no registers held), and adds the previous batch from the
+// other buffer meanwhile; each column's sum stays sequential in index order.
+constexpr int kSumWarps = 4;
+constexpr int kSumBatch = 32;
+constexpr size_t kSumSmem = (size_t)kSumWarps * 2 * kSumBatch * 32 * sizeof(double);
 
 __global__ void __launch_bounds__(kSumWarps * 32) kmeans_sums_kernel(const double* __restrict__ feat, int64_t n,
                                                                      int64_t nf, const int* __restrict__ labels,
                                                                      int k, double* __restrict__ sums,
                                                                      int* __restrict__ counts) {
-  __shared__ int queue[kSumWarps][kSumBatch + 32];
+  extern __shared__ double sum_smem[];
+  __shared__ int queue[kSumWarps][2 * kSumBatch];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int c = blockIdx.y;
   const int64_t col0 = ((int64_t)blockIdx.x * kSumWarps + warp) * 32;
@@ -380,35 +423,70 @@ __global__ void __launch_bounds__(kSumWarps * 32) kmeans_sums_kernel(const doubl
   const int64_t col = col0 + lane;
   const bool live = col < nf;
   int* q = queue[warp];
+  double* buf = sum_smem + (size_t)warp * 2 * kSumBatch * 32;  // [2][kSumBatch][32]
   double acc = 0.0;
-  int m = 0, cnt = 0;
-  auto flush = [&](int take) {
-    double v[kSumBatch];
-#pragma unroll
-    for (int p = 0; p < kSumBatch; ++p) v[p] = (p < take && live) ? __ldg(feat + (size_t)q[p] * nf + col) : 0.0;
-#pragma unroll
-    for (int p = 0; p < kSumBatch; ++p)
-      if (p < take) acc += v[p];
+  int m = 0, cnt = 0, pending = -1, pending_take = 0, nb = 0;
+  // rows q[0..take) into buffer b (this lane's column)
+  auto issue = [&](int b, int take) {
+    double* dst = buf + (size_t)b * kSumBatch * 32 + lane;
+    if (live)
+      for (int p = 0; p < take; ++p) cp_async8(dst + p * 32, feat + (size_t)q[p] * nf + col);
+    cp_async_commit();
   };
-  for (int64_t i0 = 0; i0 < n; i0 += 32) {
-    const int64_t i = i0 + lane;
-    const bool mine = i < n && __ldg(labels + i) == c;
-    const unsigned mask = __ballot_sync(0xffffffffu, mine);
-    if (mine) q[m + __popc(mask & ((1u << lane) - 1u))] = (int)i;
-    m += __popc(mask);
-    cnt += __popc(mask);
-    __syncwarp();
-    while (m >= kSumBatch) {
-      flush(kSumBatch);
-      const int rest = m - kSumBatch;  // < 32
-      const int t = lane < rest ? q[kSumBatch + lane] : 0;
+  auto consume = [&](int b, int take) {
+    const double* src = buf + (size_t)b * kSumBatch * 32 + lane;
+    for (int p = 0; p < take; ++p) acc += src[p * 32];
+  };
+  // labels are read kSumAhead chunks at a time, so that the scan does not
+  // wait for one load per 32 samples
+  constexpr int kSumAhead = 8;
+  for (int64_t i0 = 0; i0 < n; i0 += 32 * kSumAhead) {
+    int lab[kSumAhead];
+#pragma unroll
+    for (int u = 0; u < kSumAhead; ++u) {
+      const int64_t i = i0 + u * 32 + lane;
+      lab[u] = i < n ? __ldg(labels + i) : -1;
+    }
+#pragma unroll
+    for (int u = 0; u < kSumAhead; ++u) {
+      const int64_t i = i0 + u * 32 + lane;
+      const bool mine = lab[u] == c;
+      const unsigned mask = __ballot_sync(0xffffffffu, mine);
+      if (mine) q[m + __popc(mask & ((1u << lane) - 1u))] = (int)i;
+      m += __popc(mask);
+      cnt += __popc(mask);
       __syncwarp();
-      if (lane < rest) q[lane] = t;
-      m = rest;
-      __syncwarp();
+      if (m >= kSumBatch) {
+        const int b = nb & 1;
+        issue(b, kSumBatch);
+        ++nb;
+        if (pending >= 0) {
+          cp_async_wait<1>();  // the previous batch has landed
+          consume(pending, pending_take);
+        }
+        pending = b;
+        pending_take = kSumBatch;
+        const int rest = m - kSumBatch;  // < 32
+        const int t = lane < rest ? q[kSumBatch + lane] : 0;
+        __syncwarp();
+        if (lane < rest) q[lane] = t;
+        m = rest;
+        __syncwarp();
+      }
     }
   }
-  if (m > 0) flush(m);
+  if (m > 0) {
+    const int b = nb & 1;
+    issue(b, m);
+    if (pending >= 0) {
+      cp_async_wait<1>();
+      consume(pending, pending_take);
+    }
+    pending = b;
+    pending_take = m;
+  }
+  cp_async_wait<0>();
+  if (pending >= 0) consume(pending, pending_take);
   if (live) sums[(size_t)c * nf + col] = acc;
   if (col == 0) counts[c] = cnt;
 }
@@ -508,16 +586,24 @@ cudaError_t kmeans_gather(const double* feat, int64_t nf, const int64_t* idx, in
 cudaError_t kmeans_assign(const double* feat, int64_t n, int64_t nf, const double* centers, int k, int* labels,
                           double* dist_own, cudaStream_t s) {
   (void)dist_own;
-  kmeans_assign_kernel<<<(unsigned)((n + kAsRows - 1) / kAsRows), kAsWarps * 32, 0, s>>>(feat, n, nf, centers, k,
-                                                                                       labels, nullptr, nullptr,
-                                                                                       nullptr);
+  const unsigned g = (unsigned)((n + kAsRows - 1) / kAsRows);
+  if (k <= kAsWarps)
+    kmeans_assign_kernel<1><<<g, kAsWarps * 32, 0, s>>>(feat, n, nf, centers, k, labels, nullptr, nullptr, nullptr);
+  else
+    kmeans_assign_kernel<2><<<g, kAsWarps * 32, 0, s>>>(feat, n, nf, centers, k, labels, nullptr, nullptr, nullptr);
   return cudaGetLastError();
 }
 
 cudaError_t kmeans_sums(const double* feat, int64_t n, int64_t nf, const int* labels, int k, double* sums, int* counts,
                         cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(kmeans_sums_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSumSmem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
   const dim3 grid((unsigned)((nf + kSumWarps * 32 - 1) / (kSumWarps * 32)), (unsigned)k);
-  kmeans_sums_kernel<<<grid, kSumWarps * 32, 0, s>>>(feat, n, nf, labels, k, sums, counts);
+  kmeans_sums_kernel<<<grid, kSumWarps * 32, kSumSmem, s>>>(feat, n, nf, labels, k, sums, counts);
   return cudaGetLastError();
 }
 
@@ -536,9 +622,11 @@ cudaError_t kmeans_finish(const double* feat, int64_t n, int64_t nf, const doubl
   if ((e = cudaMemsetAsync(best_bits, 0xff, (size_t)k * sizeof(unsigned long long), s)) != cudaSuccess) return e;
   const unsigned lin = (unsigned)((n + 127) / 128);
   sizes_kernel<<<lin, 128, 0, s>>>(labels, n, sizes);
-  kmeans_assign_kernel<<<(unsigned)((n + kAsRows - 1) / kAsRows), kAsWarps * 32, 0, s>>>(feat, n, nf, centers, k,
-                                                                                       nullptr, labels, dist,
-                                                                                       best_bits);
+  const unsigned g = (unsigned)((n + kAsRows - 1) / kAsRows);
+  if (k <= kAsWarps)
+    kmeans_assign_kernel<1><<<g, kAsWarps * 32, 0, s>>>(feat, n, nf, centers, k, nullptr, labels, dist, best_bits);
+  else
+    kmeans_assign_kernel<2><<<g, kAsWarps * 32, 0, s>>>(feat, n, nf, centers, k, nullptr, labels, dist, best_bits);
   medoid_pick_kernel<<<lin, 128, 0, s>>>(n, labels, dist, best_bits, centroids);
   return cudaGetLastError();
 }
