@@ -222,12 +222,33 @@ __global__ void __launch_bounds__(256, 4) group_rmsd_kernel(const float* __restr
 
 }  // namespace
 
+// Frame groups: the count whose blocks fill whole waves of resident CTAs best
+// (a partial last wave leaves SMs idle while the HBM stream is the bound),
+// at least 16 frames per group.
 int fluct_groups(int64_t n_sel, int64_t n_frames, int sm_count) {
-  const int64_t blocks = (n_sel + kFluctThreads - 1) / kFluctThreads;
-  const int64_t want = (int64_t)sm_count * 8;
-  int64_t G = blocks > 0 ? (want + blocks - 1) / blocks : 1;
-  G = std::min<int64_t>(G, std::max<int64_t>(1, n_frames / 16));
-  return (int)std::max<int64_t>(1, std::min<int64_t>(G, 1024));
+  static int occ = 0;
+  if (occ == 0) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fluct_partial_kernel<3>, kFluctThreads, 0) != cudaSuccess)
+      b = 8;
+    occ = std::max(b, 1);
+  }
+  const int64_t blocks = std::max<int64_t>(1, (n_sel + kFluctThreads - 1) / kFluctThreads);
+  const int64_t cap = (int64_t)sm_count * occ;
+  const int64_t g_max = std::max<int64_t>(1, std::min<int64_t>(1024, n_frames / 16));
+  int64_t best = 1;
+  double best_eff = -1.0;
+  for (int64_t G = 1; G <= g_max && G <= 64; ++G) {
+    const int64_t total = blocks * G;
+    const int64_t waves = (total + cap - 1) / cap;
+    const double eff = (double)total / (double)(waves * cap);
+    if (eff > best_eff + 1e-9) {
+      best = G;
+      best_eff = eff;
+    }
+    if (eff > 0.95 && total >= cap) break;  // first full wave at 95 %
+  }
+  return (int)best;
 }
 
 cudaError_t launch_fluct_shift(const float* coords, int64_t n_atoms, int stride, const uint32_t* sel, int64_t n_sel,
