@@ -523,7 +523,7 @@ size_t frame_smem_bytes(int stride, int tile_atoms) {
 }
 
 void frame_plan(FrameLaunch& L, int sm_count) {
-  L.lanes = lanes_eligible(L);
+  L.lanes = lanes_eligible(L) && lanes_worthwhile(L, sm_count);
   L.tile_atoms = L.lanes ? lanes_tile(L, sm_count) : kConsumerThreads * kApt;
 }
 

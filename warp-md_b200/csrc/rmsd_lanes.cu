@@ -314,6 +314,12 @@ static int64_t lane_warps(const FrameLaunch& L, int64_t slots) {
   return std::max<int64_t>(1, (units + per - 1) / per);
 }
 
+bool lanes_worthwhile(const FrameLaunch& L, int sm_count) {
+  // fewer (256-atom tile, 32-frame group) units than two per SM: the
+  // atom-major kernel's (tile, frame) items spread better
+  return lane_units(L, 256) >= 2 * (int64_t)sm_count;
+}
+
 int lanes_tile(const FrameLaunch& L, int sm_count) {
   // Tile size from 2,048 down to 256 atoms minimising the busiest warp's
   // bytes: (units per warp) x (tile bytes + its 128-byte partial, written

@@ -75,6 +75,7 @@ void frame_plan(FrameLaunch& L, int sm_count);
 // partial record
 constexpr int kLaneTile = 2048;
 bool lanes_eligible(const FrameLaunch& L);
+bool lanes_worthwhile(const FrameLaunch& L, int sm_count);
 int lanes_tile(const FrameLaunch& L, int sm_count);
 int lanes_grid(const FrameLaunch& L, int sm_count);
 cudaError_t launch_lanes_forward(const FrameLaunch& L, bool raw, cudaStream_t s);
