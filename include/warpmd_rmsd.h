@@ -158,11 +158,13 @@ typedef struct wmd_batch_desc {
  * graph.  with_grad on wmd_batched_rmsd needs with_grad on the prepare. */
 int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, int n_traj, int with_grad);
 int wmd_batched_rmsd(wmd_ctx* ctx, const wmd_batch_desc* descs, int n_traj, int with_grad, void* stream);
-/* Layout the prepare step chose: atoms per tile (512 or 1024) and whether the
- * launch is frame-major (1: each CTA owns whole frames, QCP in-kernel, the
- * gradient pass re-reads the frame from L2) or tile-major (0: tiles of all
- * frames spread over CTAs, separate finishing kernels).  Either pointer may be
- * NULL.  WMD_ERR_INVALID_ARG when no batch is prepared. */
+/* Layout the prepare step chose: atoms per tile (512 or 1024) and the layout
+ * in *frame_major: 1 frame-major (each CTA owns whole frames, QCP in-kernel,
+ * the gradient pass re-reads the frame from L2), 0 tile-major (tiles of all
+ * frames spread over CTAs, separate finishing kernels), 2 tile-major with
+ * the forward statistics computed frames across lanes (a lane per frame of
+ * a 32-frame group).  Either pointer may be NULL.  WMD_ERR_INVALID_ARG when
+ * no batch is prepared. */
 int wmd_batched_layout(const wmd_ctx* ctx, int* tile_atoms, int* frame_major);
 
 /* ---- Optimal superposition (AlignPlan, RotationMatrixPlan, SuperposePlan,

@@ -5,9 +5,10 @@ single-trajectory entry points.
 The reference has no batched form; each trajectory's values must be what its
 own RmsdPlan gives (plan.rs:164-418), so the pins are the oracle's FP64 RMSD
 (|d| <= 1e-5 A, the per-frame bar) and its analytic gradient
-(|g - g64| <= 1e-5 max|g| + 1e-7).  Both layouts (tile-major, frame-major)
-and both tile shapes (512 and 1024 atoms) are forced once each, and the
-autotuner's own choice is run too.
+(|g - g64| <= 1e-5 max|g| + 1e-7).  Every layout (tile-major, frame-major,
+tile-major with the frames-across-lanes forward) and both tile shapes (512
+and 1024 atoms) are forced once each, and the autotuner's own choice is run
+too.
 """
 import os
 
@@ -62,6 +63,7 @@ def _run(xs, ys, with_grad, tile=None, layout=None):
     if tile is not None:
         assert b.layout()["tile_atoms"] == tile
     if layout is not None:
+        assert b.layout()["layout"] == layout
         assert b.layout()["frame_major"] == (layout == "frames")
     for r in b.rmsd:
         r.fill_(-1.0)
@@ -95,7 +97,8 @@ def _check_grad(b, xs, ys):
         assert err <= tol, (k, x.shape, err, tol)
 
 
-LAYOUTS = [(512, "tiles"), (1024, "tiles"), (512, "frames"), (1024, "frames"), (None, None)]
+LAYOUTS = [(512, "tiles"), (1024, "tiles"), (512, "frames"), (1024, "frames"), (512, "lanes"), (1024, "lanes"),
+           (None, None)]
 
 
 @pytest.mark.parametrize("tile,layout", LAYOUTS)
@@ -120,7 +123,7 @@ def test_batched_equals_single_trajectory_path():
     wmd_rmsd_backward) on it alone: the same FP64 statistics and QCP, so the
     two differ only by summation order (<= 1e-9 A here)."""
     xs, ys = _batch([(300, 8), (4100, 5), (1024, 9), (77, 30)], 31)
-    for layout in ("tiles", "frames"):
+    for layout in ("tiles", "frames", "lanes"):
         _compare_single(_run(xs, ys, with_grad=True, layout=layout), xs, ys)
 
 
@@ -152,7 +155,7 @@ def test_batched_near_zero_rmsd_takes_residual_pass():
                           [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
                           [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
             xs[k][f] = (ys[k].astype(np.float64) @ R.T + rng.normal(0, 5, 3)).astype(np.float32)
-    for layout in ("tiles", "frames"):
+    for layout in ("tiles", "frames", "lanes"):
         b = _run(xs, ys, with_grad=True, layout=layout)
         _check_rmsd(b, xs, ys)
         for r in b.rmsd:
@@ -229,7 +232,7 @@ def test_batched_many_uneven_trajectories():
     rng = np.random.default_rng(3)
     shapes = [(int(np.exp(rng.uniform(np.log(50), np.log(6000)))), int(rng.integers(5, 60))) for _ in range(96)]
     xs, ys = _batch(shapes, 1000)
-    for layout in ("tiles", "frames"):
+    for layout in ("tiles", "frames", "lanes"):
         b = _run(xs, ys, with_grad=True, layout=layout)
         _check_rmsd(b, xs, ys)
         _check_grad(b, xs, ys)

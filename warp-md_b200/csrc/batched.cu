@@ -822,6 +822,218 @@ __global__ void __launch_bounds__(kThreads, 4) batched_frame_kernel(const BatchL
   }
 }
 
+// ---------------------------------------------------------------------------
+// Lanes layout forward: units (trajectory, atom tile, 32-frame group); lane l
+// of a warp accumulates frame 32g + l over the tile, in FP64 and in atom
+// order, and stores the item partial (tile, frame) the finisher reads.  Per
+// stage (32 atoms) every lane bulk-copies its own frame's row (the 16-byte
+// hull of 32 atoms, at most 400 bytes, any atom count) and lane 0 the 32
+// reference atoms; the barrier of a stage counts 32 arrivals.  Warps take
+// contiguous runs of units of equal estimated cost.
+// ---------------------------------------------------------------------------
+constexpr int kBLWarps = 4;
+constexpr int kBLStages = 2;
+constexpr int kBLRow = 400;  // bytes per frame row of a stage
+constexpr int kBLXBytes = 32 * kBLRow;
+constexpr int kBLYBytes = 32 * 3 * 8;
+constexpr int kBLStageBytes = kBLXBytes + kBLYBytes;
+constexpr int kBLBarOffset = kBLWarps * kBLStages * kBLStageBytes;
+constexpr int kBLAbortOffset = kBLBarOffset + kBLWarps * kBLStages * 8;
+constexpr int kBLSmemBytes = kBLAbortOffset + 16;
+
+// last segment whose units start at or before cost c
+__device__ __forceinline__ int lane_seg_of(const BatchSeg* segs, int n, int64_t c) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (segs[mid].lane_cost0 <= c) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+struct LaneCur {
+  int seg;
+  int64_t k;  // unit within the segment
+};
+
+__device__ __forceinline__ void lane_skip_empty(const BatchLaunch& B, LaneCur& c) {
+  while (c.seg < B.n_segs && c.k >= B.segs[c.seg].lane_units) {
+    ++c.seg;
+    c.k = 0;
+  }
+}
+
+template <int APT>
+__global__ void __launch_bounds__(kBLWarps * 32) batched_lanes_kernel(const BatchLaunch B) {
+  constexpr int T = kConsumerThreads * APT;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kBLBarOffset);
+  uint64_t* full = bars + warp * kBLStages;
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + kBLAbortOffset);
+  unsigned char* ring = smem + warp * kBLStages * kBLStageBytes;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kBLWarps * kBLStages; ++i) mbar_init(&bars[i], 32);
+    *abort_flag = 0;
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const int64_t nw = (int64_t)gridDim.x * kBLWarps, gw = (int64_t)blockIdx.x * kBLWarps + warp;
+  const int64_t C0 = B.total_lane_cost * gw / nw, C1 = B.total_lane_cost * (gw + 1) / nw;
+  if (C0 >= C1 || B.n_segs == 0) return;
+  // first unit starting at or after C0
+  LaneCur first;
+  first.seg = lane_seg_of(B.segs, B.n_segs, C0);
+  {
+    const BatchSeg& S = B.segs[first.seg];
+    const int64_t off = C0 - S.lane_cost0;
+    first.k = S.lane_units > 0 ? (off + S.lane_unit_cost - 1) / S.lane_unit_cost : 0;
+  }
+  lane_skip_empty(B, first);
+  auto starts_before_end = [&](const LaneCur& c) {
+    return c.seg < B.n_segs && B.segs[c.seg].lane_cost0 + c.k * B.segs[c.seg].lane_unit_cost < C1;
+  };
+  auto unit_stages = [&](const LaneCur& c) {
+    const BatchSeg& S = B.segs[c.seg];
+    const int64_t groups = (S.n_frames + 31) / 32;
+    const int64_t t = c.k / groups;
+    return (int)((min((int64_t)T, S.n_atoms - t * T) + 31) / 32);
+  };
+  // producer cursor: unit pc, stage pj; every lane runs it (warp-uniform)
+  LaneCur pc = first;
+  int pj = 0;
+  bool p_live = starts_before_end(pc);
+  int p_st = p_live ? unit_stages(pc) : 0;
+  int64_t n_issued = 0;
+  auto issue_next = [&]() {
+    const BatchSeg& S = B.segs[pc.seg];
+    const int64_t groups = (S.n_frames + 31) / 32;
+    const int64_t t = pc.k / groups, g = pc.k - t * groups;
+    const int64_t a0 = t * T + (int64_t)pj * 32;
+    const int nv = (int)min((int64_t)32, S.n_atoms - a0);
+    const int slot = (int)(n_issued % kBLStages);
+    unsigned char* st = ring + slot * kBLStageBytes;
+    unsigned char* dst = st + lane * kBLRow;
+    const int64_t f = g * 32 + lane;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    uint32_t bytes = 0;
+    uint64_t c0 = 0;
+    const unsigned char* base = reinterpret_cast<const unsigned char*>(S.coords);
+    if (f < S.n_frames) {
+      const uint64_t total_al = ((uint64_t)S.n_frames * (uint64_t)S.n_atoms * 12ull) & ~15ull;
+      const uint64_t b0 = (uint64_t)(f * S.n_atoms + a0) * 12ull;
+      const uint64_t b1 = b0 + (uint64_t)nv * 12ull;
+      c0 = b0 & ~15ull;
+      uint64_t c1 = (b1 + 15ull) & ~15ull;
+      if (c1 > total_al) {  // the array's unaligned tail: plain loads
+        const uint64_t tail0 = total_al > c0 ? total_al : c0;
+        for (uint64_t bb = tail0; bb < b1; bb += 4)
+          *reinterpret_cast<float*>(dst + (bb - c0)) = __ldg(reinterpret_cast<const float*>(base + bb));
+        c1 = tail0;
+      }
+      bytes = (uint32_t)(c1 - c0);
+    }
+    const uint32_t tx = bytes + (lane == 0 ? (uint32_t)kBLYBytes : 0u);
+    if (tx) mbar_arrive_expect_tx(&full[slot], tx);
+    else mbar_arrive(&full[slot]);
+    if (bytes) bulk_copy_g2s(dst, base + c0, bytes, &full[slot]);
+    if (lane == 0) bulk_copy_g2s(st + kBLXBytes, S.yc + a0 * 3, kBLYBytes, &full[slot]);
+    ++n_issued;
+    if (++pj == p_st) {
+      pj = 0;
+      ++pc.k;
+      lane_skip_empty(B, pc);
+      p_live = starts_before_end(pc);
+      p_st = p_live ? unit_stages(pc) : 0;
+    }
+  };
+  while (p_live && n_issued < kBLStages) issue_next();
+
+  int64_t n_done = 0;
+  bool aborted = false;
+  LaneCur cu = first;
+  while (starts_before_end(cu) && !aborted) {
+    const BatchSeg& S = B.segs[cu.seg];
+    const int64_t groups = (S.n_frames + 31) / 32;
+    const int64_t t = cu.k / groups, g = cu.k - t * groups;
+    const int st_n = unit_stages(cu);
+    const int64_t f = g * 32 + lane;
+    const bool live = f < S.n_frames;
+    double acc[15];
+#pragma unroll
+    for (int e = 0; e < 15; ++e) acc[e] = 0.0;
+    for (int j = 0; j < st_n; ++j) {
+      const int slot = (int)(n_done % kBLStages);
+      const uint32_t parity = (uint32_t)((n_done / kBLStages) & 1);
+      if (!mbar_wait(&full[slot], parity, B.status, kStatusTimeoutFull, abort_flag)) {
+        aborted = true;
+        break;
+      }
+      const int64_t a0 = t * T + (int64_t)j * 32;
+      const int nv = (int)min((int64_t)32, S.n_atoms - a0);
+      const unsigned char* st = ring + slot * kBLStageBytes;
+      const double* ys = reinterpret_cast<const double*>(st + kBLXBytes);
+      if (live) {
+        const int head = (int)(((uint64_t)(f * S.n_atoms + a0) * 12ull) & 15ull);
+        const float* xr = reinterpret_cast<const float*>(st + lane * kBLRow + head);
+#pragma unroll 4
+        for (int a = 0; a < nv; ++a) {
+          const double x0 = xr[3 * a], x1 = xr[3 * a + 1], x2 = xr[3 * a + 2];
+          const double y0 = ys[3 * a], y1 = ys[3 * a + 1], y2 = ys[3 * a + 2];
+          acc[0] += x0; acc[1] += x1; acc[2] += x2;
+          acc[3] = fma(x0, x0, acc[3]); acc[4] = fma(x1, x1, acc[4]); acc[5] = fma(x2, x2, acc[5]);
+          acc[6] = fma(x0, y0, acc[6]);  acc[7] = fma(x0, y1, acc[7]);  acc[8] = fma(x0, y2, acc[8]);
+          acc[9] = fma(x1, y0, acc[9]);  acc[10] = fma(x1, y1, acc[10]); acc[11] = fma(x1, y2, acc[11]);
+          acc[12] = fma(x2, y0, acc[12]); acc[13] = fma(x2, y1, acc[13]); acc[14] = fma(x2, y2, acc[14]);
+        }
+      }
+      ++n_done;
+      __syncwarp();
+      if (p_live) issue_next();
+    }
+    if (aborted) break;
+    if (live) {
+      double2* rec = reinterpret_cast<double2*>(B.partial + (size_t)(S.item0 + t * S.n_frames + f) * kStatDoubles);
+#pragma unroll
+      for (int e = 0; e < 7; ++e) rec[e] = make_double2(acc[2 * e], acc[2 * e + 1]);
+      rec[7] = make_double2(acc[14], 0.0);
+    }
+    ++cu.k;
+    lane_skip_empty(B, cu);
+  }
+  // after an abort, copies this warp issued may still be landing
+  if (aborted) {
+    for (int64_t j = n_done; j < n_issued; ++j) {
+      const int slot = (int)(j % kBLStages);
+      const uint32_t ph = (uint32_t)((j / kBLStages) & 1);
+      const uint64_t t0 = global_timer_ns();
+      while (!mbar_try_wait(&full[slot], ph)) {
+        if (global_timer_ns() - t0 > kWaitLimitNs) {
+          atomicOr(B.status, kStatusTimeoutDrain);
+          break;
+        }
+      }
+    }
+  }
+}
+
+template <int APT>
+cudaError_t launch_lanes(const BatchLaunch& B, int grid, cudaStream_t s) {
+  auto kern = batched_lanes_kernel<APT>;
+  static bool attr_done[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!attr_done[dev]) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kBLSmemBytes);
+    if (e != cudaSuccess) return e;
+    attr_done[dev] = true;
+  }
+  kern<<<grid, kBLWarps * 32, kBLSmemBytes, s>>>(B);
+  return cudaGetLastError();
+}
+
 template <int APT, bool GRAD>
 cudaError_t launch_frames(const BatchLaunch& B, int grid, cudaStream_t s) {
   auto kern = batched_frame_kernel<APT, GRAD>;
@@ -891,7 +1103,10 @@ cudaError_t batched_enqueue(const BatchPlan& P, bool with_grad, cudaStream_t s) 
   }
   if ((e = cudaMemsetAsync(B.refine_count, 0, sizeof(unsigned), s)) != cudaSuccess) return e;
   if (B.total_items > 0) {
-    e = P.apt == 4 ? launch_stream<4, kBFwd>(B, P.grid_fwd, s) : launch_stream<8, kBFwd>(B, P.grid_fwd, s);
+    if (P.variant == kBatchLanes)
+      e = P.apt == 4 ? launch_lanes<4>(B, P.grid_fwd, s) : launch_lanes<8>(B, P.grid_fwd, s);
+    else
+      e = P.apt == 4 ? launch_stream<4, kBFwd>(B, P.grid_fwd, s) : launch_stream<8, kBFwd>(B, P.grid_fwd, s);
     if (e != cudaSuccess) return e;
   }
   if (B.total_frames > 0) {
@@ -910,6 +1125,20 @@ int batched_grid(int apt, bool backward, int sm_count, int64_t items) {
   const int occ = apt == 4 ? (backward ? occupancy_of<4, kBBwd>() : occupancy_of<4, kBFwd>())
                            : (backward ? occupancy_of<8, kBBwd>() : occupancy_of<8, kBFwd>());
   return (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)sm_count * occ));
+}
+
+int batched_lanes_grid(int sm_count, int64_t units) {
+  static int occ = 0;
+  if (occ == 0) {
+    cudaFuncSetAttribute(batched_lanes_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBLSmemBytes);
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, batched_lanes_kernel<8>, kBLWarps * 32, kBLSmemBytes) !=
+        cudaSuccess)
+      b = 1;
+    occ = std::max(b, 1);
+  }
+  const int64_t by_units = (units + kBLWarps - 1) / kBLWarps;
+  return (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sm_count * occ, by_units));
 }
 
 int batched_frame_grid(int apt, bool with_grad, int sm_count, int64_t groups) {

@@ -22,6 +22,9 @@ struct BatchSeg {
   int64_t n_groups;     //   groups of this trajectory (m_group frames each, the last may be short)
   int64_t cost0;        //   estimated cost of all groups before this trajectory's
   int64_t group_cost;   //   estimated cost of one full group
+  int64_t lane_unit_cost;  // lanes layout: estimated cost of one (tile, 32-frame group) unit
+  int64_t lane_units;      //   units of this trajectory (n_tiles x ceil(n_frames / 32))
+  int64_t lane_cost0;      //   estimated cost of all units before this trajectory's
   int n_tiles;
   int m_group;          //   frames per group
   double sum_c[3];      // sum of y_c, written on the device each call
@@ -36,6 +39,7 @@ struct BatchLaunch {
   int64_t total_frames = 0;
   int64_t total_groups = 0;          // frame-major layout
   int64_t total_cost = 0;
+  int64_t total_lane_cost = 0;       // lanes layout
   double* partial = nullptr;         // [total_items][16]
   double* rot = nullptr;             // [total_frames][16] (with gradients): R, xbar, 1/(n rmsd)
   double* refine = nullptr;          // [total_frames][16]
@@ -48,7 +52,7 @@ struct BatchPlan {
   BatchSeg* segs_dev = nullptr;
   int n_segs = 0;
   int apt = 8;       // atoms per thread: 4 (512-atom tiles) or 8 (1024-atom tiles)
-  int variant = 0;   // kBatchTiles or kBatchFrames
+  int variant = 0;   // kBatchTiles, kBatchFrames or kBatchLanes
   int grid_fwd = 0;
   int grid_bwd = 0;
 };
@@ -58,7 +62,10 @@ struct BatchPlan {
 // (36 B per atom-frame with gradients).  Frame-major: each CTA owns whole
 // frames, finishes QCP in-kernel and re-reads the frame from L2 for the
 // gradient (24 B per atom-frame from HBM).
-enum BatchVariant : int { kBatchTiles = 0, kBatchFrames = 1 };
+// Lanes: the tile-major pipeline with its forward statistics computed frames
+// across lanes (a lane per frame of a 32-frame group, no cross-lane
+// reduction), the same per-item partials, finisher and gradient pass.
+enum BatchVariant : int { kBatchTiles = 0, kBatchFrames = 1, kBatchLanes = 2 };
 
 // Frame-major grouping: up to kGroupFrames consecutive frames of one
 // trajectory with at most kGroupBytes of coordinates form a group, whose QCP
@@ -73,6 +80,7 @@ constexpr int64_t kCostFinish = 24;
 int batched_tile_atoms(int apt);
 int batched_grid(int apt, bool backward, int sm_count, int64_t items);
 int batched_frame_grid(int apt, bool with_grad, int sm_count, int64_t groups);
+int batched_lanes_grid(int sm_count, int64_t units);
 // Enqueues the whole batched pipeline on s (no allocation, no host sync).
 cudaError_t batched_enqueue(const BatchPlan& P, bool with_grad, cudaStream_t s);
 

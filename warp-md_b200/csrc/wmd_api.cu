@@ -1401,12 +1401,16 @@ WMD_EXPORT int wmd_cluster_kmeans(wmd_ctx* ctx, const float* coords, int64_t n_f
 
 // Builds the device trajectory table for a tile shape; returns total items
 // (tile-major layout) and fills the frame-group partition (frame-major).
+// Each trajectory's centred reference is followed by 32 zero atoms (the lanes
+// forward copies whole 32-atom blocks of it), every block 16-byte aligned.
+static int64_t batch_yc_doubles(int64_t n_atoms) { return (n_atoms * 3 + 1) / 2 * 2 + 32 * 3; }
+
 static int64_t build_segs(const std::vector<wmd_batch_desc>& d, int apt, double* yc_base, bool with_grad,
                           std::vector<wmd::BatchSeg>& segs, int64_t* total_frames, int64_t* total_groups,
-                          int64_t* total_cost) {
+                          int64_t* total_cost, int64_t* total_lane_cost) {
   const int tile = wmd::batched_tile_atoms(apt);
   segs.assign(d.size(), wmd::BatchSeg{});
-  int64_t items = 0, frames = 0, yoff = 0, groups = 0, cost = 0;
+  int64_t items = 0, frames = 0, yoff = 0, groups = 0, cost = 0, lane_cost = 0;
   for (size_t i = 0; i < d.size(); ++i) {
     wmd::BatchSeg& g = segs[i];
     g.coords = d[i].coords;
@@ -1417,7 +1421,19 @@ static int64_t build_segs(const std::vector<wmd_batch_desc>& d, int apt, double*
     g.n_frames = d[i].n_frames;
     g.n_tiles = (int)((d[i].n_atoms + tile - 1) / tile);
     g.yc = yc_base + yoff;
-    yoff += (d[i].n_atoms * 3 + 1) / 2 * 2;  // keep each block 16-byte aligned
+    yoff += batch_yc_doubles(d[i].n_atoms);
+    // lanes layout: (tile, 32-frame group) units; cost ~ atom-frames plus a
+    // per-stage overhead of about 8 atoms' work
+    g.lane_cost0 = lane_cost;
+    if (g.n_atoms > 0 && g.n_frames > 0) {
+      g.lane_units = (int64_t)g.n_tiles * ((g.n_frames + 31) / 32);
+      const int64_t at = std::min<int64_t>(tile, g.n_atoms);
+      g.lane_unit_cost = 32 * (at + 8 * ((at + 31) / 32));
+    } else {
+      g.lane_units = 0;
+      g.lane_unit_cost = 1;
+    }
+    lane_cost += g.lane_units * g.lane_unit_cost;
     g.item0 = items;
     g.frame0 = frames;
     items += (int64_t)g.n_tiles * g.n_frames;
@@ -1444,6 +1460,7 @@ static int64_t build_segs(const std::vector<wmd_batch_desc>& d, int apt, double*
   *total_frames = frames;
   *total_groups = groups;
   *total_cost = cost;
+  *total_lane_cost = lane_cost;
   return items;
 }
 
@@ -1475,15 +1492,17 @@ WMD_EXPORT int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, in
     if (with_grad && (reinterpret_cast<uintptr_t>(x.grad) & 15u))
       return set_err(ctx, WMD_ERR_INVALID_ARG, "trajectory %d: grad must be 16-byte aligned", i);
     if (!with_grad) x.grad = nullptr;
-    sum_atoms += (x.n_atoms * 3 + 1) / 2 * 2;
   }
+  for (int i = 0; i < n_traj; ++i) sum_atoms += batch_yc_doubles(d[i].n_atoms);
   int64_t frames4 = 0, frames8 = 0;
   std::vector<wmd::BatchSeg> s4, s8;
   if ((rc = ensure(ctx, ctx->b_yc, (size_t)std::max<int64_t>(sum_atoms, 2) * sizeof(double)))) return rc;
   double* yc = static_cast<double*>(ctx->b_yc.ptr);
-  int64_t groups4 = 0, groups8 = 0, cost4 = 0, cost8 = 0;
-  const int64_t items4 = build_segs(d, 4, yc, with_grad != 0, s4, &frames4, &groups4, &cost4);
-  const int64_t items8 = build_segs(d, 8, yc, with_grad != 0, s8, &frames8, &groups8, &cost8);
+  // the padding after every block must read as zeros
+  CU(cudaMemset(yc, 0, (size_t)std::max<int64_t>(sum_atoms, 2) * sizeof(double)), "memset");
+  int64_t groups4 = 0, groups8 = 0, cost4 = 0, cost8 = 0, lcost4 = 0, lcost8 = 0;
+  const int64_t items4 = build_segs(d, 4, yc, with_grad != 0, s4, &frames4, &groups4, &cost4, &lcost4);
+  const int64_t items8 = build_segs(d, 8, yc, with_grad != 0, s8, &frames8, &groups8, &cost8, &lcost8);
   const int64_t frames = frames4;
   const size_t rec = wmd::kStatDoubles * sizeof(double);
   if ((rc = ensure(ctx, ctx->b_segs, std::max<size_t>(1, (size_t)n_traj) * sizeof(wmd::BatchSeg))) ||
@@ -1516,7 +1535,13 @@ WMD_EXPORT int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, in
     P.launch.total_items = apt == 4 ? items4 : items8;
     P.launch.total_groups = apt == 4 ? groups4 : groups8;
     P.launch.total_cost = apt == 4 ? cost4 : cost8;
-    if (variant == wmd::kBatchFrames) {
+    P.launch.total_lane_cost = apt == 4 ? lcost4 : lcost8;
+    if (variant == wmd::kBatchLanes) {
+      int64_t units = 0;
+      for (const wmd::BatchSeg& g : sv) units += g.lane_units;
+      P.grid_fwd = wmd::batched_lanes_grid(ctx->sm_count, units);
+      P.grid_bwd = wmd::batched_grid(apt, true, ctx->sm_count, P.launch.total_items);
+    } else if (variant == wmd::kBatchFrames) {
       P.grid_fwd = wmd::batched_frame_grid(apt, with_grad != 0, ctx->sm_count, P.launch.total_groups);
       P.grid_bwd = P.grid_fwd;
     } else {
@@ -1525,7 +1550,7 @@ WMD_EXPORT int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, in
     }
     return WMD_OK;
   };
-  std::vector<int> apts = {8, 4}, layouts = {wmd::kBatchFrames, wmd::kBatchTiles};
+  std::vector<int> apts = {8, 4}, layouts = {wmd::kBatchFrames, wmd::kBatchTiles, wmd::kBatchLanes};
   if (const char* env = std::getenv("WARPMD_BATCHED_TILE_ATOMS")) {
     if (std::strcmp(env, "512") == 0) apts = {4};
     else if (std::strcmp(env, "1024") == 0) apts = {8};
@@ -1533,6 +1558,7 @@ WMD_EXPORT int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, in
   if (const char* env = std::getenv("WARPMD_BATCHED_LAYOUT")) {
     if (std::strcmp(env, "tiles") == 0) layouts = {wmd::kBatchTiles};
     else if (std::strcmp(env, "frames") == 0) layouts = {wmd::kBatchFrames};
+    else if (std::strcmp(env, "lanes") == 0) layouts = {wmd::kBatchLanes};
   }
   float best_ms = -1.f;
   int best_apt = apts[0], best_layout = layouts[0];
@@ -1586,7 +1612,7 @@ WMD_EXPORT int wmd_batched_layout(const wmd_ctx* ctx, int* tile_atoms, int* fram
   if (!ctx) return WMD_ERR_INVALID_ARG;
   if (!ctx->b_ready) return set_err(const_cast<wmd_ctx*>(ctx), WMD_ERR_INVALID_ARG, "no batch is prepared");
   if (tile_atoms) *tile_atoms = wmd::batched_tile_atoms(ctx->b_plan.apt);
-  if (frame_major) *frame_major = ctx->b_plan.variant == wmd::kBatchFrames ? 1 : 0;
+  if (frame_major) *frame_major = ctx->b_plan.variant;
   return WMD_OK;
 }
 

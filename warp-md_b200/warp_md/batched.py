@@ -89,7 +89,8 @@ class BatchedRmsd:
         """The layout the prepare step's autotuner chose."""
         t, fm = ctypes.c_int(), ctypes.c_int()
         self.ctx.check(self.ctx.lib.wmd_batched_layout(self.ctx.handle, ctypes.byref(t), ctypes.byref(fm)))
-        return {"tile_atoms": t.value, "frame_major": bool(fm.value)}
+        return {"tile_atoms": t.value, "frame_major": fm.value == 1,
+                "layout": {0: "tiles", 1: "frames", 2: "lanes"}.get(fm.value, str(fm.value))}
 
     def close(self) -> None:
         self.ctx.close()
