@@ -897,7 +897,11 @@ def run_ours(args):
             e2e = {"value": float(N_ATOMS) * e2e_frames * ws * max(1, args.e2e_steps) / (ems / 1e3), "unit": UNIT,
                    "h2d_bytes_per_step": int(e2e_frames * N_ATOMS * 12), "d2h_bytes_per_step": int(e2e_frames * 8),
                    "frames": e2e_frames, "host_buffer": "pinned"}
-            np.testing.assert_allclose(hout, vals[:e2e_frames], rtol=0, atol=0)
+            # host input runs in chunks whose launches may tile the atoms
+            # differently; the FP64 sums then round differently (~1e-8 A here)
+            e2e_diff = float(np.abs(hout - vals[:e2e_frames]).max())
+            assert e2e_diff <= 1e-6, e2e_diff
+            e2e["max_abs_diff_vs_device_resident_A"] = e2e_diff
         except RuntimeError as exc:  # e.g. pinned allocation refused on the host
             e2e = {"value": None, "unit": UNIT, "error": str(exc)[:200]}
 
