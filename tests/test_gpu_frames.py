@@ -120,6 +120,28 @@ def test_selection_gather(gpu_ctx, device_io):
     np.testing.assert_allclose(raw, expr, rtol=0, atol=TOL)
 
 
+@pytest.mark.parametrize("step,offset,n_atoms", [(2, 3, 20000), (3, 0, 4000), (1, 7, 3000), (4, 5, 2500),
+                                                 (10, 1, 3000)])
+def test_sorted_sparse_selection_spans(gpu_ctx, step, offset, n_atoms):
+    """Sorted host selections (every step-th atom from an offset) at least 1/4
+    dense run as the atom span they cover with zero-weight gaps
+    (frames-across-lanes kernel); sparser ones and an unsorted copy of the
+    same selection take the gathered path; all match the oracle, aligned and
+    raw."""
+    fr, _ = synth.make_trajectory(n_atoms, 70, (0.05, 2.0), seed=step * 100 + offset)
+    sel = np.arange(offset, n_atoms, step, dtype=np.uint32)
+    ref = fr[5][sel]
+    for s in (sel, sel[::-1].copy()):
+        r = fr[5][s]
+        got = gpu_rmsd(gpu_ctx, fr, r, sel=s)
+        _, exp = oracle.rmsd_frames(fr, r, selection=s)
+        np.testing.assert_allclose(got, exp, rtol=0, atol=TOL)
+        raw = gpu_rmsd(gpu_ctx, fr, r, sel=s, align=False)
+        _, expr = oracle.rmsd_frames(fr, r, selection=s, align=False)
+        np.testing.assert_allclose(raw, expr, rtol=0, atol=TOL)
+    assert ref.shape[0] == sel.size
+
+
 def test_unaligned_device_base(gpu_ctx):
     fr, ref = synth.make_trajectory(777, 9, 0.4, seed=12)
     flat = torch.empty(fr.size + 1, dtype=torch.float32, device="cuda")

@@ -79,7 +79,10 @@ def test_superpose_dense_matches_oracle(device_io):
 
 def test_superpose_selection_weights_and_ragged_sizes():
     rng = np.random.default_rng(3)
-    for n_atoms, F, n_sel in [(7, 3, 4), (1025, 5, 300), (5000, 4, 1100), (40000, 2, 9000)]:
+    # (1025, 300) and (8000, 4000), at least 1/4 dense, also stream their atom span with weights; the
+    # full selection of 4096 atoms streams the weighted dense selection
+    for n_atoms, F, n_sel in [(7, 3, 4), (1025, 5, 300), (5000, 4, 1100), (40000, 2, 9000), (8000, 37, 4000),
+                              (4096, 33, 4096)]:
         fr, ref_all = synth.make_trajectory(n_atoms, F, 0.7, n_atoms)
         sel = np.sort(rng.choice(n_atoms, n_sel, replace=False)).astype(np.uint32)
         w = rng.uniform(1.0, 32.0, n_atoms).astype(np.float32)

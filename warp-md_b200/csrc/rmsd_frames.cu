@@ -514,7 +514,8 @@ static int occupancy(const FrameLaunch& L) {
 }
 
 int frame_tiles(const FrameLaunch& L) {
-  return (int)((L.ref.n_sel + L.tile_atoms - 1) / L.tile_atoms);
+  const int64_t n = L.lanes ? L.lane_atoms : L.ref.n_sel;
+  return (int)((n + L.tile_atoms - 1) / L.tile_atoms);
 }
 
 size_t frame_smem_bytes(int stride, int tile_atoms) {
@@ -523,7 +524,15 @@ size_t frame_smem_bytes(int stride, int tile_atoms) {
 }
 
 void frame_plan(FrameLaunch& L, int sm_count) {
-  L.lanes = lanes_eligible(L) && lanes_worthwhile(L, sm_count);
+  // a dense selection streams itself; a gathered one only through an
+  // expansion the caller prepared (lane_y set)
+  if (!L.lane_y && !L.gather) {
+    L.lane_atom0 = 0;
+    L.lane_atoms = L.ref.n_sel;
+    L.lane_y = L.ref.yc;
+    L.lane_w = L.ref.w;
+  }
+  L.lanes = L.lane_y && lanes_eligible(L) && lanes_worthwhile(L, sm_count);
   L.tile_atoms = L.lanes ? lanes_tile(L, sm_count) : kConsumerThreads * kApt;
 }
 
@@ -561,12 +570,12 @@ cudaError_t launch_rmsd_forward(const FrameLaunch& L, cudaStream_t s) {
 
 cudaError_t launch_rmsd_stream(const FrameLaunch& L, cudaStream_t s) {
   if (L.n_frames == 0) return cudaSuccess;
-  return dispatch<kFwdFit>(L, s);
+  return L.lanes ? launch_lanes_forward(L, false, s) : dispatch<kFwdFit>(L, s);
 }
 
 cudaError_t launch_rmsd_stream_weighted(const FrameLaunch& L, cudaStream_t s) {
   if (L.n_frames == 0) return cudaSuccess;
-  return dispatch<kFwdW>(L, s);
+  return L.lanes ? launch_lanes_forward(L, false, s) : dispatch<kFwdW>(L, s);
 }
 
 cudaError_t launch_rmsd_backward(const FrameLaunch& L, const double* stats, const float* grad_rmsd,

@@ -20,11 +20,15 @@
 //     warp gets the same number of whole units, so results do not depend on
 //     the launch shape and are bitwise reproducible.
 //
-// Requirements (else the atom-major kernel runs): dense selection (the first
-// n_sel atoms), a 16-byte aligned base and a frame stride that is a multiple
-// of 16 bytes (n_atoms % 4 == 0 for packed xyz).  The reference centred
-// coordinates must be padded with 32 zero atoms (the bulk copy of the last
-// stage reads past n_sel).
+// Atoms streamed: a dense selection (the first n_sel atoms), or the span
+// [lane_atom0, lane_atom0 + lane_atoms) of a sorted selection with the
+// reference expanded onto it and per-atom weights (1 for selected atoms, 0
+// for the rest; or the masses of a weighted reference).  The weights also
+// serve weighted references over dense selections.  Requirements (else the
+// atom-major kernel runs): a 16-byte aligned first streamed atom and a frame
+// stride that is a multiple of 16 bytes (n_atoms % 4 == 0 for packed xyz).
+// The reference values and weights must be padded with 32 zero atoms (the
+// bulk copies of the last stage read past the span).
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -49,7 +53,8 @@ struct LaneGeo {
   static constexpr int kBoxes = kLaneAtoms * STRIDE / 32;  // [32 frames][32 floats] boxes per stage
   static constexpr int kXBytes = kBoxes * 32 * 32 * 4;
   static constexpr int kYBytes = kLaneAtoms * 3 * 8;
-  static constexpr int kStageBytes = (kXBytes + kYBytes + 1023) / 1024 * 1024;
+  static constexpr int kWBytes = kLaneAtoms * 4;  // per-atom weights (weighted / expanded launches)
+  static constexpr int kStageBytes = (kXBytes + kYBytes + kWBytes + 1023) / 1024 * 1024;
   static constexpr int kBarOffset = kLaneWarps * kLaneStages * kStageBytes;
   static constexpr int kAbortOffset = kBarOffset + kLaneWarps * kLaneStages * 8;
   static constexpr int kSmemBytes = kAbortOffset + 16 + 1024;  // + slack to align the base to 1024
@@ -65,17 +70,20 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 
 // One lane's sums over the valid atoms of a stage (valid is warp-uniform).
 // Packed xyz: 4 atoms = 3 swizzled 16-byte chunks; xyzw: 1 atom = 1 chunk.
-template <int STRIDE, bool RAW>
+template <int STRIDE, bool RAW, bool W>
 __device__ __forceinline__ void stage_sums(double (&acc)[15], const unsigned char* st, int lane, int valid,
                                            const FrameLaunch& L) {
+  const float* wb = reinterpret_cast<const float*>(st + LaneGeo<STRIDE>::kXBytes + LaneGeo<STRIDE>::kYBytes);
   const unsigned char* row = st + lane * 128;
   const int sw = lane & 7;
   auto chunk = [&](int c) -> float4 {
     return *reinterpret_cast<const float4*>(row + (c >> 3) * 4096 + (((c & 7) ^ sw) << 4));
   };
   const double2* yb = reinterpret_cast<const double2*>(st + LaneGeo<STRIDE>::kXBytes);
-  auto add_atom = [&](float fx, float fy, float fz, double y0, double y1, double y2, bool in) {
+  // k: the atom's index within the stage (its weight; y is pre-multiplied)
+  auto add_atom = [&](float fx, float fy, float fz, double y0, double y1, double y2, bool in, int k) {
     const double x0 = fx, x1 = fy, x2 = fz;
+    if (W && RAW) in = in && wb[k] != 0.0f;  // expanded selection: unselected atoms have weight 0
     if (RAW) {
       const double d0 = x0 - (y0 + L.ref.mean[0]);
       const double d1 = x1 - (y1 + L.ref.mean[1]);
@@ -84,8 +92,15 @@ __device__ __forceinline__ void stage_sums(double (&acc)[15], const unsigned cha
       acc[1] = fma(d1, in ? d1 : 0.0, acc[1]);
       acc[2] = fma(d2, in ? d2 : 0.0, acc[2]);
     } else {
-      acc[0] += x0; acc[1] += x1; acc[2] += x2;
-      acc[3] = fma(x0, x0, acc[3]); acc[4] = fma(x1, x1, acc[4]); acc[5] = fma(x2, x2, acc[5]);
+      if (W) {  // sum w x, sum w x_a^2 (the weighted forms of rmsd_frames_kernel)
+        const double w = wb[k];
+        const double u0 = w * x0, u1 = w * x1, u2 = w * x2;
+        acc[0] += u0; acc[1] += u1; acc[2] += u2;
+        acc[3] = fma(u0, x0, acc[3]); acc[4] = fma(u1, x1, acc[4]); acc[5] = fma(u2, x2, acc[5]);
+      } else {
+        acc[0] += x0; acc[1] += x1; acc[2] += x2;
+        acc[3] = fma(x0, x0, acc[3]); acc[4] = fma(x1, x1, acc[4]); acc[5] = fma(x2, x2, acc[5]);
+      }
       acc[6] = fma(x0, y0, acc[6]);  acc[7] = fma(x0, y1, acc[7]);  acc[8] = fma(x0, y2, acc[8]);
       acc[9] = fma(x1, y0, acc[9]);  acc[10] = fma(x1, y1, acc[10]); acc[11] = fma(x1, y2, acc[11]);
       acc[12] = fma(x2, y0, acc[12]); acc[13] = fma(x2, y1, acc[13]); acc[14] = fma(x2, y2, acc[14]);
@@ -98,10 +113,10 @@ __device__ __forceinline__ void stage_sums(double (&acc)[15], const unsigned cha
       const float4 a = chunk(3 * m), b = chunk(3 * m + 1), c = chunk(3 * m + 2);
       const double2 y01 = yb[6 * m + 0], y23 = yb[6 * m + 1], y45 = yb[6 * m + 2];
       const double2 y67 = yb[6 * m + 3], y89 = yb[6 * m + 4], yab = yb[6 * m + 5];
-      add_atom(a.x, a.y, a.z, y01.x, y01.y, y23.x, 4 * m + 0 < valid);
-      add_atom(a.w, b.x, b.y, y23.y, y45.x, y45.y, 4 * m + 1 < valid);
-      add_atom(b.z, b.w, c.x, y67.x, y67.y, y89.x, 4 * m + 2 < valid);
-      add_atom(c.y, c.z, c.w, y89.y, yab.x, yab.y, 4 * m + 3 < valid);
+      add_atom(a.x, a.y, a.z, y01.x, y01.y, y23.x, 4 * m + 0 < valid, 4 * m + 0);
+      add_atom(a.w, b.x, b.y, y23.y, y45.x, y45.y, 4 * m + 1 < valid, 4 * m + 1);
+      add_atom(b.z, b.w, c.x, y67.x, y67.y, y89.x, 4 * m + 2 < valid, 4 * m + 2);
+      add_atom(c.y, c.z, c.w, y89.y, yab.x, yab.y, 4 * m + 3 < valid, 4 * m + 3);
     }
   } else {
 #pragma unroll
@@ -109,13 +124,13 @@ __device__ __forceinline__ void stage_sums(double (&acc)[15], const unsigned cha
       if (2 * m >= valid) break;
       const float4 a = chunk(2 * m), b = chunk(2 * m + 1);
       const double2 y01 = yb[3 * m + 0], y23 = yb[3 * m + 1], y45 = yb[3 * m + 2];
-      add_atom(a.x, a.y, a.z, y01.x, y01.y, y23.x, 2 * m + 0 < valid);
-      add_atom(b.x, b.y, b.z, y23.y, y45.x, y45.y, 2 * m + 1 < valid);
+      add_atom(a.x, a.y, a.z, y01.x, y01.y, y23.x, 2 * m + 0 < valid, 2 * m + 0);
+      add_atom(b.x, b.y, b.z, y23.y, y45.x, y45.y, 2 * m + 1 < valid, 2 * m + 1);
     }
   }
 }
 
-template <int STRIDE, bool RAW>
+template <int STRIDE, bool RAW, bool W>
 __global__ void __launch_bounds__(kLaneWarps * 32) rmsd_lanes_kernel(const __grid_constant__ CUtensorMap map,
                                                                      const FrameLaunch L) {
   using G = LaneGeo<STRIDE>;
@@ -127,7 +142,9 @@ __global__ void __launch_bounds__(kLaneWarps * 32) rmsd_lanes_kernel(const __gri
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + G::kAbortOffset);
   unsigned char* ring = smem + warp * kLaneStages * G::kStageBytes;
 
-  const int64_t F = L.n_frames, n_sel = L.ref.n_sel;
+  // atoms streamed: the selection itself, or the atom span an expanded
+  // selection covers (L.lane_atom0 is folded into the tensor map's base)
+  const int64_t F = L.n_frames, n_sel = L.lane_atoms;
   const int64_t groups = (F + 31) / 32;
   const int64_t tile = L.tile_atoms;  // a multiple of kLaneAtoms
   const int n_tiles = (int)((n_sel + tile - 1) / tile);
@@ -158,11 +175,12 @@ __global__ void __launch_bounds__(kLaneWarps * 32) rmsd_lanes_kernel(const __gri
     const int64_t a0 = t * tile + (int64_t)pk * kLaneAtoms;
     // the warp's earlier generic reads of this slot before the async writes
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_arrive_expect_tx(&full[slot], G::kXBytes + G::kYBytes);
+    mbar_arrive_expect_tx(&full[slot], G::kXBytes + G::kYBytes + (W ? G::kWBytes : 0));
 #pragma unroll
     for (int b = 0; b < G::kBoxes; ++b)
       tma_load_2d(dst + b * 4096, &map, (int)(a0 * STRIDE + 32 * b), (int)(g * 32), &full[slot]);
-    bulk_copy_g2s(dst + G::kXBytes, L.ref.yc + a0 * 3, G::kYBytes, &full[slot]);
+    bulk_copy_g2s(dst + G::kXBytes, L.lane_y + a0 * 3, G::kYBytes, &full[slot]);
+    if (W) bulk_copy_g2s(dst + G::kXBytes + G::kYBytes, L.lane_w + a0, G::kWBytes, &full[slot]);
     ++n_issued;
     if (++pk == p_kst && ++pu < u1) {
       pk = 0;
@@ -189,7 +207,7 @@ __global__ void __launch_bounds__(kLaneWarps * 32) rmsd_lanes_kernel(const __gri
       }
       const int64_t a0 = t * tile + (int64_t)k * kLaneAtoms;
       const int valid = (int)min((int64_t)kLaneAtoms, n_sel - a0);
-      stage_sums<STRIDE, RAW>(acc, ring + slot * G::kStageBytes, lane, valid, L);
+      stage_sums<STRIDE, RAW, W>(acc, ring + slot * G::kStageBytes, lane, valid, L);
       ++n_done;
       __syncwarp();
       if (lane == 0 && pu < u1) issue_next();
@@ -243,12 +261,12 @@ EncodeTiled encode_fn() {
 }
 
 int64_t lane_units(const FrameLaunch& L, int64_t tile) {
-  return ((L.n_frames + 31) / 32) * ((L.ref.n_sel + tile - 1) / tile);
+  return ((L.n_frames + 31) / 32) * ((L.lane_atoms + tile - 1) / tile);
 }
 
 template <int STRIDE, bool RAW>
 int lanes_occupancy() {
-  auto kern = rmsd_lanes_kernel<STRIDE, RAW>;
+  auto kern = rmsd_lanes_kernel<STRIDE, RAW, false>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, LaneGeo<STRIDE>::kSmemBytes);
   int b = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kLaneWarps * 32, LaneGeo<STRIDE>::kSmemBytes) !=
@@ -257,20 +275,21 @@ int lanes_occupancy() {
   return std::max(b, 1);
 }
 
-template <int STRIDE, bool RAW>
+template <int STRIDE, bool RAW, bool W>
 cudaError_t launch_lanes(const FrameLaunch& L, cudaStream_t s) {
   EncodeTiled enc = encode_fn();
   if (!enc) return cudaErrorNotSupported;
   CUtensorMap map;
-  const cuuint64_t dims[2] = {(cuuint64_t)(L.ref.n_sel * STRIDE), (cuuint64_t)L.n_frames};
+  const cuuint64_t dims[2] = {(cuuint64_t)(L.lane_atoms * STRIDE), (cuuint64_t)L.n_frames};
   const cuuint64_t strides[1] = {(cuuint64_t)(L.n_atoms * STRIDE * 4)};
   const cuuint32_t box[2] = {32, 32};
   const cuuint32_t estr[2] = {1, 1};
-  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(L.coords), dims, strides, box, estr,
+  float* base = const_cast<float*>(L.coords) + L.lane_atom0 * STRIDE;
+  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr,
           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return cudaErrorInvalidValue;
-  auto kern = rmsd_lanes_kernel<STRIDE, RAW>;
+  auto kern = rmsd_lanes_kernel<STRIDE, RAW, W>;
   static bool attr_done[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -284,7 +303,29 @@ cudaError_t launch_lanes(const FrameLaunch& L, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// y_exp[(sel[i] - a0)][c] = yc[i][c], w_exp[sel[i] - a0] = w ? w[i] : 1 (the
+// buffers were zeroed; selection indices are strictly increasing)
+__global__ void lanes_expand_kernel(const uint32_t* __restrict__ sel, int64_t n_sel, int64_t a0,
+                                    const double* __restrict__ yc, const float* __restrict__ w,
+                                    double* __restrict__ y_exp, float* __restrict__ w_exp) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_sel; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = (int64_t)sel[i] - a0;
+    y_exp[k * 3 + 0] = yc[i * 3 + 0];
+    y_exp[k * 3 + 1] = yc[i * 3 + 1];
+    y_exp[k * 3 + 2] = yc[i * 3 + 2];
+    w_exp[k] = w ? w[i] : 1.0f;
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_lanes_expand(const uint32_t* sel, int64_t n_sel, int64_t a0, const double* yc, const float* w,
+                                double* y_exp, float* w_exp, cudaStream_t s) {
+  if (n_sel <= 0) return cudaSuccess;
+  const unsigned grid = (unsigned)std::min<int64_t>((n_sel + 255) / 256, 4096);
+  lanes_expand_kernel<<<grid, 256, 0, s>>>(sel, n_sel, a0, yc, w, y_exp, w_exp);
+  return cudaGetLastError();
+}
 
 bool lanes_eligible(const FrameLaunch& L) {
   static int mode = -1;
@@ -292,10 +333,11 @@ bool lanes_eligible(const FrameLaunch& L) {
     const char* e = std::getenv("WMD_FRAMES_KERNEL");
     mode = (e && std::strcmp(e, "atoms") == 0) ? 0 : 1;
   }
-  if (!mode || L.gather || L.ref.n_sel <= 0 || L.n_frames <= 0) return false;
+  if (!mode || L.lane_atoms <= 0 || L.n_frames <= 0) return false;
   if (L.stride != 4 && (L.n_atoms & 3) != 0) return false;
-  if ((reinterpret_cast<uintptr_t>(L.coords) & 15u) != 0) return false;
-  if (L.ref.n_sel * L.stride >= (int64_t(1) << 31) || L.n_frames >= (int64_t(1) << 31)) return false;
+  if ((reinterpret_cast<uintptr_t>(L.coords + L.lane_atom0 * L.stride) & 15u) != 0) return false;
+  if ((L.lane_atom0 + L.lane_atoms) * L.stride >= (int64_t(1) << 31) || L.n_frames >= (int64_t(1) << 31))
+    return false;
   return true;
 }
 
@@ -345,8 +387,13 @@ int lanes_grid(const FrameLaunch& L, int sm_count) {
 cudaError_t launch_lanes_forward(const FrameLaunch& L, bool raw, cudaStream_t s) {
   FrameLaunch K = L;
   K.lane_warps = (int)lane_warps(L, (int64_t)L.grid * kLaneWarps);
-  if (L.stride == 4) return raw ? launch_lanes<4, true>(K, s) : launch_lanes<4, false>(K, s);
-  return raw ? launch_lanes<3, true>(K, s) : launch_lanes<3, false>(K, s);
+  const bool w = L.lane_w != nullptr;
+  if (L.stride == 4) {
+    if (w) return raw ? launch_lanes<4, true, true>(K, s) : launch_lanes<4, false, true>(K, s);
+    return raw ? launch_lanes<4, true, false>(K, s) : launch_lanes<4, false, false>(K, s);
+  }
+  if (w) return raw ? launch_lanes<3, true, true>(K, s) : launch_lanes<3, false, true>(K, s);
+  return raw ? launch_lanes<3, true, false>(K, s) : launch_lanes<3, false, false>(K, s);
 }
 
 }  // namespace wmd

@@ -98,6 +98,15 @@ struct wmd_ctx {
   DevBuf partial, refine, refine_count, rot, chunk[2], out_tmp, sel_buf, aux, out_chunk;
   DevBuf fl_part, fl_acc, fl_shift;
   DevBuf cl_mat, cl_scratch, cl_out, km_feat, km_xf, km_work;  // clustering  // fluctuations, per-group RMSD
+  // a sorted host selection expanded onto its atom span for the
+  // frames-across-lanes kernel, valid for the current call
+  DevBuf lane_exp;
+  struct {
+    bool valid = false;
+    int64_t a0 = 0, span = 0;
+    const double* y = nullptr;
+    const float* w = nullptr;
+  } lx;
   HostBuf stage[2];
   std::string err;
   wmd::PairwiseWorkspace pw;
@@ -256,6 +265,53 @@ int resolve_sel(wmd_ctx* ctx, const uint32_t* sel, int64_t n_sel, int64_t n_atom
   return WMD_OK;
 }
 
+// A host selection that is strictly increasing and at least 1/4 dense is
+// streamed by the frames-across-lanes kernel as the atom span it covers: the
+// reference (centred, weighted) and the weights are expanded onto the span,
+// unselected atoms weighing 0.  At that density the gathered loads fetch
+// most sectors of the span anyway, at a latency-bound rate; the span streams
+// at the HBM rate.  Sparser selections (1 in 10: the gathered loads fetch
+// about half the span's sectors) stay on the gathered path, which measured
+// faster there.  Valid for the current call (LaneScope).
+int lanes_prepare(wmd_ctx* ctx, const uint32_t* sel, const uint32_t* dsel, int64_t n_sel, int stride,
+                  const wmd_ref* ref, cudaStream_t s) {
+  ctx->lx.valid = false;
+  if (!sel || !dsel || n_sel < 64 || !is_host(classify(sel))) return WMD_OK;
+  for (int64_t i = 1; i < n_sel; ++i)
+    if (sel[i] <= sel[i - 1]) return WMD_OK;
+  const int64_t a0 = stride == 4 ? (int64_t)sel[0] : (int64_t)(sel[0] & ~3u);  // 16-byte aligned first atom
+  const int64_t span = (int64_t)sel[n_sel - 1] + 1 - a0;
+  if (span > 4 * n_sel) return WMD_OK;
+  const size_t ybytes = ((size_t)(span + 32) * 3 * sizeof(double) + 255) & ~size_t(255);
+  const size_t wbytes = (size_t)(span + 32) * sizeof(float);
+  int rc = ensure(ctx, ctx->lane_exp, ybytes + wbytes);
+  if (rc) return rc;
+  double* y = static_cast<double*>(ctx->lane_exp.ptr);
+  float* w = reinterpret_cast<float*>(static_cast<char*>(ctx->lane_exp.ptr) + ybytes);
+  CU(cudaMemsetAsync(ctx->lane_exp.ptr, 0, ybytes + wbytes, s), "memset");
+  CU(wmd::launch_lanes_expand(dsel, n_sel, a0, ref->yc, ref->info.w, y, w, s), "selection expansion");
+  ctx->lx.valid = true;
+  ctx->lx.a0 = a0;
+  ctx->lx.span = span;
+  ctx->lx.y = y;
+  ctx->lx.w = w;
+  return WMD_OK;
+}
+
+struct LaneScope {
+  wmd_ctx* ctx;
+  ~LaneScope() { ctx->lx.valid = false; }
+};
+
+// The expansion of the current call, if any, for launches over `dsel`.
+void apply_lanes(wmd_ctx* ctx, wmd::FrameLaunch& L, const uint32_t* dsel) {
+  if (!dsel || !ctx->lx.valid) return;
+  L.lane_atom0 = ctx->lx.a0;
+  L.lane_atoms = ctx->lx.span;
+  L.lane_y = ctx->lx.y;
+  L.lane_w = ctx->lx.w;
+}
+
 wmd::FrameLaunch base_launch(wmd_ctx* ctx, const wmd_ref* ref, int64_t n_atoms, int stride, const uint32_t* dsel) {
   wmd::FrameLaunch L;
   L.n_atoms = n_atoms;
@@ -278,6 +334,7 @@ int forward_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames, int64_t
   L.gather = dsel != nullptr || (reinterpret_cast<uintptr_t>(dcoords) & 15u) != 0;
   L.coords = dcoords;
   L.n_frames = n_frames;
+  apply_lanes(ctx, L, dsel);
   wmd::frame_plan(L, ctx->sm_count);
   const int tiles = wmd::frame_tiles(L);
   const size_t per_frame = (size_t)tiles * wmd::kStatDoubles * sizeof(double);
@@ -425,7 +482,7 @@ WMD_EXPORT int wmd_destroy(wmd_ctx* ctx) {
   cudaDeviceSynchronize();
   for (DevBuf* b : {&ctx->partial, &ctx->refine, &ctx->refine_count, &ctx->rot, &ctx->chunk[0], &ctx->chunk[1], &ctx->out_tmp,
                     &ctx->sel_buf, &ctx->aux, &ctx->out_chunk, &ctx->fl_part, &ctx->fl_acc, &ctx->fl_shift, &ctx->cl_mat, &ctx->cl_scratch,
-                    &ctx->cl_out, &ctx->km_feat, &ctx->km_xf, &ctx->km_work, &ctx->b_segs, &ctx->b_yc, &ctx->b_partial, &ctx->b_rot,
+                    &ctx->cl_out, &ctx->km_feat, &ctx->km_xf, &ctx->km_work, &ctx->lane_exp, &ctx->b_segs, &ctx->b_yc, &ctx->b_partial, &ctx->b_rot,
                     &ctx->b_refine, &ctx->b_count})
     if (b->ptr) cudaFree(b->ptr);
   for (HostBuf* b : {&ctx->stage[0], &ctx->stage[1]})
@@ -531,7 +588,10 @@ static int reference_upload(wmd_ctx* ctx, const float* ref, int64_t n_sel, int s
   const size_t yc_pad = 32 * 3;
   cudaError_t e = cudaMalloc(&r->yc, (yc.size() + yc_pad) * sizeof(double));
   if (e == cudaSuccess) e = cudaMemset(r->yc + yc.size(), 0, yc_pad * sizeof(double));
-  if (e == cudaSuccess && weights && n_sel > 0) e = cudaMalloc(&r->w, (size_t)n_sel * sizeof(float));
+  if (e == cudaSuccess && weights && n_sel > 0) {
+    e = cudaMalloc(&r->w, (size_t)(n_sel + 32) * sizeof(float));  // + 32 zero weights, as yc
+    if (e == cudaSuccess) e = cudaMemset(r->w + n_sel, 0, 32 * sizeof(float));
+  }
   if (e != cudaSuccess) {
     cudaFree(r->yc);
     delete r;
@@ -582,6 +642,8 @@ static int frames_common(wmd_ctx* ctx, const float* coords, int64_t n_frames, in
   const uint32_t* dsel = nullptr;
   int rc = resolve_sel(ctx, sel, n_sel, n_atoms, &dsel, s);
   if (rc) return rc;
+  LaneScope lane_scope{ctx};
+  if ((rc = lanes_prepare(ctx, sel, dsel, n_sel, stride, ref, s))) return rc;
   if (n_sel == 0) {
     // the reference returns 0.0 for every frame (plan.rs:1166-1168)
     if (o_user.rmsd) {
@@ -703,6 +765,10 @@ static int superpose_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames
   wmd::FrameLaunch L = base_launch(ctx, ref, n_atoms, stride, dsel);
   L.align = 1;
   L.gather = dsel != nullptr || (reinterpret_cast<uintptr_t>(dcoords) & 15u) != 0;
+  L.coords = dcoords;
+  L.n_frames = n_frames;
+  apply_lanes(ctx, L, dsel);
+  wmd::frame_plan(L, ctx->sm_count);
   const int tiles = wmd::frame_tiles(L);
   const size_t per_frame = (size_t)std::max(tiles, 1) * wmd::kStatDoubles * sizeof(double);
   const int64_t batch = std::min<int64_t>(n_frames, std::max<int64_t>(1, (int64_t)(kPartialBytesMax / per_frame)));
@@ -802,6 +868,8 @@ static int superpose_common(wmd_ctx* ctx, const float* coords, int64_t n_frames,
   if (n_frames == 0) return WMD_OK;
   const uint32_t* dsel = nullptr;
   if ((rc = resolve_sel(ctx, sel, n_sel, n_atoms, &dsel, s))) return rc;
+  LaneScope lane_scope{ctx};
+  if ((rc = lanes_prepare(ctx, sel, dsel, n_sel, stride, ref, s))) return rc;
   const Mem cm = classify(coords);
   const bool out_host = out && is_host(classify(out));
   const bool xf_host = transforms && is_host(classify(transforms));
@@ -1069,6 +1137,8 @@ WMD_EXPORT int wmd_rmsd_per_group(wmd_ctx* ctx, const float* coords, int64_t n_f
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const uint32_t* dsel = nullptr;
   if (align && (rc = resolve_sel(ctx, sel, n_sel, n_atoms, &dsel, s))) return rc;
+  LaneScope lane_scope{ctx};
+  if (align && (rc = lanes_prepare(ctx, sel, dsel, n_sel, stride, ref, s))) return rc;
   GroupJob job;
   job.goff = groups->goff;
   job.gatoms = groups->gatoms;

@@ -45,6 +45,10 @@ struct FrameLaunch {
   int tile_atoms = 2048;          // atoms per tile (kConsumerThreads * atoms/thread, or kLaneTile)
   bool lanes = false;             // frames-across-lanes forward kernel (rmsd_lanes.cu)
   int lane_warps = 0;             // its active warps (set at launch)
+  int64_t lane_atom0 = 0;         // its atoms: [lane_atom0, lane_atom0 + lane_atoms) of every frame
+  int64_t lane_atoms = 0;
+  const double* lane_y = nullptr; // reference values over those atoms (centred, weighted), +32 zero atoms
+  const float* lane_w = nullptr;  // per-atom weights over those atoms, or null (all 1)
   int align = 1;
   RefInfo ref;
   FrameOutputs out;
@@ -79,6 +83,11 @@ bool lanes_worthwhile(const FrameLaunch& L, int sm_count);
 int lanes_tile(const FrameLaunch& L, int sm_count);
 int lanes_grid(const FrameLaunch& L, int sm_count);
 cudaError_t launch_lanes_forward(const FrameLaunch& L, bool raw, cudaStream_t s);
+// Expands a strictly increasing device selection's reference values (yc
+// [n_sel][3]) and weights (w, or all 1 when null) onto the atom span starting
+// at a0, into zeroed buffers.
+cudaError_t launch_lanes_expand(const uint32_t* sel, int64_t n_sel, int64_t a0, const double* yc, const float* w,
+                                double* y_exp, float* w_exp, cudaStream_t s);
 size_t frame_smem_bytes(int stride, int tile_atoms);
 // Forward: zeroes L.refine_count, runs the fused kernel, then the residual pass
 // over the frames it flagged.
