@@ -369,7 +369,13 @@ void dcd_close(DcdFile* f) {
 }
 
 ReadPool::ReadPool(int threads) {
-  for (int t = 1; t < threads; ++t) workers_.emplace_back([this] { work(); });
+  // a thread that cannot be started leaves a smaller pool (the caller always
+  // takes parts itself), never a half-built object
+  try {
+    workers_.reserve((size_t)std::max(threads - 1, 0));
+    for (int t = 1; t < threads; ++t) workers_.emplace_back([this] { work(); });
+  } catch (...) {
+  }
 }
 
 ReadPool::~ReadPool() {

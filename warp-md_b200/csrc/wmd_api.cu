@@ -1853,7 +1853,13 @@ WMD_EXPORT int wmd_dcd_open(wmd_ctx* ctx, const char* path, float length_scale, 
     const int t = std::atoi(v);
     if (t > 0 && t <= 64) threads = t;
   }
-  d->pool.reset(new wmd::ReadPool(threads));
+  try {  // nothing may throw across the C ABI
+    d->pool.reset(new wmd::ReadPool(threads));
+  } catch (...) {
+    wmd::dcd_close(&d->f);
+    delete d;
+    return set_err(ctx, WMD_ERR_OOM, "could not allocate the file reader");
+  }
   for (int k = 0; k < 2; ++k) {
     cudaError_t e = cudaEventCreateWithFlags(&d->h2d_done[k], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&d->consumed[k], cudaEventDisableTiming);
