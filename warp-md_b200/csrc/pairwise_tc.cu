@@ -29,9 +29,9 @@
 //              pair's shift-group accumulator (5 x 96 columns for 3 limbs),
 //              commits stages back to the producer and tiles to the epilogue;
 //   warps 2-13 drain: tcgen05.ld of its 32 lanes x 32 columns per group,
-//              exact combination of the groups in int64, its 30 x 30 block of
-//              H staged in shared memory, release of TMEM (the next tile's
-//              MMAs start);
+//              exact combination of the groups in int64, the 9 entries of H
+//              of its 10 x 10 frame pairs staged pair-major in shared memory,
+//              release of TMEM (the next tile's MMAs start);
 //   warps 14-21 stage the tile's per-frame terms (G, centroids);
 //   warps 2-21 then run the FP64 pair epilogue (QCP) for the tile's 1,200
 //              pairs, one pair per lane per round, and the symmetric store.
@@ -67,8 +67,10 @@ constexpr int kQcpWarps = kEpiWarps + kHelpWarps;
 constexpr int kTcThreads = 64 + 32 * kQcpWarps;
 constexpr int kKChunk = 64;            // atoms (= bytes per operand row) per stage
 constexpr int kTmemCols = 512;
-constexpr int kEpiLd = 31;             // row pitch (doubles) of the per-warp 30 x 30 H staging
-constexpr int kEpiWarpBytes = 30 * kEpiLd * 8;
+constexpr int kBlockPairs = kFramesPerQuarter * kSliceFrames;  // 100 frame pairs per drain warp
+// per-warp H staging, pair-major: element e = 3a + b of pair p at [e][p], so
+// the epilogue's lanes (consecutive pairs) read consecutive doubles
+constexpr int kEpiWarpBytes = 9 * kBlockPairs * 8;
 
 template <int LIMBS>
 struct TcGeo {
@@ -324,9 +326,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
               for (int c = 0; c < 16; ++c) acc[c] += (long long)v[c] << (8 * g);
             }
             if (lane < 30) {
+              // lane = 3 pi + a (row frame pi, component a); column 3 pj + b
+              const int pi = lane / 3, a = lane - 3 * pi;
+              double* row = epi + a * 3 * kBlockPairs + pi * kSliceFrames;
 #pragma unroll
-              for (int c = 0; c < 16; ++c)
-                if (16 * half + c < 30) epi[lane * kEpiLd + 16 * half + c] = (double)acc[c] * s2;
+              for (int c = 0; c < 16; ++c) {
+                const int cc = 16 * half + c;
+                if (cc < 30) row[(cc % 3) * kBlockPairs + cc / 3] = (double)acc[c] * s2;
+              }
             }
           }
           tc_fence_before();
@@ -352,7 +359,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       constexpr int kPairs = kEpiWarps * kFramesPerQuarter * kSliceFrames;  // 1200
 #pragma unroll 1
       for (int gp = wq * 32 + lane; gp < kPairs; gp += kQcpWarps * 32) {
-        const int blk = gp / 100, pl = gp - blk * 100;
+        const int blk = gp / kBlockPairs, pl = gp - blk * kBlockPairs;
         const int pi = pl / kSliceFrames, pj = pl - pi * kSliceFrames;
         const int bq = (blk + 2) & 3, bs = blk >> 2;  // lane quarter and slice of drain warp blk
         const int fi = bq * kFramesPerQuarter + pi, fj = kTileFramesM + bs * kSliceFrames + pj;
@@ -362,9 +369,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const double* epi = reinterpret_cast<const double*>(smem + G::kEpiOffset + blk * kEpiWarpBytes);
         double h[9];
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-          for (int b = 0; b < 3; ++b) h[a * 3 + b] = epi[(3 * pi + a) * kEpiLd + 3 * pj + b];
+        for (int e = 0; e < 9; ++e) h[e] = epi[e * kBlockPairs + pl];
         const double gi = frm[fi], gj = frm[fj];
         double v;
         if (args.metric == WMD_PAIR_NOFIT) {
@@ -374,7 +379,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           const double ssq = gi + gj - 2.0 * (h[0] + h[4] + h[8]) + args.n * (d0 * d0 + d1 * d1 + d2 * d2);
           v = ssq > 0.0 ? sqrt(ssq / args.n) : 0.0;
         } else {
-          const QcpOut q = qcp_lambda<true>(h, 0.5 * (gi + gj));
+          const QcpOut q = qcp_lambda(h, 0.5 * (gi + gj));
           v = sqrt(msd_from(gi, gj, q.lambda, args.n));
         }
         args.out[(size_t)i * args.F + j] = (float)v;

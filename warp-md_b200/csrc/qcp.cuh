@@ -130,26 +130,9 @@ struct QcpOut {
   int fallback;  // 1 when lambda came from the SVD
 };
 
-// p / d for the Newton step.  With FAST, on the device and for d within the
-// normal float range, a float reciprocal refined by two Newton-Raphson steps
-// in FP64 (each doubles the correct bits: 24 -> 48 -> 96); the iteration is
-// self-correcting, so the last-bit difference to an IEEE division does not
-// change the converged root.
-template <bool FAST>
-WMD_HD double newton_div(double p, double d) {
-#if defined(__CUDA_ARCH__)
-  if (FAST && fabs(d) > 1e-30 && fabs(d) < 1e30) {
-    double r = (double)__frcp_rn((float)d);
-    r = fma(r, fma(-d, r, 1.0), r);
-    r = fma(r, fma(-d, r, 1.0), r);
-    return p * r;
-  }
-#endif
-  return p / d;
-}
-
-// Largest eigenvalue of K(H); e0 = (G_x + G_y) / 2 >= lambda_max.
-template <bool FAST = false>
+// Largest eigenvalue of K(H); e0 = (G_x + G_y) / 2 >= lambda_max.  The
+// Newton step divides in IEEE FP64: on sm_100a that measured faster than a
+// float reciprocal refined by FP64 Newton-Raphson steps.
 WMD_HD QcpOut qcp_lambda(const double h[9], double e0) {
   QcpOut o{0.0, 0, 0};
   if (!(e0 > 0.0)) return o;
@@ -170,7 +153,7 @@ WMD_HD QcpOut qcp_lambda(const double h[9], double e0) {
     const double p = a * l + c0;               // P(l)  = l^4 + c2 l^2 + c1 l + c0
     const double dp = 2.0 * l2 * l + b + a;    // P'(l) = 4 l^3 + 2 c2 l + c1
     if (!(dp != 0.0)) break;
-    const double delta = newton_div<FAST>(p, dp);
+    const double delta = p / dp;
     l -= delta;
     if (fabs(delta) <= 1e-15 * fabs(l)) {
       converged = true;
