@@ -30,6 +30,9 @@
 // The backward kernel streams the same items again, re-derives R from the QCP
 // eigenvector of the stored H (a per-frame prologue kernel), and writes
 // grad = dL/drmsd * (x - x_bar - R^T y_c) / (n rmsd) as float32.
+//
+// Gathered forward launches (atoms by index, or an unaligned base) run
+// rmsd_gather_kernel instead: a warp per item, no staging, the same partials.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -464,9 +467,130 @@ __global__ void __launch_bounds__(256) rmsd_refine_kernel(const FrameLaunch L) {
   }
 }
 
+// Gathered forward statistics (a selection's scattered atoms, or frames whose
+// base is not 16-byte aligned).  One warp per (tile, frame) item, tiles of
+// kConsumerThreads * kApt list positions as in the streaming kernel, so the
+// partial records and rmsd_finalize_kernel are shared.  No block barrier: a
+// warp walks its contiguous run of items (tile-major, so a tile's indices and
+// reference stay in L1 across frames) in sub-chunks of 32 x kGatherJ
+// positions, all of a sub-chunk's loads in flight before any use, and
+// reduces its sums with shuffles.  Latency is hidden by the warps resident
+// per SM instead of by a CTA-wide pipeline.
+//
+// An atom's 12 bytes cost two loads, not three: an 8-byte load of the pair
+// that starts on an 8-byte boundary (x,y or y,z) and a 4-byte load of the
+// other coordinate.
+constexpr int kGatherJ = 4;
+constexpr int kGatherThreads = 128;
+
+__device__ __forceinline__ void load_xyz(const float* p, float& x, float& y, float& z) {
+  const bool odd = (reinterpret_cast<uintptr_t>(p) & 7u) != 0;
+  const float2 pr = __ldg(reinterpret_cast<const float2*>(p + (odd ? 1 : 0)));
+  const float s = __ldg(p + (odd ? 0 : 2));
+  x = odd ? s : pr.x;
+  y = odd ? pr.x : pr.y;
+  z = odd ? pr.y : s;
+}
+
+template <int STRIDE, int MODE>
+__global__ void __launch_bounds__(kGatherThreads) rmsd_gather_kernel(const FrameLaunch L, int tile) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = ((int64_t)blockIdx.x * kGatherThreads + threadIdx.x) >> 5;
+  const int64_t n_warps = (int64_t)gridDim.x * (kGatherThreads / 32);
+  const int64_t n_sel = L.ref.n_sel;
+  const int64_t F = L.n_frames;
+  const int n_tiles = (int)((n_sel + tile - 1) / tile);
+  const int64_t W = (int64_t)n_tiles * F;
+  const int64_t w0 = W * gw / n_warps, w1 = W * (gw + 1) / n_warps;
+  int t = (int)(w0 / F);
+  int64_t f = w0 - (int64_t)t * F;
+  for (int64_t w = w0; w < w1; ++w) {
+    const int64_t a0 = (int64_t)t * tile;
+    const int64_t a1 = min(n_sel, a0 + tile);
+    const float* frame = L.coords + (size_t)f * L.n_atoms * STRIDE;
+    double acc[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) acc[e] = 0.0;
+#pragma unroll 1
+    for (int64_t c0 = a0; c0 < a1; c0 += 32 * kGatherJ) {
+      float x[kGatherJ][3];
+      double y[kGatherJ][3];
+      float wt[MODE == kFwdW ? kGatherJ : 1];
+#pragma unroll
+      for (int j = 0; j < kGatherJ; ++j) {
+        const int64_t k = c0 + lane + 32 * j;
+        if (k < a1) {
+          int64_t idx = L.sel ? (int64_t)__ldg(L.sel + k) : k;
+          if (idx >= L.n_atoms) {  // bad device-side selection: report, read atom 0
+            atomicOr(L.status, kStatusBadIndex);
+            idx = 0;
+          }
+          load_xyz(frame + idx * STRIDE, x[j][0], x[j][1], x[j][2]);
+          const double* yp = L.ref.yc + k * 3;
+          y[j][0] = __ldg(yp); y[j][1] = __ldg(yp + 1); y[j][2] = __ldg(yp + 2);
+          if (MODE == kFwdW) wt[MODE == kFwdW ? j : 0] = __ldg(L.ref.w + k);
+        } else {
+          x[j][0] = x[j][1] = x[j][2] = 0.f;
+          y[j][0] = y[j][1] = y[j][2] = 0.0;
+          if (MODE == kFwdW) wt[MODE == kFwdW ? j : 0] = 0.f;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kGatherJ; ++j) {
+        const double x0 = x[j][0], x1 = x[j][1], x2 = x[j][2];
+        if (MODE == kFwdRaw) {
+          if (c0 + lane + 32 * j < a1) {
+            const double d0 = x0 - (y[j][0] + L.ref.mean[0]);
+            const double d1 = x1 - (y[j][1] + L.ref.mean[1]);
+            const double d2 = x2 - (y[j][2] + L.ref.mean[2]);
+            acc[0] = fma(d0, d0, acc[0]);
+            acc[1] = fma(d1, d1, acc[1]);
+            acc[2] = fma(d2, d2, acc[2]);
+          }
+        } else {
+          if (MODE == kFwdW) {
+            const double wj = wt[MODE == kFwdW ? j : 0];
+            const double u0 = wj * x0, u1 = wj * x1, u2 = wj * x2;
+            acc[0] += u0; acc[1] += u1; acc[2] += u2;
+            acc[3] = fma(u0, x0, acc[3]); acc[4] = fma(u1, x1, acc[4]); acc[5] = fma(u2, x2, acc[5]);
+          } else {
+            acc[0] += x0; acc[1] += x1; acc[2] += x2;
+            acc[3] = fma(x0, x0, acc[3]); acc[4] = fma(x1, x1, acc[4]); acc[5] = fma(x2, x2, acc[5]);
+          }
+          acc[6] = fma(x0, y[j][0], acc[6]);  acc[7] = fma(x0, y[j][1], acc[7]);  acc[8] = fma(x0, y[j][2], acc[8]);
+          acc[9] = fma(x1, y[j][0], acc[9]);  acc[10] = fma(x1, y[j][1], acc[10]); acc[11] = fma(x1, y[j][2], acc[11]);
+          acc[12] = fma(x2, y[j][0], acc[12]); acc[13] = fma(x2, y[j][1], acc[13]); acc[14] = fma(x2, y[j][2], acc[14]);
+        }
+      }
+    }
+    if (MODE == kFwdRaw) {
+      acc[0] += acc[1] + acc[2];
+      acc[1] = acc[2] = 0.0;
+    }
+    const double v = warp_reduce_scatter16(acc);
+    if ((lane & 1) == 0) L.partial[((size_t)f * n_tiles + t) * kStatDoubles + (lane >> 1)] = v;
+    if (++f == F) { f = 0; ++t; }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // host-side launch helpers
 // ---------------------------------------------------------------------------
+
+template <int STRIDE, int MODE>
+static cudaError_t launch_gather(const FrameLaunch& L, cudaStream_t s) {
+  rmsd_gather_kernel<STRIDE, MODE><<<L.grid, kGatherThreads, 0, s>>>(L, L.tile_atoms);
+  return cudaGetLastError();
+}
+
+template <int STRIDE>
+static int gather_occupancy() {
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, rmsd_gather_kernel<STRIDE, kFwdW>, kGatherThreads, 0) !=
+      cudaSuccess)
+    blocks = 4;
+  return blocks < 1 ? 1 : blocks;
+}
 
 template <int STRIDE, int APT, int MODE, bool GATHER>
 static cudaError_t launch_one(const FrameLaunch& L, cudaStream_t s) {
@@ -503,6 +627,9 @@ constexpr int kApt = 8;
 
 template <int MODE>
 static cudaError_t dispatch(const FrameLaunch& L, cudaStream_t s) {
+  if constexpr (MODE != kBwd) {
+    if (L.gather) return L.stride == 4 ? launch_gather<4, MODE>(L, s) : launch_gather<3, MODE>(L, s);
+  }
   if (L.stride == 4) return L.gather ? launch_one<4, kApt, MODE, true>(L, s) : launch_one<4, kApt, MODE, false>(L, s);
   return L.gather ? launch_one<3, kApt, MODE, true>(L, s) : launch_one<3, kApt, MODE, false>(L, s);
 }
@@ -538,6 +665,14 @@ void frame_plan(FrameLaunch& L, int sm_count) {
 
 int frame_grid(const FrameLaunch& L, int sm_count, bool backward) {
   if (L.lanes && !backward) return lanes_grid(L, sm_count);
+  if (L.gather && !backward) {
+    static int gocc[2] = {};
+    int& occ = gocc[L.stride == 4];
+    if (occ == 0) occ = L.stride == 4 ? gather_occupancy<4>() : gather_occupancy<3>();
+    const int64_t warps = (int64_t)frame_tiles(L) * L.n_frames;  // one warp per item at most
+    const int64_t cap = (int64_t)sm_count * occ;
+    return (int)std::max<int64_t>(1, std::min<int64_t>((warps + kGatherThreads / 32 - 1) / (kGatherThreads / 32), cap));
+  }
   static int cache[2][2][2] = {};  // [bwd][stride4][gather]
   int& occ = cache[backward ? 1 : 0][L.stride == 4][L.gather ? 1 : 0];
   if (occ == 0) occ = backward ? occupancy<kBwd>(L) : occupancy<kFwdFit>(L);
