@@ -101,3 +101,34 @@ def test_zero_rmsd_gives_zero_gradient():
     val.sum().backward()
     assert torch.all(val < 1e-5)
     assert torch.all(torch.isfinite(x.grad))
+
+
+def test_gradient_buffer_fully_written():
+    """Without a selection the gradient buffer is not zero-filled first: the
+    kernel must write every element.  Freed NaN blocks of the same size are
+    left in torch's caching allocator so that unwritten entries would show;
+    a dense prefix (reference shorter than the frame) still gets zeros beyond
+    it, and a selection gets zeros outside it."""
+    from warp_md.torch_ops import rmsd
+
+    for n, F, seed in [(1000, 7, 11), (2048, 4, 12), (37, 9, 13)]:
+        fr, ref = synth.make_trajectory(n, F, 0.3, seed)
+        for _ in range(4):
+            junk = torch.full((F, n, 3), float("nan"), device="cuda")
+            del junk
+        x = torch.from_numpy(fr).cuda().requires_grad_(True)
+        rmsd(x, torch.from_numpy(ref).cuda()).sum().backward()
+        g = x.grad.cpu().numpy()
+        assert np.isfinite(g).all()
+        _check(g, oracle.rmsd_grad(fr, ref)[1])
+        # dense prefix: atoms past the reference get a zero gradient
+        k = n // 2
+        for _ in range(4):
+            junk = torch.full((F, n, 3), float("nan"), device="cuda")
+            del junk
+        x2 = torch.from_numpy(fr).cuda().requires_grad_(True)
+        rmsd(x2, torch.from_numpy(np.ascontiguousarray(ref[:k])).cuda()).sum().backward()
+        g2 = x2.grad.cpu().numpy()
+        assert np.isfinite(g2).all()
+        assert (g2[:, k:] == 0).all()
+        _check(g2[:, :k], oracle.rmsd_grad(np.ascontiguousarray(fr[:, :k]), ref[:k])[1])

@@ -75,7 +75,10 @@ class RmsdFunction(torch.autograd.Function):
         ctx = N.context(x.device.index or 0)
         F, n_atoms = x.shape[0], x.shape[1]
         g = grad_out.to(torch.float32).contiguous()
-        grad = torch.zeros_like(x)
+        # the kernel writes every selected atom of every frame; only atoms
+        # outside the selection need zeros
+        covers_all = not ctx_.has_sel and ref.n_sel == n_atoms
+        grad = torch.empty_like(x) if covers_all else torch.zeros_like(x)
         ctx.check(ctx.lib.wmd_rmsd_backward(ctx.handle, x.data_ptr(), F, n_atoms, 3,
                                             sel.data_ptr() if ctx_.has_sel else None, ref.n_sel, ref.handle,
                                             stats.data_ptr(), g.data_ptr(), grad.data_ptr(), _stream()))
