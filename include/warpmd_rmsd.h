@@ -49,6 +49,7 @@ extern "C" {
 
 #define WMD_PAIR_RMS 0   /* optimal-superposition RMSD (metric "rms")  */
 #define WMD_PAIR_NOFIT 1 /* plain coordinate RMSD (metric "nofit")     */
+#define WMD_PAIR_DME 2   /* distance-matrix error (metric "dme")        */
 
 #define WMD_MODE_FP32 0  /* plain FP32 SIMT covariance tiles, FP64 QCP epilogue       */
 #define WMD_MODE_I8X3 1  /* tcgen05 int8 tensor cores, 3 limbs (24-bit fixed point), */
@@ -124,9 +125,23 @@ int wmd_rmsd_covariance(wmd_ctx* ctx, const float* coords, int64_t n_frames, int
 /* All-pairs RMSD matrix (PairwiseRmsdPlan::finalize, plan.rs:593-674): out is
  * row-major n_frames x n_frames float32, symmetric, zero diagonal, all zeros
  * when n_sel < 2.  coords/sel/out host or device.  metric WMD_PAIR_*,
- * mode WMD_MODE_*. */
+ * mode WMD_MODE_* (ignored for WMD_PAIR_DME, which is wmd_pairwise_dme
+ * without a box). */
 int wmd_pairwise_rmsd(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
                       const uint32_t* sel, int64_t n_sel, int metric, int mode, float* out, void* stream);
+
+/* All-pairs distance-matrix error (PairwiseRmsdPlan metric "dme",
+ * plan.rs:612-645 with pair_distances_compact, plan.rs:1279-1302): per frame the
+ * distances of every selected atom pair a < b (difference in f32, distance in
+ * FP64; with `box`, the minimum image per axis of length > 0 as apply_pbc,
+ * crates/traj-core/src/pbc_math.rs:17-27), then out[i][j] =
+ * sqrt(sum_k (d_i[k] - d_j[k])^2 / n_pairs) in FP64, summed in pair order and
+ * rounded to float32: the reference's numbers.  Symmetric, zero diagonal, all
+ * zeros when n_sel < 2.  box: per-frame orthorhombic lengths [n_frames][3]
+ * float32 (pbc "orthorhombic") or NULL (pbc "none").  coords/sel/box/out host
+ * or device. */
+int wmd_pairwise_dme(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                     const uint32_t* sel, int64_t n_sel, const float* box, float* out, void* stream);
 
 /* One trajectory of a batched launch.  All pointers are device pointers. */
 typedef struct wmd_batch_desc {

@@ -45,6 +45,8 @@ def lib():
         L.wmdo_rmsd_grad.restype = None
         L.wmdo_pairwise_block.argtypes = [_vp, _i64, _i64, _int, _int, _i64, _i64, _i64, _i64, _vp, _vp, _i64, _int]
         L.wmdo_pairwise_block.restype = None
+        L.wmdo_pairwise_dme.argtypes = [_vp, _i64, _i64, _int, _vp, _vp, _vp, _int]
+        L.wmdo_pairwise_dme.restype = None
         L.wmdo_qcp_rmsd.argtypes = [_vp, _vp, _i64, _int, _int]
         L.wmdo_qcp_rmsd.restype = ctypes.c_double
         L.wmdo_svd3.argtypes = [_f64p, _f64p, _f64p, _f64p]
@@ -119,6 +121,19 @@ def pairwise(frames, metric: str = "rms", block=None, threads: int = 0):
     out64 = np.empty((i1 - i0, j1 - j0), np.float64)
     lib().wmdo_pairwise_block(_ptr(c), n, c.shape[1], stride, m, i0, i1, j0, j1, _ptr(out32), _ptr(out64),
                               j1 - j0, int(threads))
+    return out32, out64
+
+
+def pairwise_dme(frames, box=None, threads: int = 0):
+    """PairwiseRmsdPlan metric "dme" over already-selected frames; box =
+    per-frame orthorhombic lengths (n_frames, 3) for pbc "orthorhombic", or
+    None.  Returns (f32, f64) matrices."""
+    c, stride = _coords(frames)
+    n = c.shape[0]
+    b = None if box is None else np.ascontiguousarray(np.broadcast_to(np.asarray(box, np.float32), (n, 3)))
+    out32 = np.empty((n, n), np.float32)
+    out64 = np.empty((n, n), np.float64)
+    lib().wmdo_pairwise_dme(_ptr(c), n, c.shape[1], stride, _ptr(b), _ptr(out32), _ptr(out64), int(threads))
     return out32, out64
 
 

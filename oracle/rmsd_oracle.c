@@ -14,7 +14,9 @@
  *   - rmsd_aligned            plan.rs:1112-1159   (pairwise metric "rms")
  *   - rmsd_raw                plan.rs:1081-1091   (pairwise metric "nofit")
  *   - PairwiseRmsdPlan::finalize  plan.rs:593-674 (symmetric fill, zero
- *       diagonal, n_sel < 2 -> all zeros)
+ *       diagonal, n_sel < 2 -> all zeros); metric "dme" plan.rs:612-645 with
+ *       pair_distances_compact plan.rs:1279-1302 and apply_pbc
+ *       (crates/traj-core/src/pbc_math.rs:17-27)
  *   - AlignPlan / SuperposePlan   crates/traj-engine/src/plans/geometry/align/
  *       plan_exec.rs:125-266, 325-459 with kabsch_rotation_weighted and
  *       centroid_weighted (crates/traj-engine/src/plans/geometry/
@@ -319,6 +321,78 @@ WMDO_API void wmdo_pairwise_block(const float* frames, int64_t n_frames, int64_t
       if (out64) out64[(i - i0) * ld + (j - j0)] = v;
     }
   }
+  (void)n_threads;
+}
+
+/* ------------------------------------------------------------------ */
+/* Pairwise metric "dme" (distance-matrix error)                        */
+/* ------------------------------------------------------------------ */
+
+/* pair_distances_compact (plan.rs:1279-1302) with apply_pbc
+ * (crates/traj-core/src/pbc_math.rs:17-27): every atom pair a < b in
+ * lexicographic order, the coordinate difference taken in f32 and widened to
+ * f64; with a box, the minimum image per axis whose length is > 0
+ * (d -= round(d / L) * L, round half away from zero); distance in f64. */
+static void dme_distances(const float* frame, int64_t n, int stride, const float* box, double* out) {
+  const double lx = box ? (double)box[0] : 0.0, ly = box ? (double)box[1] : 0.0, lz = box ? (double)box[2] : 0.0;
+  int64_t k = 0;
+  for (int64_t a = 0; a < n; ++a) {
+    const float* pa = frame + a * stride;
+    for (int64_t b = a + 1; b < n; ++b) {
+      const float* pb = frame + b * stride;
+      double dx = (double)(float)(pb[0] - pa[0]);
+      double dy = (double)(float)(pb[1] - pa[1]);
+      double dz = (double)(float)(pb[2] - pa[2]);
+      if (box) {
+        if (lx > 0.0) dx -= round(dx / lx) * lx;
+        if (ly > 0.0) dy -= round(dy / ly) * ly;
+        if (lz > 0.0) dz -= round(dz / lz) * lz;
+      }
+      out[k++] = sqrt(dx * dx + dy * dy + dz * dz);
+    }
+  }
+}
+
+/* PairwiseRmsdPlan::finalize for metric Dme (plan.rs:612-645): per frame pair
+ * i < j, sqrt(sum_k (d_i[k] - d_j[k])^2 / n_pairs), the sum in pair order, the
+ * result rounded to f32 and mirrored; zero diagonal; n_sel < 2 -> zeros.
+ * frames: already-selected atoms [n_frames][n_sel][stride]; box: per-frame
+ * orthorhombic lengths [n_frames][3] (pbc "orthorhombic") or NULL ("none"). */
+WMDO_API void wmdo_pairwise_dme(const float* frames, int64_t n_frames, int64_t n_sel, int stride, const float* box,
+                                float* out32, double* out64, int n_threads) {
+  const int64_t nn = n_frames * n_frames;
+  for (int64_t e = 0; e < nn; ++e) {
+    if (out32) out32[e] = 0.f;
+    if (out64) out64[e] = 0.0;
+  }
+  if (n_sel < 2 || n_frames == 0) return;
+  const int64_t n_pairs = n_sel * (n_sel - 1) / 2;
+  double* d = (double*)malloc((size_t)n_frames * (size_t)n_pairs * sizeof(double));
+  if (!d) return;
+#ifdef _OPENMP
+  int nt = n_threads > 0 ? n_threads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+#endif
+  for (int64_t f = 0; f < n_frames; ++f)
+    dme_distances(frames + f * n_sel * stride, n_sel, stride, box ? box + f * 3 : NULL, d + f * n_pairs);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+#endif
+  for (int64_t i = 0; i < n_frames; ++i) {
+    for (int64_t j = i + 1; j < n_frames; ++j) {
+      const double* di = d + i * n_pairs;
+      const double* dj = d + j * n_pairs;
+      double sum = 0.0;
+      for (int64_t k = 0; k < n_pairs; ++k) {
+        const double diff = di[k] - dj[k];
+        sum += diff * diff;
+      }
+      const double v = sqrt(sum / (double)n_pairs);
+      if (out32) out32[i * n_frames + j] = out32[j * n_frames + i] = (float)v;
+      if (out64) out64[i * n_frames + j] = out64[j * n_frames + i] = v;
+    }
+  }
+  free(d);
   (void)n_threads;
 }
 

@@ -122,3 +122,96 @@ def test_plan_api_known_answers():
     np.testing.assert_allclose(m[0, 1], 0.5, rtol=1e-6)
     half = pairwise_rmsd(traj, system, mask="all", metric="nofit", mat_type="half")
     assert half.shape == (3,)
+
+
+# ---------------------------------------------------------------------------
+# metric "dme" (distance-matrix error): the kernel sums in the reference's
+# order with the reference's roundings, so it is compared bit for bit with the
+# oracle (tolerance 0), and cross-checked for host/device inputs.
+# ---------------------------------------------------------------------------
+
+def gpu_dme(ctx, frames, sel=None, box=None, device_io=False, stride=3):
+    fr = np.ascontiguousarray(frames, np.float32)
+    if stride == 4:
+        fr = np.ascontiguousarray(np.concatenate([fr, np.full(fr.shape[:2] + (1,), 7.0, np.float32)], axis=2))
+    F, n_atoms = fr.shape[0], fr.shape[1]
+    n_sel = n_atoms if sel is None else len(sel)
+    b = None if box is None else np.array(np.broadcast_to(np.asarray(box, np.float32), (F, 3)))
+    if device_io:
+        d = torch.from_numpy(fr).cuda()
+        out = torch.empty(F, F, dtype=torch.float32, device="cuda")
+        ds = None if sel is None else torch.from_numpy(np.asarray(sel, np.int32)).cuda()
+        db = None if b is None else torch.from_numpy(b).cuda()
+        ctx.check(ctx.lib.wmd_pairwise_dme(ctx.handle, d.data_ptr(), F, n_atoms, stride,
+                                           None if ds is None else ds.data_ptr(), n_sel,
+                                           None if db is None else db.data_ptr(), out.data_ptr(), None))
+        torch.cuda.synchronize()
+        return out.cpu().numpy()
+    out = np.empty((F, F), np.float32)
+    s = None if sel is None else np.ascontiguousarray(sel, np.uint32)
+    ctx.check(ctx.lib.wmd_pairwise_dme(ctx.handle, fr.ctypes.data, F, n_atoms, stride, N.ptr(s), n_sel, N.ptr(b),
+                                       out.ctypes.data, None))
+    return out
+
+
+@pytest.mark.parametrize("F,n", [(1, 5), (31, 7), (32, 40), (33, 2), (65, 33), (100, 64)])
+def test_dme_matches_oracle(gpu_ctx, F, n):
+    fr = synth.make_drift_trajectory(n, F, 0.3, seed=F + n)
+    got = gpu_dme(gpu_ctx, fr)
+    want, _ = oracle.pairwise_dme(fr)
+    np.testing.assert_array_equal(got, want)
+    assert (np.diag(got) == 0).all()
+
+
+@pytest.mark.parametrize("device_io", [False, True])
+def test_dme_selection_pbc_and_stride(gpu_ctx, device_io):
+    rng = np.random.default_rng(3)
+    fr = rng.uniform(0, 12, size=(45, 60, 3)).astype(np.float32)  # atoms spread over the box
+    sel = rng.permutation(60)[:37]  # unsorted selection
+    box = np.stack([np.full(45, 12.0), np.full(45, 11.5), np.linspace(10.0, 13.0, 45)], 1).astype(np.float32)
+    for b in (None, box, np.array([12.0, 0.0, 12.0], np.float32)):
+        want, _ = oracle.pairwise_dme(fr[:, sel], box=b)
+        got = gpu_dme(gpu_ctx, fr, sel=sel, box=b, device_io=device_io)
+        np.testing.assert_array_equal(got, want)
+        got4 = gpu_dme(gpu_ctx, fr, sel=sel, box=b, device_io=device_io, stride=4)
+        np.testing.assert_array_equal(got4, want)
+
+
+def test_dme_small_selection_and_metric_code(gpu_ctx):
+    fr = synth.make_drift_trajectory(20, 9, 0.3, seed=5)
+    out = np.full((9, 9), np.nan, np.float32)
+    gpu_ctx.check(gpu_ctx.lib.wmd_pairwise_dme(gpu_ctx.handle, fr.ctypes.data, 9, 20, 3,
+                                               N.ptr(np.array([4], np.uint32)), 1, None, out.ctypes.data, None))
+    assert (out == 0).all()  # n_sel < 2 -> zeros (plan.rs:604-610)
+    # wmd_pairwise_rmsd with metric WMD_PAIR_DME is the same call without a box
+    from warp_md.plans import _PAIR_MODES
+
+    out2 = np.empty((9, 9), np.float32)
+    gpu_ctx.check(gpu_ctx.lib.wmd_pairwise_rmsd(gpu_ctx.handle, fr.ctypes.data, 9, 20, 3, None, 20, N.PAIR_DME,
+                                                _PAIR_MODES["fp64"], out2.ctypes.data, None))
+    np.testing.assert_array_equal(out2, oracle.pairwise_dme(fr)[0])
+
+
+def test_dme_plan_api():
+    coords = np.array([[[0, 0, 0], [1, 0, 0]], [[0, 0, 0], [1, 0, 0]]], np.float32)
+    system = warp_md.System.from_arrays({"name": ["A", "B"], "resid": [1, 2]}, positions0=coords[0])
+    from warp_md.analysis.rmsd import pairwise_rmsd
+
+    # the reference's test_pairwise_rmsd_dme_zero_for_identical (test_pairwise_rmsd.py:64-75)
+    mat = pairwise_rmsd(warp_md.Trajectory.from_numpy(coords), system, mask="all", metric="dme", mat_type="full")
+    assert np.allclose(mat[0, 1], 0.0)
+    fr = synth.make_drift_trajectory(30, 12, 0.5, seed=9)
+    sys30 = warp_md.System.from_arrays({"name": ["CA"] * 30, "resid": list(range(1, 31))}, positions0=fr[0])
+    sel = sys30.select("resid 3:27")
+    idx = np.asarray(sel.indices)
+    box = np.array([40.0, 35.0, 50.0], np.float32)
+    traj = warp_md.Trajectory.from_numpy(fr, box=box)
+    m = warp_md.PairwiseRmsdPlan(sel, metric="dme", pbc="orthorhombic").run(traj, sys30, frame_indices=[0, 5, 11])
+    want, _ = oracle.pairwise_dme(fr[[0, 5, 11]][:, idx], box=box)
+    np.testing.assert_array_equal(m, want)
+    m = warp_md.PairwiseRmsdPlan(sel, metric="dme").run(traj, sys30)
+    np.testing.assert_array_equal(m, oracle.pairwise_dme(fr[:, idx])[0])
+    # length_scale multiplies the matrix (python/warp_md/analysis/rmsd.py:197)
+    half = pairwise_rmsd(traj, sys30, mask="resid 3:27", metric="dme", mat_type="half", length_scale=0.1)
+    full = oracle.pairwise_dme(fr[:, idx])[0] * np.float32(0.1)
+    np.testing.assert_array_equal(half, full[np.triu_indices(12, k=1)])

@@ -84,8 +84,13 @@ def test_plan_input_errors_before_device_work():
         warp_md.RmsdPlan(s.select("all"), reference="topology").run(t6, s)
     with pytest.raises(warp_md.WarpMdError):
         warp_md.RmsdPlan(s.select("all"), reference="frame0").run(t6, s, device="cpu")
-    with pytest.raises(warp_md.WarpMdError, match="dme"):
-        warp_md.PairwiseRmsdPlan(s.select("all"), metric="dme").run(t6, s)
+    # metric "dme" with pbc "orthorhombic" needs per-frame box lengths
+    with pytest.raises(warp_md.WarpMdError, match="orthorhombic box required"):
+        warp_md.PairwiseRmsdPlan(s.select("all"), metric="dme", pbc="orthorhombic").run(t6, s)
+    for bad in (np.ones((3, 3), np.float32), np.ones(4, np.float32), np.ones((5, 3), np.float32)):
+        tb = warp_md.Trajectory.from_numpy(np.zeros((2, 6, 3), np.float32), box=bad)
+        with pytest.raises(RuntimeError, match="box must"):
+            warp_md.PairwiseRmsdPlan(s.select("all"), metric="dme", pbc="orthorhombic").run(tb, s)
 
 
 def test_synth_shapes_and_seeding():

@@ -31,6 +31,7 @@
 #include "device_util.cuh"
 #include "fluct.h"
 #include "pairwise.h"
+#include "pairwise_dme.h"
 #include "superpose.h"
 #include "wmd_internal.h"
 
@@ -1231,8 +1232,9 @@ WMD_EXPORT int wmd_pairwise_rmsd(wmd_ctx* ctx, const float* coords, int64_t n_fr
   if (!ctx) return WMD_ERR_INVALID_ARG;
   if (stride != 3 && stride != 4) return set_err(ctx, WMD_ERR_INVALID_ARG, "stride must be 3 or 4 (got %d)", stride);
   if (n_frames < 0 || n_atoms < 0 || n_sel < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "negative size");
+  if (metric == WMD_PAIR_DME) return wmd_pairwise_dme(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, nullptr, out, stream);
   if (metric != WMD_PAIR_RMS && metric != WMD_PAIR_NOFIT)
-    return set_err(ctx, WMD_ERR_UNSUPPORTED, "pairwise metric %d is not provided (rms=0, nofit=1)", metric);
+    return set_err(ctx, WMD_ERR_UNSUPPORTED, "pairwise metric %d is not provided (rms=0, nofit=1, dme=2)", metric);
   if (mode < WMD_MODE_FP32 || mode > WMD_MODE_FP64)
     return set_err(ctx, WMD_ERR_INVALID_ARG, "unknown pairwise mode %d", mode);
   if (n_frames > 0 && (!coords || !out)) return set_err(ctx, WMD_ERR_INVALID_ARG, "coords/out is null");
@@ -1266,6 +1268,57 @@ WMD_EXPORT int wmd_pairwise_rmsd(wmd_ctx* ctx, const float* coords, int64_t n_fr
   if (prc) return set_err(ctx, prc, "%s", msg.c_str());
   if (is_host(om)) CU(cudaMemcpyAsync(out, dout, out_bytes, cudaMemcpyDeviceToHost, s), "D2H");
   if (is_host(om) || is_host(cm) || (sel && classify(sel) != Mem::Device)) {
+    CU(cudaStreamSynchronize(s), "synchronize");
+    return check_status(ctx);
+  }
+  return WMD_OK;
+}
+
+WMD_EXPORT int wmd_pairwise_dme(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                                const uint32_t* sel, int64_t n_sel, const float* box, float* out, void* stream) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  if (stride != 3 && stride != 4) return set_err(ctx, WMD_ERR_INVALID_ARG, "stride must be 3 or 4 (got %d)", stride);
+  if (n_frames < 0 || n_atoms < 0 || n_sel < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "negative size");
+  if (n_frames > 0 && (!coords || !out)) return set_err(ctx, WMD_ERR_INVALID_ARG, "coords/out is null");
+  if (!sel && n_sel > n_atoms)
+    return set_err(ctx, WMD_ERR_MISMATCH, "selection of %lld atoms exceeds the frame's %lld atoms", (long long)n_sel,
+                   (long long)n_atoms);
+  if ((n_frames + 31) / 32 > 65535) return set_err(ctx, WMD_ERR_UNSUPPORTED, "too many frames for one pairwise call");
+  DeviceGuard g(ctx->device);
+  int rc = check_status(ctx);
+  if (rc) return rc;
+  if (n_frames == 0) return WMD_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const Mem cm = classify(coords), om = classify(out), bm = box ? classify(box) : Mem::Device;
+  const uint32_t* dsel = nullptr;
+  if ((rc = resolve_sel(ctx, sel, n_sel, n_atoms, &dsel, s))) return rc;
+  // host inputs: coordinates, then the box lengths, in the context's staging buffer
+  const size_t cbytes = is_host(cm) ? ((size_t)n_frames * n_atoms * stride * sizeof(float) + 255) / 256 * 256 : 0;
+  const size_t bbytes = box && is_host(bm) ? (size_t)n_frames * 3 * sizeof(float) : 0;
+  if (cbytes + bbytes && (rc = ensure(ctx, ctx->aux, cbytes + bbytes))) return rc;
+  const float* dcoords = coords;
+  if (cbytes) {
+    CU(cudaMemcpyAsync(ctx->aux.ptr, coords, (size_t)n_frames * n_atoms * stride * sizeof(float),
+                       cudaMemcpyHostToDevice, s),
+       "H2D");
+    dcoords = static_cast<const float*>(ctx->aux.ptr);
+  }
+  const float* dbox = box;
+  if (bbytes) {
+    float* bd = reinterpret_cast<float*>(static_cast<char*>(ctx->aux.ptr) + cbytes);
+    CU(cudaMemcpyAsync(bd, box, bbytes, cudaMemcpyHostToDevice, s), "H2D");
+    dbox = bd;
+  }
+  float* dout = out;
+  const size_t out_bytes = (size_t)n_frames * n_frames * sizeof(float);
+  if (is_host(om)) {
+    if ((rc = ensure(ctx, ctx->out_tmp, out_bytes))) return rc;
+    dout = static_cast<float*>(ctx->out_tmp.ptr);
+  }
+  CU(wmd::launch_pair_dme(dcoords, n_frames, n_atoms, stride, dsel, n_sel, dbox, dout, ctx->status_dev, s),
+     "pairwise dme");
+  if (is_host(om)) CU(cudaMemcpyAsync(out, dout, out_bytes, cudaMemcpyDeviceToHost, s), "D2H");
+  if (is_host(om) || is_host(cm) || bbytes || (sel && classify(sel) != Mem::Device)) {
     CU(cudaStreamSynchronize(s), "synchronize");
     return check_status(ctx);
   }

@@ -28,6 +28,7 @@ WMD_ERR_PARSE = -9
 
 PAIR_RMS = 0
 PAIR_NOFIT = 1
+PAIR_DME = 2
 
 MODE_FP32 = 0
 MODE_I8X3 = 1
@@ -39,7 +40,7 @@ FRAME_STATS = 16
 # every symbol include/warpmd_rmsd.h declares
 EXPORTED = (
     "wmd_create", "wmd_destroy", "wmd_last_error", "wmd_version", "wmd_reference_upload", "wmd_reference_free",
-    "wmd_rmsd_frames", "wmd_rmsd_forward", "wmd_rmsd_backward", "wmd_rmsd_covariance", "wmd_pairwise_rmsd",
+    "wmd_rmsd_frames", "wmd_rmsd_forward", "wmd_rmsd_backward", "wmd_rmsd_covariance", "wmd_pairwise_rmsd", "wmd_pairwise_dme",
     "wmd_batched_prepare", "wmd_batched_rmsd", "wmd_batched_layout", "wmd_rmsd_frames_noalloc",
     "wmd_reference_upload_weighted", "wmd_superpose_transforms", "wmd_superpose", "wmd_rmsf", "wmd_rmsd_per_group",
     "wmd_group_ref_upload", "wmd_group_ref_free", "wmd_cluster_dbscan", "wmd_cluster_kmeans", "wmd_dcd_open",
@@ -95,6 +96,7 @@ def load() -> ctypes.CDLL:
         L.wmd_rmsd_backward.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, vp, vp, vp]
         L.wmd_rmsd_covariance.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, vp, vp, vp]
         L.wmd_pairwise_rmsd.argtypes = [vp, vp, i64, i64, i32, vp, i64, i32, i32, vp, vp]
+        L.wmd_pairwise_dme.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, vp]
         L.wmd_batched_prepare.argtypes = [vp, ctypes.POINTER(BatchDesc), i32, i32]
         L.wmd_batched_rmsd.argtypes = [vp, ctypes.POINTER(BatchDesc), i32, i32, vp]
         L.wmd_batched_layout.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32)]

@@ -24,7 +24,7 @@ def pairwise_rmsd(
     device: str = "auto",
     mode: str = "fp64",
 ) -> np.ndarray:
-    """Compute pairwise RMSD matrix (rms, nofit, srmsd)."""
+    """Compute pairwise RMSD matrix (rms, nofit, dme, srmsd)."""
     metric = metric.lower()
     if metric == "srmsd":
         metric = "rms"
@@ -37,11 +37,11 @@ def pairwise_rmsd(
     if pbc not in ("none", "orthorhombic"):
         raise ValueError("pbc must be 'none' or 'orthorhombic'")
     sel = system.select(mask if mask else "all")
-    t = traj
-    if length_scale != 1.0:
-        t = Trajectory.from_numpy(traj.coords * np.float32(length_scale))
     values = PairwiseRmsdPlan(sel, metric=metric, pbc=pbc, mode=mode).run(
-        t, system, chunk_frames=chunk_frames, device=device, frame_indices=frame_indices)
+        traj, system, chunk_frames=chunk_frames, device=device, frame_indices=frame_indices)
+    # the reference scales the matrix, not the coordinates
+    # (python/warp_md/analysis/rmsd.py:197)
+    values = values * np.float32(length_scale)
     if mat_type == "full":
         return values
     if values.size == 0:

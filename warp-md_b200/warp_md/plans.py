@@ -161,6 +161,29 @@ class RmsdPlan:
         return out.astype(dtype, copy=False)
 
 
+def _dme_boxes(traj: Trajectory, n_frames: int, sub: Optional[np.ndarray]) -> np.ndarray:
+    """Per-frame orthorhombic box lengths (n_frames, 3) float32 for metric
+    "dme" with pbc "orthorhombic".  The trajectory's box is (3,) for every
+    frame or (frames, 3), as Trajectory.from_numpy takes it (io.rs:2062-2112);
+    without one the reference stops with box_lengths' mismatch
+    (crates/traj-core/src/pbc_math.rs:11-15)."""
+    b = getattr(traj, "box", None)
+    if b is None:
+        raise N.WarpMdError(N.WMD_ERR_MISMATCH, "mismatch: orthorhombic box required for PBC")
+    a = np.asarray(b, dtype=np.float32)
+    if a.ndim == 1:
+        if a.shape[0] != 3:
+            raise RuntimeError("box must have length 3")
+        return np.ascontiguousarray(np.broadcast_to(a, (n_frames, 3)))
+    if a.ndim != 2 or a.shape[1] != 3:
+        raise RuntimeError("box must have shape (3,) or (frames, 3)")
+    if sub is not None:
+        a = a[sub]
+    if a.shape[0] != n_frames:
+        raise RuntimeError("box must have shape (frames, 3)")
+    return np.ascontiguousarray(a)
+
+
 class PairwiseRmsdPlan:
     """All-pairs frame x frame RMSD matrix (warp_md.PairwiseRmsdPlan).
 
@@ -180,8 +203,6 @@ class PairwiseRmsdPlan:
     def run(self, traj: Trajectory, system: System, chunk_frames: Optional[int] = None, device: str = "auto",
             frame_indices: Optional[Sequence[int]] = None) -> np.ndarray:
         dev = parse_device(device)
-        if self.metric == "dme":
-            raise N.WarpMdError(N.WMD_ERR_UNSUPPORTED, "unsupported: pairwise metric 'dme' is not provided by this build")
         sel = _check_inputs(traj, system, self.selection)
         coords = traj.coords
         sub = frame_subset(coords.shape[0], frame_indices)
@@ -191,9 +212,14 @@ class PairwiseRmsdPlan:
         out = np.zeros((n, n), np.float32)
         if n == 0:
             return np.zeros((0, 0), np.float32)
+        box = _dme_boxes(traj, n, sub) if self.metric == "dme" and self.pbc == "orthorhombic" else None
         ctx = N.context(dev)
         dense = _dense_prefix(sel)
         sel_arr = None if dense else np.ascontiguousarray(sel, dtype=np.uint32)
+        if self.metric == "dme":
+            ctx.check(ctx.lib.wmd_pairwise_dme(ctx.handle, coords.ctypes.data, n, coords.shape[1], 3, N.ptr(sel_arr),
+                                               int(sel.size), N.ptr(box), out.ctypes.data, None))
+            return out
         metric = N.PAIR_RMS if self.metric == "rms" else N.PAIR_NOFIT
         ctx.check(ctx.lib.wmd_pairwise_rmsd(ctx.handle, coords.ctypes.data, n, coords.shape[1], 3, N.ptr(sel_arr),
                                             int(sel.size), metric, _PAIR_MODES[self.mode], out.ctypes.data, None))
