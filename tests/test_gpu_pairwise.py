@@ -136,7 +136,7 @@ def gpu_dme(ctx, frames, sel=None, box=None, device_io=False, stride=3):
         fr = np.ascontiguousarray(np.concatenate([fr, np.full(fr.shape[:2] + (1,), 7.0, np.float32)], axis=2))
     F, n_atoms = fr.shape[0], fr.shape[1]
     n_sel = n_atoms if sel is None else len(sel)
-    b = None if box is None else np.array(np.broadcast_to(np.asarray(box, np.float32), (F, 3)))
+    b = None if box is None else np.array(np.broadcast_to(np.asarray(box, np.float32), (F, 3)), order="C")
     if device_io:
         d = torch.from_numpy(fr).cuda()
         out = torch.empty(F, F, dtype=torch.float32, device="cuda")
