@@ -190,3 +190,35 @@ def test_dcd_rmsd_device_output_and_offsets(tmp_path, gpu_ctx):
         r.close()
     finally:
         ctx.lib.wmd_dcd_close(ctx.handle, h)
+
+
+def test_dcd_boxes_feed_dme_pbc(tmp_path):
+    """A DCD with orthorhombic unit cells exposes per-frame box lengths
+    (Trajectory.box, bit-identical to the oracle reader's), and
+    PairwiseRmsdPlan(metric="dme", pbc="orthorhombic") uses them; a file
+    without cells has no box and the PBC form stops with the reference's
+    mismatch."""
+    import warp_md
+
+    rng = np.random.default_rng(4)
+    n, nf = 40, 19
+    fr = rng.uniform(0, 20, (nf, n, 3)).astype(np.float32)
+    cells = [[20.0 + 0.1 * i, 0.0, 19.0, 0.0, 0.0, 21.0 - 0.05 * i] for i in range(nf)]  # CHARMM: A, cos g, B, cos b, cos a, C
+    p = _write(tmp_path, "cells.dcd", fr, cells=cells, charmm_version=24)
+    coords, kinds, mats = D.read_all(p)
+    assert np.all(np.asarray(kinds) == 1)
+    want_box = np.asarray(mats)[:, [0, 4, 8]]
+    system = _system(n)
+    sel = system.select("name CA")
+    idx = sel.as_array()
+    traj = warp_md.Trajectory.open_dcd(p, system)
+    np.testing.assert_array_equal(traj.box, want_box)
+    got = warp_md.PairwiseRmsdPlan(sel, metric="dme", pbc="orthorhombic").run(traj, system)
+    np.testing.assert_array_equal(got, oracle.pairwise_dme(np.asarray(coords)[:, idx], box=want_box)[0])
+    traj.close()
+    q = _write(tmp_path, "nocells.dcd", fr)
+    traj = warp_md.Trajectory.open_dcd(q, system)
+    assert traj.box is None
+    with pytest.raises(warp_md.WarpMdError, match="orthorhombic box required"):
+        warp_md.PairwiseRmsdPlan(sel, metric="dme", pbc="orthorhombic").run(traj, system)
+    traj.close()

@@ -66,7 +66,7 @@ class DcdTrajectory(Trajectory):
             raise RuntimeError("trajectory atom count does not match system")
         self._cursor = 0
         self._coords: Optional[np.ndarray] = None
-        self.box = None
+        self._box: Optional[np.ndarray] = None
         self.time_ps = None
 
     # -- reference surface -------------------------------------------------
@@ -129,15 +129,19 @@ class DcdTrajectory(Trajectory):
     @property
     def coords(self) -> np.ndarray:
         if self._coords is None:
-            parts, pos = [], 0
+            parts, kinds, mats, pos = [], [], [], 0
             step = max(1, (1 << 30) // max(1, self._n_atoms * 12))
             while True:
-                c, _, _ = self._read(pos, step, None, False)
+                c, k, m = self._read(pos, step, None, True)
                 if c.shape[0] == 0:
                     break
                 parts.append(c)
+                kinds.append(k)
+                mats.append(m)
                 pos += c.shape[0]
             self._coords = np.concatenate(parts) if parts else np.zeros((0, self._n_atoms, 3), np.float32)
+            if parts:
+                self._box, _ = _box_arrays(np.concatenate(kinds), np.concatenate(mats), True, False)
         return self._coords
 
     def read_device(self, first: int, n: int, atom_indices=None, out=None):
@@ -182,6 +186,15 @@ class DcdTrajectory(Trajectory):
             self.close()
         except Exception:
             pass
+
+    @property
+    def box(self) -> Optional[np.ndarray]:
+        """Per-frame orthorhombic box lengths (frames, 3), float32, when every
+        frame carries an orthorhombic unit cell; otherwise None.  Read with
+        ``coords``."""
+        if self._coords is None:
+            self.coords
+        return self._box
 
     # -- internals -----------------------------------------------------------
     def _frames(self) -> int:
