@@ -102,3 +102,18 @@ def test_synth_shapes_and_seeding():
     np.testing.assert_allclose(steps, 3.8, rtol=1e-5)
     d = warp_md.synth.make_drift_trajectory(20, 3, 0.1, seed=1)
     assert d.shape == (3, 20, 3)
+
+
+def test_dme_box_lengths_per_frame():
+    """Box lengths handed to wmd_pairwise_dme: (3,) for every frame, or
+    (frames, 3) subset like the coordinates; always C-contiguous float32."""
+    t = warp_md.Trajectory.from_numpy(np.zeros((4, 6, 3), np.float32), box=np.array([10.0, 11.0, 12.0]))
+    b = plans._dme_boxes(t, 4, None)
+    assert b.shape == (4, 3) and b.dtype == np.float32 and b.flags["C_CONTIGUOUS"]
+    assert (b == np.array([10, 11, 12], np.float32)).all()
+    per = np.arange(12, dtype=np.float64).reshape(4, 3) + 5
+    t = warp_md.Trajectory.from_numpy(np.zeros((4, 6, 3), np.float32), box=per)
+    sub = plans.frame_subset(4, [3, -4])
+    b = plans._dme_boxes(t, 2, sub)
+    np.testing.assert_array_equal(b, per[[3, 0]].astype(np.float32))
+    assert b.flags["C_CONTIGUOUS"]
