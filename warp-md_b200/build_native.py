@@ -8,6 +8,7 @@ with the source tree).  Objects go to warp-md_b200/_build/.
 from __future__ import annotations
 
 import argparse
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -48,15 +49,20 @@ def build(force: bool = False, debug: bool = False, verbose: bool = False) -> st
     if verbose:
         common += ["-Xptxas", "-v"]
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(inc, "warpmd_rmsd.h")]
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES:
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD, src.replace(".cu", ".o"))
         objs.append(obj)
         if force or _stale(obj, [path, *hdrs]):
-            cmd = common + ["-c", path, "-o", obj]
+            cmds.append(common + ["-c", path, "-o", obj])
+    # translation units compile independently: one nvcc per core
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as pool:
+        for cmd in cmds:
             print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+        for cmd, rc in zip(cmds, pool.map(lambda c: subprocess.run(c).returncode, cmds)):
+            if rc != 0:
+                raise subprocess.CalledProcessError(rc, cmd)
     if force or _stale(LIB, objs):
         cmd = [nvcc(), *ARCH, "-shared", "--cudart", "static", "-o", LIB, *objs, "-Xcompiler", "-fvisibility=hidden"]
         print(" ".join(cmd), flush=True)

@@ -15,13 +15,23 @@
 // Host code cannot use the array's name as a device address, so the first
 // call on each device (with that device current) looks the address up with
 // cudaGetSymbolAddress and caches it; make that first call before any stream
-// capture.  All calls on a device share the array and it keeps the last
-// call's contents: calls that may run at the same time on the GPU (different
-// streams, or different host threads) race on it and must be serialised by
-// the caller.
+// capture.  The cached address is not refreshed: after cudaDeviceReset (or
+// anything else that replaces the device's primary context) it is stale, and
+// the library must be reloaded before this entry point is used again on that
+// device.  All calls on a device share the array and it keeps the last call's
+// contents (each call clears what must start at zero): calls that may run at
+// the same time on the GPU (different streams, or different host threads)
+// race on it and must be serialised by the caller.
+//
+// A device-side wait that gives up (the streaming kernel's bounded mbarrier
+// waits, 4 s) cannot be returned as an error code, because the call returns
+// before the GPU runs and reading the status back would need a host
+// synchronisation.  The kernels report it in the output instead: every frame
+// of the affected batch is NaN.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -51,7 +61,7 @@ constexpr size_t kStatusOffset = 132;  // int: device-side status bits
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-void* g_scratch_addr[64] = {};  // per device, set on first use
+std::atomic<void*> g_scratch_addr[64] = {};  // per device, set on first use
 
 // the message is read back with wmd_last_error(NULL)
 int fail(int code, const char* msg) {
@@ -132,6 +142,10 @@ __global__ void __launch_bounds__(256) na_finalize(const double* __restrict__ pa
 #pragma unroll
   for (int e = 0; e < 16; ++e) tot[e] = __shfl_sync(0xffffffffu, s, e);
   if (lane != 0) return;
+  if (*reinterpret_cast<const volatile int*>(scratch + kStatusOffset) != 0) {
+    out[f] = __longlong_as_double(0x7ff8000000000000ll);  // the batch's partials are incomplete
+    return;
+  }
   const double* hdr = reinterpret_cast<const double*>(scratch);
   const double n = (double)n_sel, inv_n = 1.0 / n;
   const double sx[3] = {tot[0], tot[1], tot[2]};
@@ -197,13 +211,16 @@ __global__ void __launch_bounds__(256) na_refine(const float* __restrict__ coord
   }
 }
 
-bool is_device(const void* p) {
+// Device (or managed) memory that the current device can address without
+// peer access: a buffer of another GPU would be an illegal address here.
+bool is_device_here(const void* p, int dev) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
 }  // namespace
@@ -228,27 +245,28 @@ WMD_EXPORT int wmd_rmsd_frames_noalloc(const float* coords, int64_t n_frames, in
   }
   if (n_frames == 0) return WMD_OK;
   if (!coords || !out || (n_sel > 0 && !ref)) return fail(WMD_ERR_INVALID_ARG, "null pointer");
-  if (!is_device(coords) || !is_device(out) || (n_sel > 0 && !is_device(ref)))
-    return fail(WMD_ERR_INVALID_ARG, "coords, ref and out must be device memory");
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   cudaError_t e;
+  int dev = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess || dev < 0 || dev >= 64) return fail(WMD_ERR_CUDA, "no current device");
+  if (!is_device_here(coords, dev) || !is_device_here(out, dev) || (n_sel > 0 && !is_device_here(ref, dev)))
+    return fail(WMD_ERR_INVALID_ARG, "coords, ref and out must be device memory of the current device");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (n_sel == 0) {
     e = cudaMemsetAsync(out, 0, (size_t)n_frames * sizeof(double), s);
     return e == cudaSuccess ? WMD_OK : fail(WMD_ERR_CUDA, cudaGetErrorString(e));
   }
-  int dev = 0;
-  if ((e = cudaGetDevice(&dev)) != cudaSuccess || dev < 0 || dev >= 64) return fail(WMD_ERR_CUDA, "no current device");
   int major = 0, sms = 0;
   cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (major != 10) return fail(WMD_ERR_NO_DEVICE, "current device is not an sm_100 (B200) device");
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    if ((e = cudaGetSymbolAddress(&p, g_noalloc_scratch)) != cudaSuccess || !p)
+  void* addr = g_scratch_addr[dev].load(std::memory_order_acquire);
+  if (!addr) {
+    // every thread that races here looks up the same address
+    if ((e = cudaGetSymbolAddress(&addr, g_noalloc_scratch)) != cudaSuccess || !addr)
       return fail(WMD_ERR_CUDA, e == cudaSuccess ? "scratch address lookup returned null" : cudaGetErrorString(e));
-    g_scratch_addr[dev] = p;
+    g_scratch_addr[dev].store(addr, std::memory_order_release);
   }
-  unsigned char* scratch = static_cast<unsigned char*>(g_scratch_addr[dev]);
+  unsigned char* scratch = static_cast<unsigned char*>(addr);
 
   na_ref_prep<<<1, 256, 0, s>>>(ref, n_sel, ref_stride, scratch);
   if ((e = cudaGetLastError()) != cudaSuccess) return fail(WMD_ERR_CUDA, cudaGetErrorString(e));
@@ -263,19 +281,26 @@ WMD_EXPORT int wmd_rmsd_frames_noalloc(const float* coords, int64_t n_frames, in
   L.ref.n_sel = n_sel;
   L.status = reinterpret_cast<int*>(scratch + kStatusOffset);
   const int tiles = frame_tiles(L);
-  // frames per launch so that partials and refine records fit the work area
+  // Frames per launch so that partials and refine records fit the work area,
+  // a multiple of 4 so that each batch's first frame keeps the 16-byte
+  // alignment of `coords` (4 frames of stride-3 floats are 48 n_atoms bytes).
   const size_t per_frame = (size_t)(tiles + 1) * kStatDoubles * sizeof(double);
-  const int64_t batch = std::max<int64_t>(1, std::min<int64_t>(n_frames, (int64_t)(kWorkBytes / per_frame)));
+  int64_t batch = std::max<int64_t>(1, std::min<int64_t>(n_frames, (int64_t)(kWorkBytes / per_frame)));
+  if (batch < n_frames && batch >= 4) batch &= ~int64_t(3);
   double* partial = reinterpret_cast<double*>(scratch + kWorkOffset);
   double* refine = partial + (size_t)batch * tiles * kStatDoubles;
   for (int64_t f0 = 0; f0 < n_frames; f0 += batch) {
     const int64_t nf = std::min(batch, n_frames - f0);
     FrameLaunch B = L;
     B.coords = coords + (size_t)f0 * n_atoms * stride;
+    // the staged kernel bulk-copies from 16-byte boundaries of its base
+    B.gather = (reinterpret_cast<uintptr_t>(B.coords) & 15u) != 0;
     B.n_frames = nf;
     B.partial = partial;
     B.grid = frame_grid(B, sms, false);
-    if ((e = cudaMemsetAsync(scratch + kCountOffset, 0, sizeof(unsigned), s)) != cudaSuccess)
+    // refine count and status word start at zero for every batch
+    static_assert(kStatusOffset == kCountOffset + sizeof(unsigned), "count and status are adjacent");
+    if ((e = cudaMemsetAsync(scratch + kCountOffset, 0, sizeof(unsigned) + sizeof(int), s)) != cudaSuccess)
       return fail(WMD_ERR_CUDA, cudaGetErrorString(e));
     if ((e = launch_rmsd_stream(B, s)) != cudaSuccess) return fail(WMD_ERR_CUDA, cudaGetErrorString(e));
     na_finalize<<<(unsigned)((nf + 7) / 8), 256, 0, s>>>(partial, tiles, nf, n_sel, scratch, refine, out + f0);

@@ -325,6 +325,23 @@ wmd::FrameLaunch base_launch(wmd_ctx* ctx, const wmd_ref* ref, int64_t n_atoms, 
   return L;
 }
 
+// Frames per batch when at most `fit` fit the scratch: a multiple of 4 when the
+// frames are split, so that every batch starts at the 16-byte alignment of
+// frame 0 (4 frames of float32 atoms are a multiple of 16 bytes).
+int64_t frame_batch(size_t fit, int64_t n_frames) {
+  int64_t b = std::max<int64_t>(1, (int64_t)std::min<size_t>(fit, (size_t)INT64_MAX));
+  if (b >= n_frames) return n_frames;
+  return b >= 4 ? (b & ~int64_t(3)) : b;
+}
+
+// The staged atom-major kernel bulk-copies from 16-byte boundaries of its base:
+// a batch whose first frame is not 16-byte aligned runs the gathered kernel
+// (same tiles, same partials).  The frames-across-lanes kernel needs no check:
+// it only runs when the frame stride is a multiple of 16 bytes.
+void keep_aligned(wmd::FrameLaunch& B) {
+  if (!B.lanes && !B.gather && (reinterpret_cast<uintptr_t>(B.coords) & 15u) != 0) B.gather = true;
+}
+
 // Runs the forward over device-resident frames, splitting into frame batches
 // so the tile-partial scratch stays bounded.  `o` points at frame 0 outputs.
 int forward_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames, int64_t n_atoms, int stride,
@@ -339,8 +356,7 @@ int forward_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames, int64_t
   wmd::frame_plan(L, ctx->sm_count);
   const int tiles = wmd::frame_tiles(L);
   const size_t per_frame = (size_t)tiles * wmd::kStatDoubles * sizeof(double);
-  int64_t batch = std::max<int64_t>(1, (int64_t)(kPartialBytesMax / per_frame));
-  batch = std::min(batch, n_frames);
+  const int64_t batch = frame_batch(kPartialBytesMax / per_frame, n_frames);
   {
     int rc = ensure(ctx, ctx->partial, per_frame * (size_t)batch);
     if (rc) return rc;
@@ -359,6 +375,7 @@ int forward_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames, int64_t
       B.refine_count = static_cast<unsigned*>(ctx->refine_count.ptr);
     }
     B.coords = dcoords + (size_t)f0 * n_atoms * stride;
+    keep_aligned(B);
     B.n_frames = nf;
     B.out.rmsd = o.rmsd ? o.rmsd + f0 : nullptr;
     B.out.stats = o.stats ? o.stats + f0 * wmd::kStatDoubles : nullptr;
@@ -772,7 +789,7 @@ static int superpose_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames
   wmd::frame_plan(L, ctx->sm_count);
   const int tiles = wmd::frame_tiles(L);
   const size_t per_frame = (size_t)std::max(tiles, 1) * wmd::kStatDoubles * sizeof(double);
-  const int64_t batch = std::min<int64_t>(n_frames, std::max<int64_t>(1, (int64_t)(kPartialBytesMax / per_frame)));
+  const int64_t batch = frame_batch(kPartialBytesMax / per_frame, n_frames);
   int rc;
   if ((rc = ensure(ctx, ctx->partial, per_frame * (size_t)batch)) ||
       (rc = ensure(ctx, ctx->rot, (size_t)batch * wmd::kStatDoubles * sizeof(double))))
@@ -781,6 +798,7 @@ static int superpose_device(wmd_ctx* ctx, const float* dcoords, int64_t n_frames
     const int64_t nf = std::min(batch, n_frames - f0);
     wmd::FrameLaunch B = L;
     B.coords = dcoords + (size_t)f0 * n_atoms * stride;
+    keep_aligned(B);
     B.n_frames = nf;
     B.partial = static_cast<double*>(ctx->partial.ptr);
     B.grid = wmd::frame_grid(B, ctx->sm_count, false);
