@@ -772,28 +772,86 @@ def run_dcd(args, ctx, stream, rank):
 
 
 def run_reference(args):
+    """The reference's CPU path for the headline workload: the oracle port of
+    rmsd_aligned_selected (no build of the Rust reference is possible here) on
+    all host threads, statically scheduled so every thread gets an equal run of
+    frames.  One sample of frames is generated once; every step times one pass
+    over it.  The reference path itself is single-threaded, so a 1-thread pass
+    over a smaller sample is reported beside it."""
     ws, rank, _ = _dist()
     if rank != 0:
         return 0
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import oracle
+    from warp_md import synth
+
     threads = os.cpu_count() or 1
     frames = args.ref_frames
+    fr, ref = synth.make_trajectory(N_ATOMS, frames, SIGMA, seed=100)
     vals = []
     for i in range(args.warmup + args.steps):
-        v, _, _ = cpu_baseline(threads, frames, seed=100 + i)
+        t0 = time.perf_counter()
+        oracle.rmsd_frames(fr, ref, threads=threads)
+        dt = time.perf_counter() - t0
         if i >= args.warmup:
-            vals.append(v)
+            vals.append(N_ATOMS * frames / dt)
     value = statistics.median(vals)
+    one = max(2, min(args.ref_frames_single, frames))
+    t0 = time.perf_counter()
+    oracle.rmsd_frames(fr[:one], ref, threads=1)
+    dt_one = time.perf_counter() - t0
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": N_ATOMS * frames / value * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n_atoms": N_ATOMS, "n_frames": N_FRAMES, "sample_frames": frames},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{frames} frames x {N_ATOMS} atoms of the workload per step"},
+                         "sample": (f"the same {frames} frames x {N_ATOMS} atoms of the workload every step, "
+                                    f"OpenMP static schedule over {threads} threads"),
+                         "single_thread": {"value": N_ATOMS * one / dt_one, "frames": one, "seconds": dt_one,
+                                           "note": "the reference's RmsdPlan CPU path runs on one thread"}},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _r(v, digits=4):
+    """Rounds to `digits` significant digits (compact JSON)."""
+    if v is None:
+        return None
+    return float(f"{v:.{digits}g}")
+
+
+def _summary(pairwise, differentiable, batched):
+    """The pairwise (plain vs mixed), differentiable and batched figures in a
+    few hundred characters."""
+    out = {}
+    if pairwise:
+        p = {"metric": "2D-RMSD pairs/s at <=1e-4 A, plain FP32 vs tensor int8 limbs",
+             "frames": pairwise["n_frames"], "atoms": pairwise["n_atoms"], "err_block": "512x512 vs FP64 oracle"}
+        for m in ("fp32", "i8x3", "i8x2"):
+            e = pairwise.get(m)
+            if e:
+                p[m] = {"ms": _r(e["ms"]), "pairs_s": _r(e["value"]), "max_err_A": _r(e["max_err_A"], 2),
+                        "rms_err_A": _r(e["rms_err_A"], 2)}
+                if "roofline" in e:
+                    p[m]["tensor_frac"] = _r(e["roofline"]["frac"], 3)
+        for k in ("speedup_i8x3_vs_fp32", "speedup_i8x2_vs_fp32"):
+            if k in pairwise:
+                p[k] = _r(pairwise[k], 3)
+        out["pairwise"] = p
+    if differentiable:
+        d = differentiable
+        out["differentiable"] = {"ms": _r(d["ms"]), "af_s": _r(d["value"]), "hbm_frac": _r(d["roofline"]["frac"], 3),
+                                 "bytes_per_af": d["roofline"].get("bytes_per_atom_frame", 36)}
+    if batched:
+        b = batched
+        out["batched_uneven"] = {"ms": _r(b["batched"]["ms"]), "af_s": _r(b["batched"]["value"]),
+                                 "hbm_frac": _r(b["roofline"]["frac"], 3),
+                                 "per_traj_ms": _r(b["per_trajectory"]["ms"]),
+                                 "oracle_err_A": _r(b["max_abs_err_vs_oracle_A"], 2)}
+    return out
 
 
 def run_ours(args):
@@ -967,13 +1025,16 @@ def run_ours(args):
             "e2e": e2e,
             "gpu_launches": 3 * args.steps,
             "clocks": clocks,
-            "pairwise": pairwise,
-            "differentiable": differentiable,
-            "batched_uneven": batched,
             "superpose": superpose,
             "fluct": fluct,
             "cluster": cluster,
             "dcd": dcd,
+            "pairwise": pairwise,
+            "differentiable": differentiable,
+            "batched_uneven": batched,
+            # last, so that a reader that keeps only the end of the line still
+            # has the second half of the metric
+            "summary": _summary(pairwise, differentiable, batched),
         }
         print(json.dumps(line), flush=True)
     r.close()
@@ -991,7 +1052,8 @@ def main():
     ap.add_argument("--cpu-frames", type=int, default=10_000)
     ap.add_argument("--cpu-frames-single", type=int, default=1_000)
     ap.add_argument("--n-frames", type=int, default=N_FRAMES, help="frames per GPU (profiling runs only)")
-    ap.add_argument("--ref-frames", type=int, default=48)
+    ap.add_argument("--ref-frames", type=int, default=2000, help="reference arm: frames per timed sample")
+    ap.add_argument("--ref-frames-single", type=int, default=300, help="reference arm: frames of the 1-thread pass")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")

@@ -234,7 +234,7 @@ WMDO_API void wmdo_rmsd_frames(const float* coords, int64_t n_frames, int64_t n_
                                int align, float* out32, double* out64, int n_threads) {
 #ifdef _OPENMP
   int nt = n_threads > 0 ? n_threads : omp_get_max_threads();
-#pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
+#pragma omp parallel for schedule(static) num_threads(nt)
 #endif
   for (int64_t f = 0; f < n_frames; ++f) {
     const float* frame = coords + f * n_atoms * stride;
