@@ -11,23 +11,32 @@ import numpy as np
 MaskLike = Union[str, Sequence[int], np.ndarray]
 
 
-def _all_resid_mask(system) -> str:
-    if not hasattr(system, "atom_table"):
+_WHOLE_SYSTEM = frozenset({"", "*", "all"})
+
+
+def _whole_system_expression(system) -> str:
+    """The expression a blank mask stands for: every residue, written as the
+    closed resid range of the system's atom table (``all`` for a system that
+    has no table, ``resid 0:0`` for an empty one)."""
+    table = system.atom_table() if hasattr(system, "atom_table") else None
+    if table is None:
         return "all"
-    resids = system.atom_table().get("resid", [])
-    if not len(resids):
-        return "resid 0:0"
-    return f"resid {min(resids)}:{max(resids)}"
+    ids = np.asarray(table.get("resid", []), dtype=np.int64).reshape(-1)
+    lo, hi = (int(ids.min()), int(ids.max())) if ids.size else (0, 0)
+    return "resid %d:%d" % (lo, hi)
 
 
-def _select(system, mask: MaskLike):
-    if isinstance(mask, str):
-        expr = mask if mask not in ("", "*", "all", None) else _all_resid_mask(system)
-        return system.select(expr)
-    indices = np.asarray(mask, dtype=np.int64).reshape(-1).tolist()
-    if hasattr(system, "select_indices"):
-        return system.select_indices(indices)
-    raise RuntimeError("system does not support index-based selection (missing select_indices)")
+def _selection_for(system, mask: MaskLike):
+    """A string mask is a selection expression (blank, ``*`` and ``all``
+    mean the whole system, as does None); anything else is a list of atom
+    indices, which the system must accept through ``select_indices``."""
+    if mask is None or isinstance(mask, str):
+        text = "" if mask is None else mask
+        return system.select(_whole_system_expression(system) if text in _WHOLE_SYSTEM else text)
+    by_index = getattr(system, "select_indices", None)
+    if by_index is None:
+        raise RuntimeError("an index mask needs a system with select_indices(); this one has none")
+    return by_index([int(i) for i in np.asarray(mask, dtype=np.int64).ravel()])
 
 
 def cluster_trajectory(traj, system, mask: MaskLike = "", method: str = "dbscan", eps: float = 2.0,
@@ -41,7 +50,7 @@ def cluster_trajectory(traj, system, mask: MaskLike = "", method: str = "dbscan"
         raise ValueError("method must be 'dbscan' or 'kmeans'")
     import warp_md
 
-    plan = warp_md.TrajectoryClusterPlan(_select(system, mask), method=m, eps=float(eps),
+    plan = warp_md.TrajectoryClusterPlan(_selection_for(system, mask), method=m, eps=float(eps),
                                          min_samples=int(min_samples), n_clusters=int(n_clusters),
                                          max_iter=int(max_iter), tol=float(tol), seed=int(seed),
                                          memory_budget_bytes=memory_budget_bytes)

@@ -25,17 +25,15 @@ def pairwise_rmsd(
     mode: str = "fp64",
 ) -> np.ndarray:
     """Compute pairwise RMSD matrix (rms, nofit, dme, srmsd)."""
-    metric = metric.lower()
-    if metric == "srmsd":
-        metric = "rms"
-    if metric not in ("rms", "nofit", "dme"):
-        raise ValueError("metric must be 'rms', 'nofit', 'dme', or 'srmsd'")
-    mat_type = mat_type.lower()
-    if mat_type not in ("full", "half"):
-        raise ValueError("mat_type must be 'full' or 'half'")
-    pbc = pbc.lower()
-    if pbc not in ("none", "orthorhombic"):
-        raise ValueError("pbc must be 'none' or 'orthorhombic'")
+    aliases = {"srmsd": "rms"}
+    metric = aliases.get(metric.lower(), metric.lower())
+    mat_type, pbc = mat_type.lower(), pbc.lower()
+    for name, value, allowed in (("metric", metric, ("rms", "nofit", "dme")),
+                                 ("mat_type", mat_type, ("full", "half")),
+                                 ("pbc", pbc, ("none", "orthorhombic"))):
+        if value not in allowed:
+            extra = " (or the alias 'srmsd')" if name == "metric" else ""
+            raise ValueError(f"unknown {name} {value!r}: expected one of {', '.join(allowed)}{extra}")
     sel = system.select(mask if mask else "all")
     values = PairwiseRmsdPlan(sel, metric=metric, pbc=pbc, mode=mode).run(
         traj, system, chunk_frames=chunk_frames, device=device, frame_indices=frame_indices)

@@ -9,37 +9,43 @@ import numpy as np
 
 
 class ArrayTrajectory:
+    """Frames held in memory behind the chunked reader protocol: a cursor
+    walks the frames, and each ``read_chunk`` hands out the next slice as a
+    dict ("coords" always; "box" and "time" when given), None at the end.
+    Arrays are kept as float32 coordinates and box, float64 times."""
+
     def __init__(self, coords, box: Optional[np.ndarray] = None, time_ps: Optional[np.ndarray] = None):
-        self._coords = np.asarray(coords, dtype=np.float32)
-        if self._coords.ndim != 3 or self._coords.shape[-1] != 3:
-            raise ValueError("coords must be (n_frames, n_atoms, 3)")
-        self._box = None if box is None else np.asarray(box, dtype=np.float32)
-        self._time = None if time_ps is None else np.asarray(time_ps, dtype=np.float64)
-        self._index = 0
+        frames = np.asarray(coords, dtype=np.float32)
+        if frames.ndim != 3 or frames.shape[2] != 3:
+            raise ValueError(f"ArrayTrajectory needs coordinates shaped (frames, atoms, 3); got {frames.shape}")
+        self.frames = frames
+        self.box_values = None if box is None else np.asarray(box, dtype=np.float32)
+        self.time_values = None if time_ps is None else np.asarray(time_ps, dtype=np.float64)
+        self.cursor = 0
 
     @property
     def coords(self) -> np.ndarray:
-        return self._coords
-
-    def reset(self):
-        self._index = 0
-
-    def n_atoms(self) -> int:
-        return int(self._coords.shape[1])
+        return self.frames
 
     def n_frames(self) -> int:
-        return int(self._coords.shape[0])
+        return self.frames.shape[0]
+
+    def n_atoms(self) -> int:
+        return self.frames.shape[1]
+
+    def reset(self):
+        self.cursor = 0
 
     def read_chunk(self, max_frames: int = 128):
-        if self._index >= self._coords.shape[0]:
+        lo = self.cursor
+        if lo >= self.n_frames():
             return None
-        end = min(self._index + max(1, int(max_frames)), self._coords.shape[0])
-        chunk = {"coords": self._coords[self._index:end]}
-        if self._box is not None:
-            chunk["box"] = self._box[self._index:end]
-        if self._time is not None:
-            chunk["time"] = self._time[self._index:end]
-        self._index = end
+        hi = min(self.n_frames(), lo + max(int(max_frames), 1))
+        self.cursor = hi
+        chunk = {"coords": self.frames[lo:hi]}
+        for key, values in (("box", self.box_values), ("time", self.time_values)):
+            if values is not None:
+                chunk[key] = values[lo:hi]
         return chunk
 
 
@@ -50,8 +56,10 @@ def read_all_frames(traj, chunk_frames: Optional[int] = None):
     box or None, time or None)."""
     if hasattr(traj, "coords") and not callable(getattr(traj, "coords")):
         coords = np.asarray(traj.coords, dtype=np.float32)
-        box = getattr(traj, "box", None) if not isinstance(traj, ArrayTrajectory) else traj._box
-        time = getattr(traj, "time_ps", None) if not isinstance(traj, ArrayTrajectory) else traj._time
+        if isinstance(traj, ArrayTrajectory):
+            return coords, traj.box_values, traj.time_values
+        box = getattr(traj, "box", None)
+        time = getattr(traj, "time_ps", None)
         return coords, box, time
     if hasattr(traj, "reset"):
         traj.reset()
