@@ -85,6 +85,18 @@ const char* wmd_version(void);
 int wmd_reference_upload(wmd_ctx* ctx, const float* ref, int64_t n_sel, int stride, wmd_ref** out);
 int wmd_reference_free(wmd_ctx* ctx, wmd_ref* ref);
 
+/* Error-path diagnostics (no counterpart in the reference, whose CUDA failures
+ * surface as TrajError::Unsupported, crates/traj-gpu/src/cuda.rs:384-390).
+ * Every device-side wait of this library is bounded: a wait that runs out
+ * stops the kernel, lets its copies in flight land, and the call (or the next
+ * call on the context) returns WMD_ERR_TIMEOUT.  For the per-frame streaming
+ * forward kernels and the tensor-core pairwise kernel launched on `ctx` from
+ * now on, the consumers' waits give up after wait_limit_ns (0 restores the
+ * default of 4 s), and withhold_first_stage != 0 leaves the first pipeline
+ * stage of their first CTA unfilled, so that its wait must run out.  For tests
+ * of that path; the results of such calls are not valid. */
+int wmd_set_wait_test(wmd_ctx* ctx, uint64_t wait_limit_ns, int withhold_first_stage);
+
 /* Per-frame RMSD of n_frames frames against `ref` (RmsdPlan, plan.rs:323-404
  * and rmsd_aligned_selected plan.rs:1161-1248 when align != 0; rmsd_raw_selected
  * plan.rs:1093-1110 when align == 0).
@@ -129,6 +141,19 @@ int wmd_rmsd_covariance(wmd_ctx* ctx, const float* coords, int64_t n_frames, int
  * without a box). */
 int wmd_pairwise_rmsd(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
                       const uint32_t* sel, int64_t n_sel, int metric, int mode, float* out, void* stream);
+
+/* One part of the all-pairs matrix for a computation split over `parts` GPUs
+ * (the tile partition of PairwiseRmsdPlan::finalize's i < j loop,
+ * plan.rs:593-674, which the reference runs as one loop).  Every caller holds
+ * all frames; part `part` computes the pairs i < j whose tile row (40 frames
+ * in the tensor-core modes, 32 in the SIMT modes) is part (mod parts), writes
+ * each at (i, j) and (j, i), and leaves every other entry 0.  The parts for
+ * part = 0..parts-1 are disjoint and their sum is wmd_pairwise_rmsd's matrix
+ * exactly (the tensor-core modes quantise every frame with the same
+ * trajectory-wide scale in every part).  WMD_PAIR_DME only with parts = 1. */
+int wmd_pairwise_rmsd_part(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                           const uint32_t* sel, int64_t n_sel, int metric, int mode, int part, int parts,
+                           float* out, void* stream);
 
 /* All-pairs distance-matrix error (PairwiseRmsdPlan metric "dme",
  * plan.rs:612-645 with pair_distances_compact, plan.rs:1279-1302): per frame the

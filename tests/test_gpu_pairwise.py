@@ -248,3 +248,37 @@ def test_i8x3_full_all_pairs_workload_blocks_against_oracle():
     assert bool(torch.equal(blk, blk.t()))
     del out, d
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_parts_are_disjoint_and_sum_to_the_full_matrix(mode):
+    """wmd_pairwise_rmsd_part: the tile-row partition of the i < j loop
+    (plan.rs:593-674) that the multi-GPU assembly sums.  For 2, 3 and 7 parts,
+    no entry is written by two parts and the sum of the parts is the
+    single-call matrix bit for bit."""
+    from warp_md.plans import _PAIR_MODES
+
+    ctx = N.context(0)
+    if not _supported(ctx, mode):
+        pytest.skip(f"{mode} not supported on this device")
+    d = synth.make_drift_trajectory(120, 300, 0.1, seed=31)
+    x = torch.from_numpy(d).cuda()
+    F = d.shape[0]
+    full = torch.empty(F, F, dtype=torch.float32, device="cuda")
+    ctx.check(ctx.lib.wmd_pairwise_rmsd(ctx.handle, x.data_ptr(), F, 120, 3, None, 120, N.PAIR_RMS,
+                                        _PAIR_MODES[mode], full.data_ptr(), None))
+    for parts in (2, 3, 7):
+        total = torch.zeros_like(full)
+        written = torch.zeros(F, F, dtype=torch.int32, device="cuda")
+        for part in range(parts):
+            out = torch.full((F, F), -1.0, dtype=torch.float32, device="cuda")
+            ctx.check(ctx.lib.wmd_pairwise_rmsd_part(ctx.handle, x.data_ptr(), F, 120, 3, None, 120, N.PAIR_RMS,
+                                                     _PAIR_MODES[mode], part, parts, out.data_ptr(), None))
+            total += out
+            written += (out != 0).int()
+        torch.cuda.synchronize()
+        assert int(written.max().item()) == 1
+        assert bool(torch.equal(total, full)), (mode, parts)
+    bad = ctx.lib.wmd_pairwise_rmsd_part(ctx.handle, x.data_ptr(), F, 120, 3, None, 120, N.PAIR_RMS,
+                                         _PAIR_MODES[mode], 3, 3, full.data_ptr(), None)
+    assert bad == N.WMD_ERR_INVALID_ARG

@@ -11,6 +11,18 @@ namespace wmd {
 // through the context's status word instead of spinning forever.
 constexpr uint64_t kWaitLimitNs = 4000000000ull;
 
+// Limits of a launch's bounded device waits.  limit_ns replaces the default
+// for the waits of a pipeline's consumers (exit-time drains of copies in
+// flight keep kWaitLimitNs).  withhold != 0 is the error path's test: the
+// producer serving the first consumer of CTA 0 arms nothing and copies
+// nothing for its first stage, so that wait can only run out.  The kernels
+// that honour it are the per-frame streaming forward kernels and the
+// tensor-core pairwise kernel.
+struct WaitCfg {
+  uint64_t limit_ns = kWaitLimitNs;
+  int withhold = 0;
+};
+
 enum DeviceStatus : int {
   kStatusOk = 0,
   kStatusTimeoutFull = 1,   // consumer waited too long for a copy to land
@@ -63,21 +75,34 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Waits for the phase with the given parity to complete.  Returns false (and
-// records `code` in *status) when kWaitLimitNs passes first, or when *abort
-// (a CTA-shared flag) is raised by another thread of the block.
+// records `code` in *status) when limit_ns passes first, or when *abort (a
+// CTA-shared flag) is raised by another thread of the block.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status, int code,
-                                          volatile int* abort) {
+                                          volatile int* abort, uint64_t limit_ns = kWaitLimitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_timer_ns();
   for (uint32_t it = 1;; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((it & 63u) == 0) {
       if (*abort) return false;
-      if (global_timer_ns() - t0 > kWaitLimitNs) {
+      if (global_timer_ns() - t0 > limit_ns) {
         if (status) atomicOr(status, code);
         *abort = 1;
         return false;
       }
+    }
+  }
+}
+
+// Exit-time wait for a stage's copies to land (phase `parity` of `bar`):
+// a CTA must not exit while copies into its shared memory are in flight.
+// Gives up after kWaitLimitNs, recording kStatusTimeoutDrain.
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t parity, int* status) {
+  const uint64_t t0 = global_timer_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (global_timer_ns() - t0 > kWaitLimitNs) {
+      if (status) atomicOr(status, kStatusTimeoutDrain);
+      return;
     }
   }
 }

@@ -130,13 +130,14 @@ struct Pair2 { T x, y; };
 template <typename T>
 __global__ void __launch_bounds__(256) pair_tile_simt(const T* __restrict__ xc, const double* __restrict__ gsum,
                                                       const double* __restrict__ cen, int64_t F, int64_t n_pad,
-                                                      double n, int metric, float* __restrict__ out) {
+                                                      double n, int metric, float* __restrict__ out, int part,
+                                                      int parts) {
   constexpr int kStep = kPairKc * kPanelRows;  // elements per panel K step
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* As = reinterpret_cast<T*>(smem_raw);      // [2][kPairKc][96]
   T* Bs = As + 2 * kStep;
   const int bi = blockIdx.y, bj = blockIdx.x;
-  if (bi > bj) return;
+  if (bi > bj || bi % parts != part) return;
   const int64_t I0 = (int64_t)bi * kPanelFrames, J0 = (int64_t)bj * kPanelFrames;
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   const T* pa = xc + (size_t)bi * n_pad * kPanelRows;
@@ -245,7 +246,8 @@ static cudaError_t run_simt(PairwiseWorkspace& w, int64_t F, int64_t n_pad, int6
   if (e != cudaSuccess) return e;
   const unsigned nb = (unsigned)((F + kPanelFrames - 1) / kPanelFrames);
   dim3 grid(nb, nb);
-  kern<<<grid, 256, smem, s>>>(static_cast<const T*>(w.centred), w.gsum, w.cen, F, n_pad, (double)n_sel, metric, out);
+  kern<<<grid, 256, smem, s>>>(static_cast<const T*>(w.centred), w.gsum, w.cen, F, n_pad, (double)n_sel, metric, out,
+                               w.part, w.parts);
   return cudaGetLastError();
 }
 
@@ -262,7 +264,7 @@ int pairwise_run(PairwiseWorkspace& w, int sm_count, const float* coords, int64_
 
   if (mode == WMD_MODE_I8X3 || mode == WMD_MODE_I8X2)
     return pairwise_tc_run(w, sm_count, coords, n_frames, n_atoms, stride, sel, n_sel, metric,
-                           mode == WMD_MODE_I8X3 ? 3 : 2, out, status, s, msg);
+                           mode == WMD_MODE_I8X3 ? 3 : 2, out, status, w.wait, s, msg);
 
   const bool f64 = mode == WMD_MODE_FP64;
   const int64_t n_pad = (n_sel + kPairKc - 1) / kPairKc * kPairKc;

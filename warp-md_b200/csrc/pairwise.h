@@ -6,6 +6,8 @@
 #include <cstdint>
 #include <string>
 
+#include "device_util.cuh"
+
 namespace wmd {
 
 struct PairwiseWorkspace {
@@ -16,6 +18,11 @@ struct PairwiseWorkspace {
   size_t frames_cap = 0;
   void* extra = nullptr;    // mode-specific scratch
   size_t extra_bytes = 0;
+  WaitCfg wait;             // limits of the tensor-core kernel's bounded waits
+  // Partition of the upper triangle over `parts` callers (one per GPU): a
+  // launch computes only the tiles whose tile row is part (mod parts), and
+  // leaves every other entry zero, so the parts sum to the whole matrix.
+  int part = 0, parts = 1;
 };
 
 void pairwise_workspace_free(PairwiseWorkspace& w);

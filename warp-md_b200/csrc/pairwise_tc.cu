@@ -151,16 +151,19 @@ constexpr uint32_t kIdesc = (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(kTile
 
 // bounded wait on an mbarrier phase (no shared abort fallback needed by
 // callers other than through the flag)
-__device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t parity, int* status, volatile int* abort) {
-  return mbar_wait(bar, parity, status, kStatusTimeoutFull, abort);
+__device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t parity, int* status, volatile int* abort,
+                                        uint64_t limit_ns) {
+  return mbar_wait(bar, parity, status, kStatusTimeoutFull, abort, limit_ns);
 }
 
 struct TileList {
   int ni, nj;  // I blocks (40 frames) x J blocks (30 frames)
   int64_t F;
+  int part, parts;  // this launch computes the I blocks bi = part (mod parts)
   __device__ __forceinline__ bool valid(int64_t t, int& bi, int& bj) const {
     bi = (int)(t / nj);
     bj = (int)(t - (int64_t)bi * nj);
+    if (bi % parts != part) return false;
     const int64_t i0 = (int64_t)bi * kTileFramesM;
     const int64_t jmax = min((int64_t)(bj + 1) * kTileFramesN, F) - 1;
     return i0 < jmax && (int64_t)bj * kTileFramesN < F;  // some pair i < j in the tile
@@ -177,6 +180,7 @@ struct TcArgs {
   const double* scale; // device scalar s
   float* out;          // [F][F]
   int* status;
+  WaitCfg wait;
 };
 
 // -------------------------------------------------------------- kernel --
@@ -221,6 +225,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (warp == 0) {
     // ---------------- TMA producer ----------------
     if (lane == 0) {
+      // under the error-path test CTA 0's first stage is never armed
+      const bool withheld = args.wait.withhold && blockIdx.x == 0;
       uint32_t it = 0;
       bool ok = true;
       for (int64_t t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
@@ -229,13 +235,20 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         for (int kc = 0; kc < n_k; ++kc, ++it) {
           const int s = it % kStagesTc;
           const uint32_t ph = (it / kStagesTc) & 1u;
-          if (!tc_wait(&empty[s], ph ^ 1u, args.status, abort_flag)) { ok = false; break; }
+          if (!tc_wait(&empty[s], ph ^ 1u, args.status, abort_flag, args.wait.limit_ns)) { ok = false; break; }
+          if (withheld && it == 0) continue;
           unsigned char* st = smem + s * G::kStageBytes;
           mbar_arrive_expect_tx(&full[s], G::kStageBytes);
           tma_load_3d(st, &map_a, kc * kKChunk, bi * kTileM, 0, &full[s]);
           tma_load_3d(st + G::kABytes, &map_b, kc * kKChunk, bj * kTileN, 0, &full[s]);
         }
       }
+      // When the MMAs stopped early (a wait ran out), stages loaded for them
+      // may still be landing; every load must complete before the CTA exits.
+      // In a complete run the MMAs consumed every stage and these return at once.
+      const uint32_t first = it > (uint32_t)kStagesTc ? it - (uint32_t)kStagesTc : 0u;
+      for (uint32_t j = first; j < it; ++j)
+        if (!(withheld && j == 0)) mbar_drain(&full[j % kStagesTc], (j / kStagesTc) & 1u, args.status);
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
@@ -246,12 +259,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         int bi, bj;
         if (!tiles.valid(t, bi, bj)) continue;
         // the epilogue must have drained the previous tile's accumulators
-        if (!tc_wait(tmem_empty, (tc & 1u) ^ 1u, args.status, abort_flag)) { ok = false; break; }
+        if (!tc_wait(tmem_empty, (tc & 1u) ^ 1u, args.status, abort_flag, args.wait.limit_ns)) { ok = false; break; }
         tc_fence_after();
         for (int kc = 0; kc < n_k; ++kc, ++it) {
           const int s = it % kStagesTc;
           const uint32_t ph = (it / kStagesTc) & 1u;
-          if (!tc_wait(&full[s], ph, args.status, abort_flag)) { ok = false; break; }
+          if (!tc_wait(&full[s], ph, args.status, abort_flag, args.wait.limit_ns)) { ok = false; break; }
           tc_fence_after();
           const unsigned char* st = smem + s * G::kStageBytes;
 #pragma unroll
@@ -305,7 +318,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       int bi, bj;
       if (!tiles.valid(t, bi, bj)) continue;
       if (drainer) {
-        if (tc_wait(tmem_full, tc & 1u, args.status, abort_flag)) {
+        if (tc_wait(tmem_full, tc & 1u, args.status, abort_flag, args.wait.limit_ns)) {
           tc_fence_after();
           double* epi = reinterpret_cast<double*>(smem + G::kEpiOffset + wq * kEpiWarpBytes);
 #pragma unroll
@@ -522,8 +535,8 @@ EncodeTiled encode_fn(std::string* msg) {
 
 template <int LIMBS>
 int run_tc(PairwiseWorkspace& w, int sm_count, const float* coords, int64_t F, int64_t n_atoms, int stride,
-           const uint32_t* sel, int64_t n_sel, int metric, float* out, int* status, cudaStream_t s,
-           std::string* msg) {
+           const uint32_t* sel, int64_t n_sel, int metric, float* out, int* status, const WaitCfg& wait,
+           cudaStream_t s, std::string* msg) {
   using G = TcGeo<LIMBS>;
   const int64_t n_pad = (n_sel + kKChunk - 1) / kKChunk * kKChunk;
   const int64_t rows = (F + kFramesPerQuarter - 1) / kFramesPerQuarter * 32;
@@ -595,10 +608,13 @@ int run_tc(PairwiseWorkspace& w, int sm_count, const float* coords, int64_t F, i
   a.scale = scale;
   a.out = out;
   a.status = status;
+  a.wait = wait;
   TileList tl;
   tl.ni = (int)((F + kTileFramesM - 1) / kTileFramesM);
   tl.nj = (int)((F + kTileFramesN - 1) / kTileFramesN);
   tl.F = F;
+  tl.part = w.part;
+  tl.parts = w.parts;
   auto kern = pair_tc_kernel<LIMBS>;
   if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::kSmemBytes)) != cudaSuccess) {
     *msg = std::string("cuda driver error: ") + cudaGetErrorString(e);
@@ -618,7 +634,7 @@ int run_tc(PairwiseWorkspace& w, int sm_count, const float* coords, int64_t F, i
 
 int pairwise_tc_run(PairwiseWorkspace& w, int sm_count, const float* coords, int64_t n_frames, int64_t n_atoms,
                     int stride, const uint32_t* sel, int64_t n_sel, int metric, int limbs, float* out, int* status,
-                    cudaStream_t s, std::string* msg) {
+                    const WaitCfg& wait, cudaStream_t s, std::string* msg) {
   // exact int32 accumulation: LIMBS n_pad 128^2 < 2^31
   const int64_t max_atoms = limbs == 3 ? 43648 : 65472;
   if (n_sel > max_atoms) {
@@ -630,8 +646,9 @@ int pairwise_tc_run(PairwiseWorkspace& w, int sm_count, const float* coords, int
     *msg = "too many frames for one pairwise call";
     return WMD_ERR_INVALID_ARG;
   }
-  return limbs == 3 ? run_tc<3>(w, sm_count, coords, n_frames, n_atoms, stride, sel, n_sel, metric, out, status, s, msg)
-                    : run_tc<2>(w, sm_count, coords, n_frames, n_atoms, stride, sel, n_sel, metric, out, status, s, msg);
+  return limbs == 3
+             ? run_tc<3>(w, sm_count, coords, n_frames, n_atoms, stride, sel, n_sel, metric, out, status, wait, s, msg)
+             : run_tc<2>(w, sm_count, coords, n_frames, n_atoms, stride, sel, n_sel, metric, out, status, wait, s, msg);
 }
 
 }  // namespace wmd

@@ -198,13 +198,16 @@ __global__ void __launch_bounds__(kThreads, 3) rmsd_frames_kernel(const FrameLau
   }
   __syncthreads();
 
-  // producer cursor (thread 0 only)
+  // producer cursor (thread 0 only).  Under the error-path test the first
+  // stage of CTA 0 is never armed (WaitCfg::withhold).
   int tp = (int)(w0 / F);
   int64_t fp = w0 - (int64_t)tp * F;
   int64_t issued = 0;
+  const bool withheld = L.wait.withhold && blockIdx.x == 0;
   if (!GATHER && tid == 0) {
     for (; issued < S - 1 && issued < n_items; ++issued) {
-      issue_item<STRIDE, T>(L, tp, fp, smem + (issued % S) * G::kStageBytes, &full[issued % S], total_al);
+      if (!(withheld && issued == 0))
+        issue_item<STRIDE, T>(L, tp, fp, smem + (issued % S) * G::kStageBytes, &full[issued % S], total_al);
       if (++fp == F) { fp = 0; ++tp; }
     }
   }
@@ -220,7 +223,7 @@ __global__ void __launch_bounds__(kThreads, 3) rmsd_frames_kernel(const FrameLau
   for (int64_t i = 0; i < n_items; ++i) {
     if (!GATHER && tid == 0 && issued < n_items) {
       const int sp = (int)(issued % S);
-      issue_item<STRIDE, T>(L, tp, fp, smem + sp * G::kStageBytes, &full[sp], total_al);
+      if (!(withheld && issued == 0)) issue_item<STRIDE, T>(L, tp, fp, smem + sp * G::kStageBytes, &full[sp], total_al);
       ++issued;
       if (++fp == F) { fp = 0; ++tp; }
     }
@@ -253,7 +256,7 @@ __global__ void __launch_bounds__(kThreads, 3) rmsd_frames_kernel(const FrameLau
     const float* xs = nullptr;
     bool ok = true;
     if (!GATHER) {
-      ok = mbar_wait(&full[s], phase, L.status, kStatusTimeoutFull, abort_flag);
+      ok = mbar_wait(&full[s], phase, L.status, kStatusTimeoutFull, abort_flag, L.wait.limit_ns);
       xs = reinterpret_cast<const float*>(smem + s * G::kStageBytes) +
            (int)(((uint64_t)(f * L.n_atoms + a0) * STRIDE) & 3ull);
     }
@@ -378,20 +381,12 @@ __global__ void __launch_bounds__(kThreads, 3) rmsd_frames_kernel(const FrameLau
     if (++f == F) { f = 0; ++t; }
   }
 
-  // every copy this CTA issued must land before the CTA may exit
+  // every copy this CTA issued must land before the CTA may exit (a withheld
+  // stage has none)
   if (!GATHER && tid == 0) {
     const int64_t first = issued > S ? issued - S : 0;
-    for (int64_t j = first; j < issued; ++j) {
-      const int st = (int)(j % S);
-      const uint32_t ph = (uint32_t)((j / S) & 1);
-      const uint64_t t0 = global_timer_ns();
-      while (!mbar_try_wait(&full[st], ph)) {
-        if (global_timer_ns() - t0 > kWaitLimitNs) {
-          atomicOr(L.status, kStatusTimeoutDrain);
-          break;
-        }
-      }
-    }
+    for (int64_t j = first; j < issued; ++j)
+      if (!(withheld && j == 0)) mbar_drain(&full[j % S], (uint32_t)((j / S) & 1), L.status);
   }
 }
 

@@ -168,19 +168,23 @@ __global__ void __launch_bounds__(kLaneWarps * 32) rmsd_lanes_kernel(const __gri
   int64_t pu = u0;
   int pk = 0, p_kst = unit_stages(u0);
   int64_t n_issued = 0;
+  // under the error-path test the first stage of CTA 0's warp 0 is never armed
+  const bool withheld = L.wait.withhold && blockIdx.x == 0 && warp == 0;
   auto issue_next = [&]() {  // lane 0
     const int64_t t = pu / groups, g = pu - t * groups;
     const int slot = (int)(n_issued % kLaneStages);
     unsigned char* dst = ring + slot * G::kStageBytes;
     const int64_t a0 = t * tile + (int64_t)pk * kLaneAtoms;
-    // the warp's earlier generic reads of this slot before the async writes
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_arrive_expect_tx(&full[slot], G::kXBytes + G::kYBytes + (W ? G::kWBytes : 0));
+    if (!(withheld && n_issued == 0)) {
+      // the warp's earlier generic reads of this slot before the async writes
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive_expect_tx(&full[slot], G::kXBytes + G::kYBytes + (W ? G::kWBytes : 0));
 #pragma unroll
-    for (int b = 0; b < G::kBoxes; ++b)
-      tma_load_2d(dst + b * 4096, &map, (int)(a0 * STRIDE + 32 * b), (int)(g * 32), &full[slot]);
-    bulk_copy_g2s(dst + G::kXBytes, L.lane_y + a0 * 3, G::kYBytes, &full[slot]);
-    if (W) bulk_copy_g2s(dst + G::kXBytes + G::kYBytes, L.lane_w + a0, G::kWBytes, &full[slot]);
+      for (int b = 0; b < G::kBoxes; ++b)
+        tma_load_2d(dst + b * 4096, &map, (int)(a0 * STRIDE + 32 * b), (int)(g * 32), &full[slot]);
+      bulk_copy_g2s(dst + G::kXBytes, L.lane_y + a0 * 3, G::kYBytes, &full[slot]);
+      if (W) bulk_copy_g2s(dst + G::kXBytes + G::kYBytes, L.lane_w + a0, G::kWBytes, &full[slot]);
+    }
     ++n_issued;
     if (++pk == p_kst && ++pu < u1) {
       pk = 0;
@@ -201,7 +205,7 @@ __global__ void __launch_bounds__(kLaneWarps * 32) rmsd_lanes_kernel(const __gri
     for (int k = 0; k < kst; ++k) {
       const int slot = (int)(n_done % kLaneStages);
       const uint32_t parity = (uint32_t)((n_done / kLaneStages) & 1);
-      if (!mbar_wait(&full[slot], parity, L.status, kStatusTimeoutFull, abort_flag)) {
+      if (!mbar_wait(&full[slot], parity, L.status, kStatusTimeoutFull, abort_flag, L.wait.limit_ns)) {
         aborted = true;
         break;
       }
@@ -226,19 +230,11 @@ __global__ void __launch_bounds__(kLaneWarps * 32) rmsd_lanes_kernel(const __gri
     }
   }
 
-  // after an abort, copies this warp issued may still be landing
+  // after an abort, copies this warp issued may still be landing (a withheld
+  // stage has none)
   if (aborted && lane == 0) {
-    for (int64_t j = n_done; j < n_issued; ++j) {
-      const int slot = (int)(j % kLaneStages);
-      const uint32_t ph = (uint32_t)((j / kLaneStages) & 1);
-      const uint64_t t0 = global_timer_ns();
-      while (!mbar_try_wait(&full[slot], ph)) {
-        if (global_timer_ns() - t0 > kWaitLimitNs) {
-          atomicOr(L.status, kStatusTimeoutDrain);
-          break;
-        }
-      }
-    }
+    for (int64_t j = n_done; j < n_issued; ++j)
+      if (!(withheld && j == 0)) mbar_drain(&full[j % kLaneStages], (uint32_t)((j / kLaneStages) & 1), L.status);
   }
 }
 

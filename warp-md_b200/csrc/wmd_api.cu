@@ -96,6 +96,7 @@ struct wmd_ctx {
   cudaEvent_t kern_done[2] = {nullptr, nullptr};
   int* status_host = nullptr;  // mapped pinned word the kernels report into
   int* status_dev = nullptr;
+  wmd::WaitCfg wait;           // bounded-wait limits (wmd_set_wait_test)
   DevBuf partial, refine, refine_count, rot, chunk[2], out_tmp, sel_buf, aux, out_chunk;
   DevBuf fl_part, fl_acc, fl_shift;
   DevBuf cl_mat, cl_scratch, cl_out, km_feat, km_xf, km_work;  // clustering  // fluctuations, per-group RMSD
@@ -321,6 +322,7 @@ wmd::FrameLaunch base_launch(wmd_ctx* ctx, const wmd_ref* ref, int64_t n_atoms, 
   L.ref = ref->info;
   L.ref.yc = ref->yc;
   L.status = ctx->status_dev;
+  L.wait = ctx->wait;
   L.tile_atoms = wmd::kConsumerThreads * 8;
   return L;
 }
@@ -650,6 +652,14 @@ WMD_EXPORT int wmd_reference_free(wmd_ctx* ctx, wmd_ref* ref) {
     if (ref->w) cudaFree(ref->w);
   }
   delete ref;
+  return WMD_OK;
+}
+
+WMD_EXPORT int wmd_set_wait_test(wmd_ctx* ctx, uint64_t wait_limit_ns, int withhold_first_stage) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  ctx->wait.limit_ns = wait_limit_ns ? wait_limit_ns : wmd::kWaitLimitNs;
+  ctx->wait.withhold = withhold_first_stage ? 1 : 0;
+  ctx->pw.wait = ctx->wait;
   return WMD_OK;
 }
 
@@ -1245,8 +1255,29 @@ WMD_EXPORT int wmd_rmsd_backward(wmd_ctx* ctx, const float* coords, int64_t n_fr
   return WMD_OK;
 }
 
+static int pairwise_common(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                           const uint32_t* sel, int64_t n_sel, int metric, int mode, int part, int parts, float* out,
+                           void* stream);
+
 WMD_EXPORT int wmd_pairwise_rmsd(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
                                  const uint32_t* sel, int64_t n_sel, int metric, int mode, float* out, void* stream) {
+  return pairwise_common(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, metric, mode, 0, 1, out, stream);
+}
+
+WMD_EXPORT int wmd_pairwise_rmsd_part(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms,
+                                      int stride, const uint32_t* sel, int64_t n_sel, int metric, int mode, int part,
+                                      int parts, float* out, void* stream) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  if (parts < 1 || part < 0 || part >= parts)
+    return set_err(ctx, WMD_ERR_INVALID_ARG, "part %d of %d: need 0 <= part < parts", part, parts);
+  if (metric == WMD_PAIR_DME && parts > 1)
+    return set_err(ctx, WMD_ERR_UNSUPPORTED, "the dme metric is not partitioned (call with parts = 1)");
+  return pairwise_common(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, metric, mode, part, parts, out, stream);
+}
+
+static int pairwise_common(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                           const uint32_t* sel, int64_t n_sel, int metric, int mode, int part, int parts, float* out,
+                           void* stream) {
   if (!ctx) return WMD_ERR_INVALID_ARG;
   if (stride != 3 && stride != 4) return set_err(ctx, WMD_ERR_INVALID_ARG, "stride must be 3 or 4 (got %d)", stride);
   if (n_frames < 0 || n_atoms < 0 || n_sel < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "negative size");
@@ -1281,8 +1312,12 @@ WMD_EXPORT int wmd_pairwise_rmsd(wmd_ctx* ctx, const float* coords, int64_t n_fr
     dout = static_cast<float*>(ctx->out_tmp.ptr);
   }
   std::string msg;
+  ctx->pw.part = part;
+  ctx->pw.parts = parts;
   const int prc = wmd::pairwise_run(ctx->pw, ctx->sm_count, dcoords, n_frames, n_atoms, stride, dsel, n_sel, metric,
                                     mode, dout, ctx->status_dev, s, &msg);
+  ctx->pw.part = 0;
+  ctx->pw.parts = 1;
   if (prc) return set_err(ctx, prc, "%s", msg.c_str());
   if (is_host(om)) CU(cudaMemcpyAsync(out, dout, out_bytes, cudaMemcpyDeviceToHost, s), "D2H");
   if (is_host(om) || is_host(cm) || (sel && classify(sel) != Mem::Device)) {

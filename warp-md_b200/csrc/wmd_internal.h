@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "device_util.cuh"
+
 namespace wmd {
 
 // Per-frame kernel geometry: 4 warps per CTA (thread 0 also issues the bulk
@@ -60,6 +62,7 @@ struct FrameLaunch {
   double* refine = nullptr;     // [n_frames][16] records of frames needing the residual pass
   unsigned* refine_count = nullptr;  // number of records, zeroed before each forward
   int* status = nullptr;        // device-visible status word (mapped host)
+  WaitCfg wait;                 // limits of the bounded waits
   int grid = 0;                 // CTAs (persistent)
 };
 

@@ -41,7 +41,8 @@ FRAME_STATS = 16
 EXPORTED = (
     "wmd_create", "wmd_destroy", "wmd_last_error", "wmd_version", "wmd_reference_upload", "wmd_reference_free",
     "wmd_rmsd_frames", "wmd_rmsd_forward", "wmd_rmsd_backward", "wmd_rmsd_covariance", "wmd_pairwise_rmsd", "wmd_pairwise_dme",
-    "wmd_batched_prepare", "wmd_batched_rmsd", "wmd_batched_layout", "wmd_rmsd_frames_noalloc",
+    "wmd_batched_prepare", "wmd_batched_rmsd", "wmd_batched_layout", "wmd_rmsd_frames_noalloc", "wmd_set_wait_test",
+    "wmd_pairwise_rmsd_part",
     "wmd_reference_upload_weighted", "wmd_superpose_transforms", "wmd_superpose", "wmd_rmsf", "wmd_rmsd_per_group",
     "wmd_group_ref_upload", "wmd_group_ref_free", "wmd_cluster_dbscan", "wmd_cluster_kmeans", "wmd_dcd_open",
     "wmd_dcd_close", "wmd_dcd_info", "wmd_dcd_read", "wmd_dcd_rmsd",
@@ -91,11 +92,13 @@ def load() -> ctypes.CDLL:
         L.wmd_version.restype = ctypes.c_char_p
         L.wmd_reference_upload.argtypes = [vp, vp, i64, i32, ctypes.POINTER(vp)]
         L.wmd_reference_free.argtypes = [vp, vp]
+        L.wmd_set_wait_test.argtypes = [vp, ctypes.c_uint64, i32]
         L.wmd_rmsd_frames.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, i32, vp, vp]
         L.wmd_rmsd_forward.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, vp, vp]
         L.wmd_rmsd_backward.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, vp, vp, vp]
         L.wmd_rmsd_covariance.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, vp, vp, vp]
         L.wmd_pairwise_rmsd.argtypes = [vp, vp, i64, i64, i32, vp, i64, i32, i32, vp, vp]
+        L.wmd_pairwise_rmsd_part.argtypes = [vp, vp, i64, i64, i32, vp, i64, i32, i32, i32, i32, vp, vp]
         L.wmd_pairwise_dme.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, vp]
         L.wmd_batched_prepare.argtypes = [vp, ctypes.POINTER(BatchDesc), i32, i32]
         L.wmd_batched_rmsd.argtypes = [vp, ctypes.POINTER(BatchDesc), i32, i32, vp]
