@@ -238,13 +238,16 @@ def _l2_flush_buffer():
 
 def run_differentiable(args, stream, rank):
     """Differentiable RMSD: 4,096 frames x 2,000 atoms (98 MB, smaller than
-    L2), forward + hand-written backward through torch.autograd.  L2 is
-    flushed (256 MB write) before every timed step; only the step is timed."""
+    L2), forward + hand-written backward.  Three forms of the step, each timed
+    with L2 flushed (256 MB write) before it: torch.autograd eagerly, the same
+    autograd step replayed from a CUDA graph, and rmsd_value_and_grad (value
+    and gradient in one launch).  Algorithmic bytes: x read once and the
+    gradient written once, 24 B per atom-frame, + 8 B per frame."""
     import numpy as np
     import torch
 
     from warp_md import synth
-    from warp_md.torch_ops import rmsd
+    from warp_md.torch_ops import rmsd, rmsd_value_and_grad
 
     F, n = 4096, 2000
     x, ref = synth.make_trajectory_torch(n, F, 0.3, seed=17 + rank, device="cuda")
@@ -257,32 +260,78 @@ def run_differentiable(args, stream, rank):
         v.sum().backward()
         return v
 
+    def timed(fn, reps):
+        times = []
+        for _ in range(reps):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        return statistics.median(times)
+
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
-    times = []
-    for _ in range(args.diff_steps):
-        flush.fill_(1)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        step()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        times.append(e0.elapsed_time(e1))
-    ms = statistics.median(times)
-    peak, _ = _measured_peaks()
-    alg = 36.0 * n * F + 8.0 * F  # forward read, backward read + write (float32 xyz), rmsd out
-    g = x.grad
-    ok = bool(torch.isfinite(g).all().item())
-    del x, g, flush
+    ms_eager = timed(step, args.diff_steps)
+    g_autograd = x.grad.detach().clone()
+
+    # the same autograd step captured once and replayed
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(3):
+            step()
+    torch.cuda.current_stream().wait_stream(side)
+    x.grad = None
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        v = rmsd(x, ref)
+        v.sum().backward()
+    for _ in range(3):
+        graph.replay()
+    torch.cuda.synchronize()
+    ms_graph = timed(graph.replay, args.diff_steps)
+    graph_diff = float((x.grad - g_autograd).abs().max().item())
+
+    xd = x.detach()
+    for _ in range(3):
+        rmsd_value_and_grad(xd, ref)
+    torch.cuda.synchronize()
+    ms_vg = timed(lambda: rmsd_value_and_grad(xd, ref), args.diff_steps)
+    val_vg, g_vg = rmsd_value_and_grad(xd, ref)
+    vg_diff = float((g_vg - g_autograd).abs().max().item())
+    # oracle check on 16 frames: RMSD and analytic FP64 gradient
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import oracle
+
+    idx = torch.arange(0, F, F // 16, device="cuda")
+    rm, go = oracle.rmsd_grad(xd.index_select(0, idx).cpu().numpy(), ref.cpu().numpy())
+    rerr = float(np.abs(val_vg.index_select(0, idx).cpu().numpy() - rm).max())
+    gerr = float(np.abs(g_vg.index_select(0, idx).cpu().numpy() - go).max() / np.abs(go).max())
+    ok = bool(torch.isfinite(g_vg).all().item())
+    del graph, v, x, g_vg, g_autograd, xd, flush
     torch.cuda.empty_cache()
+    peak, _ = _measured_peaks()
+    alg = 24.0 * n * F + 8.0 * F
+
+    def entry(ms, how):
+        return {"ms": ms, "value": n * F / (ms / 1e3), "how": how,
+                "roofline": {"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                             "frac": alg / (ms / 1e3) / 1e9 / peak, "bytes_per_atom_frame": 24}}
+
+    eager = entry(ms_eager, "torch.autograd: rmsd(x, ref).sum().backward(), eager")
+    graphed = entry(ms_graph, "the same autograd step replayed from a CUDA graph")
+    fused = entry(ms_vg, "rmsd_value_and_grad: value and gradient in one launch")
     return {"metric": "RMSD forward+backward atom-frames/s", "unit": "atom-frames/s", "n_frames": F, "n_atoms": n,
-            "value": n * F / (ms / 1e3), "ms": ms, "l2": "flushed before each step (256 MB write)",
-            "roofline": {"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                         "frac": alg / (ms / 1e3) / 1e9 / peak,
-                         "note": "36 B/atom-frame over forward+backward incl. autograd overhead"},
-            "finite": ok}
+            "value": fused["value"], "ms": ms_vg, "l2": "flushed before each step (256 MB write)",
+            "roofline": fused["roofline"], "autograd_eager": eager, "autograd_graph": graphed,
+            "value_and_grad": fused,
+            "max_abs_diff_grad_graph_vs_eager": graph_diff, "max_abs_diff_grad_fused_vs_autograd": vg_diff,
+            "oracle_16_frames": {"max_abs_err_rmsd_A": rerr, "max_rel_err_grad": gerr}, "finite": ok}
 
 
 def run_batched(args, ctx, stream, rank):
@@ -843,8 +892,12 @@ def _summary(pairwise, differentiable, batched):
         out["pairwise"] = p
     if differentiable:
         d = differentiable
-        out["differentiable"] = {"ms": _r(d["ms"]), "af_s": _r(d["value"]), "hbm_frac": _r(d["roofline"]["frac"], 3),
-                                 "bytes_per_af": d["roofline"].get("bytes_per_atom_frame", 36)}
+        out["differentiable"] = {
+            "bytes_per_af": 24,
+            "value_and_grad": {"ms": _r(d["value_and_grad"]["ms"]), "hbm_frac": _r(d["value_and_grad"]["roofline"]["frac"], 3)},
+            "autograd_graph": {"ms": _r(d["autograd_graph"]["ms"]), "hbm_frac": _r(d["autograd_graph"]["roofline"]["frac"], 3)},
+            "autograd_eager": {"ms": _r(d["autograd_eager"]["ms"]), "hbm_frac": _r(d["autograd_eager"]["roofline"]["frac"], 3)},
+            "oracle_err": [_r(d["oracle_16_frames"]["max_abs_err_rmsd_A"], 2), _r(d["oracle_16_frames"]["max_rel_err_grad"], 2)]}
     if batched:
         b = batched
         out["batched_uneven"] = {"ms": _r(b["batched"]["ms"]), "af_s": _r(b["batched"]["value"]),

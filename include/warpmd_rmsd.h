@@ -125,6 +125,25 @@ int wmd_rmsd_backward(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64
                       const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, const double* stats,
                       const float* grad_rmsd, float* grad, void* stream);
 
+/* wmd_rmsd_backward with the per-frame weights dL/drmsd as doubles at
+ * grad_rmsd[f * grad_stride] (grad_stride 0: one weight for every frame, as a
+ * broadcast tensor has), or all 1 when grad_rmsd is NULL.  Device pointers. */
+int wmd_rmsd_backward_f64(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                          const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, const double* stats,
+                          const double* grad_rmsd, int64_t grad_stride, float* grad, void* stream);
+
+/* Per-frame aligned RMSD and the gradient of L = sum_f w_f rmsd_f in one call
+ * (no counterpart in the reference, which has no derivative): rmsd[f] as
+ * wmd_rmsd_forward (NULL to skip), grad as wmd_rmsd_backward with weights
+ * w_f = weights[f * weight_stride] (NULL: all 1).  For a dense selection of
+ * packed xyz frames (n_atoms % 4 == 0, at most 16,384 atoms, at least 16
+ * frames per SM) one launch reads every frame from DRAM once and writes its
+ * gradient: 24 bytes per atom-frame; other shapes run the forward and the
+ * backward.  Device pointers only. */
+int wmd_rmsd_value_and_grad(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                            const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, const double* weights,
+                            int64_t weight_stride, double* rmsd, float* grad, void* stream);
+
 /* Shape drop-in for GpuContext::rmsd_covariance
  * (crates/traj-gpu/src/cuda/runtime_core.rs:375-472): per frame the 3x3
  * covariance cov[f*9 + 3*a + b] = sum (x_a - cx_a)(y_b - cy_b) and the centred

@@ -79,3 +79,51 @@ def test_tensor_core_pairwise_wait_runs_out_and_context_recovers():
     rc, after = run()
     assert rc == N.WMD_OK, ctx.lib.wmd_last_error(ctx.handle)
     assert np.array_equal(before, after)
+
+
+@pytest.mark.parametrize("entry", ["forward", "backward", "value_and_grad"])
+def test_whole_frame_kernel_wait_runs_out_and_context_recovers(entry):
+    """The whole-frame kernels (many small frames: wmd_rmsd_forward,
+    wmd_rmsd_backward_f64, wmd_rmsd_value_and_grad) take device outputs and
+    return before the GPU runs, so the timeout surfaces at the next call on
+    the context, which reports it and clears it."""
+    ctx = N.context(0)
+    F, n = 2400, 600
+    fr, ref = synth.make_trajectory(n, F, 0.5, seed=73)
+    x = torch.from_numpy(fr).cuda()
+    r = N.Reference.from_numpy(ctx, (ref + 0.1).astype(np.float32))
+    out = torch.empty(F, dtype=torch.float64, device="cuda")
+    stats = torch.empty(F, N.FRAME_STATS, dtype=torch.float64, device="cuda")
+    grad = torch.empty_like(x)
+    ones = torch.ones(F, dtype=torch.float64, device="cuda")
+
+    def call():
+        if entry == "forward":
+            return ctx.lib.wmd_rmsd_forward(ctx.handle, x.data_ptr(), F, n, 3, None, n, r.handle, out.data_ptr(),
+                                            stats.data_ptr(), None)
+        if entry == "backward":
+            return ctx.lib.wmd_rmsd_backward_f64(ctx.handle, x.data_ptr(), F, n, 3, None, n, r.handle,
+                                                 stats.data_ptr(), ones.data_ptr(), 1, grad.data_ptr(), None)
+        return ctx.lib.wmd_rmsd_value_and_grad(ctx.handle, x.data_ptr(), F, n, 3, None, n, r.handle, None, 0,
+                                               out.data_ptr(), grad.data_ptr(), None)
+
+    try:
+        ctx.check(ctx.lib.wmd_rmsd_forward(ctx.handle, x.data_ptr(), F, n, 3, None, n, r.handle, out.data_ptr(),
+                                           stats.data_ptr(), None))
+        assert call() == N.WMD_OK
+        torch.cuda.synchronize()
+        before = (out.clone(), stats.clone(), grad.clone())
+        ctx.check(ctx.lib.wmd_set_wait_test(ctx.handle, LIMIT_NS, 1))
+        try:
+            assert call() == N.WMD_OK  # launched; the GPU has not run it yet
+            torch.cuda.synchronize()
+        finally:
+            ctx.check(ctx.lib.wmd_set_wait_test(ctx.handle, 0, 0))
+        assert call() == N.WMD_ERR_TIMEOUT
+        assert call() == N.WMD_OK
+        torch.cuda.synchronize()
+        after = (out, stats, grad)
+        for a, b in zip(before, after):
+            assert torch.equal(a, b)
+    finally:
+        r.close()

@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 OUT_DIR = os.path.join(HERE, "warp_md", "_native")
 LIB = os.path.join(OUT_DIR, "libwarpmd_rmsd.so")
-SOURCES = ["wmd_api.cu", "rmsd_frames.cu", "rmsd_lanes.cu", "pairwise.cu", "pairwise_tc.cu", "pairwise_dme.cu", "noalloc.cu", "batched.cu", "superpose.cu", "fluct.cu", "cluster.cu", "dcd.cu"]
+SOURCES = ["wmd_api.cu", "rmsd_frames.cu", "rmsd_lanes.cu", "rmsd_vg.cu", "pairwise.cu", "pairwise_tc.cu", "pairwise_dme.cu", "noalloc.cu", "batched.cu", "superpose.cu", "fluct.cu", "cluster.cu", "dcd.cu"]
 HEADERS = ["device_util.cuh", "qcp.cuh", "wmd_internal.h", "pairwise.h", "pairwise_tc.h", "pairwise_dme.h", "batched.h", "superpose.h", "fluct.h", "cluster.h", "dcd.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

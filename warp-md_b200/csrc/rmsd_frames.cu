@@ -393,7 +393,8 @@ __global__ void __launch_bounds__(kThreads, 3) rmsd_frames_kernel(const FrameLau
 // Backward prologue: per frame, the rotation from the QCP eigenvector of the
 // stored H, the centroid and the scale dL/drmsd / (n rmsd).
 __global__ void rmsd_bwd_prologue(const double* __restrict__ stats, const float* __restrict__ grad_rmsd,
-                                  int64_t n_frames, double* __restrict__ rot) {
+                                  const double* __restrict__ grad_f64, int64_t grad_stride, int64_t n_frames,
+                                  double* __restrict__ rot) {
   const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= n_frames) return;
   const double* st = stats + f * kStatDoubles;
@@ -401,7 +402,7 @@ __global__ void rmsd_bwd_prologue(const double* __restrict__ stats, const float*
   for (int e = 0; e < 9; ++e) h[e] = st[3 + e];
   rotation_from_qcp(h, st[12], r);
   const double rmsd = st[13], n = st[14];
-  const double g = grad_rmsd ? (double)grad_rmsd[f] : 1.0;
+  const double g = grad_f64 ? grad_f64[f * grad_stride] : grad_rmsd ? (double)grad_rmsd[f] : 1.0;
   const double scale = (rmsd > 0.0 && n > 0.0) ? g / (n * rmsd) : 0.0;
   double* o = rot + f * kStatDoubles;
   for (int e = 0; e < 9; ++e) o[e] = r[e];
@@ -709,11 +710,11 @@ cudaError_t launch_rmsd_stream_weighted(const FrameLaunch& L, cudaStream_t s) {
 }
 
 cudaError_t launch_rmsd_backward(const FrameLaunch& L, const double* stats, const float* grad_rmsd,
-                                 double* rot_scratch, cudaStream_t s) {
+                                 const double* grad_f64, int64_t grad_stride, double* rot_scratch, cudaStream_t s) {
   if (L.n_frames == 0) return cudaSuccess;
   const int threads = 128;
   const int blocks = (int)((L.n_frames + threads - 1) / threads);
-  rmsd_bwd_prologue<<<blocks, threads, 0, s>>>(stats, grad_rmsd, L.n_frames, rot_scratch);
+  rmsd_bwd_prologue<<<blocks, threads, 0, s>>>(stats, grad_rmsd, grad_f64, grad_stride, L.n_frames, rot_scratch);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   FrameLaunch B = L;

@@ -99,6 +99,7 @@ struct wmd_ctx {
   wmd::WaitCfg wait;           // bounded-wait limits (wmd_set_wait_test)
   DevBuf partial, refine, refine_count, rot, chunk[2], out_tmp, sel_buf, aux, out_chunk;
   DevBuf fl_part, fl_acc, fl_shift;
+  DevBuf vg_stats;  // frame records of wmd_rmsd_value_and_grad's two-kernel route
   DevBuf cl_mat, cl_scratch, cl_out, km_feat, km_xf, km_work;  // clustering  // fluctuations, per-group RMSD
   // a sorted host selection expanded onto its atom span for the
   // frames-across-lanes kernel, valid for the current call
@@ -327,6 +328,18 @@ wmd::FrameLaunch base_launch(wmd_ctx* ctx, const wmd_ref* ref, int64_t n_atoms, 
   return L;
 }
 
+wmd::VgLaunch vg_launch(wmd_ctx* ctx, const wmd_ref* ref, const float* coords, int64_t n_frames, int64_t n_atoms) {
+  wmd::VgLaunch V;
+  V.coords = coords;
+  V.n_frames = n_frames;
+  V.n_atoms = n_atoms;
+  V.ref = ref->info;
+  V.ref.yc = ref->yc;
+  V.status = ctx->status_dev;
+  V.wait = ctx->wait;
+  return V;
+}
+
 // Frames per batch when at most `fit` fit the scratch: a multiple of 4 when the
 // frames are split, so that every batch starts at the 16-byte alignment of
 // frame 0 (4 frames of float32 atoms are a multiple of 16 bytes).
@@ -502,7 +515,7 @@ WMD_EXPORT int wmd_destroy(wmd_ctx* ctx) {
   cudaDeviceSynchronize();
   for (DevBuf* b : {&ctx->partial, &ctx->refine, &ctx->refine_count, &ctx->rot, &ctx->chunk[0], &ctx->chunk[1], &ctx->out_tmp,
                     &ctx->sel_buf, &ctx->aux, &ctx->out_chunk, &ctx->fl_part, &ctx->fl_acc, &ctx->fl_shift, &ctx->cl_mat, &ctx->cl_scratch,
-                    &ctx->cl_out, &ctx->km_feat, &ctx->km_xf, &ctx->km_work, &ctx->lane_exp, &ctx->b_segs, &ctx->b_yc, &ctx->b_partial, &ctx->b_rot,
+                    &ctx->cl_out, &ctx->km_feat, &ctx->km_xf, &ctx->km_work, &ctx->lane_exp, &ctx->vg_stats, &ctx->b_segs, &ctx->b_yc, &ctx->b_partial, &ctx->b_rot,
                     &ctx->b_refine, &ctx->b_count})
     if (b->ptr) cudaFree(b->ptr);
   for (HostBuf* b : {&ctx->stage[0], &ctx->stage[1]})
@@ -1223,27 +1236,35 @@ WMD_EXPORT int wmd_rmsd_forward(wmd_ctx* ctx, const float* coords, int64_t n_fra
     if (stats) CU(cudaMemsetAsync(stats, 0, (size_t)n_frames * wmd::kStatDoubles * 8, s), "memset");
     return WMD_OK;
   }
+  if (!sel && wmd::vg_usable(coords, nullptr, n_frames, n_atoms, stride, ctx->sm_count)) {
+    wmd::VgLaunch V = vg_launch(ctx, ref, coords, n_frames, n_atoms);
+    V.rmsd = out;
+    V.stats = stats;
+    CU(wmd::launch_vg(wmd::kVgFwd, V, ctx->sm_count, s), "rmsd forward launch");
+    return WMD_OK;
+  }
   wmd::FrameOutputs o;
   o.rmsd = out;
   o.stats = stats;
   return forward_device(ctx, coords, n_frames, n_atoms, stride, sel, ref, 1, o, s);
 }
 
-WMD_EXPORT int wmd_rmsd_backward(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
-                                 const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, const double* stats,
-                                 const float* grad_rmsd, float* grad, void* stream) {
-  int rc = check_common(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, ref);
-  if (rc) return rc;
-  DeviceGuard g(ctx->device);
-  if ((rc = check_status(ctx))) return rc;
-  if (n_frames == 0 || n_sel == 0) return WMD_OK;
-  if (!stats || !grad) return set_err(ctx, WMD_ERR_INVALID_ARG, "stats and grad are required");
-  if ((rc = require_device(ctx, coords, "coords")) || (rc = require_device(ctx, sel, "sel")) ||
-      (rc = require_device(ctx, stats, "stats")) || (rc = require_device(ctx, grad_rmsd, "grad_rmsd")) ||
-      (rc = require_device(ctx, grad, "grad")))
-    return rc;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  rc = ensure(ctx, ctx->rot, (size_t)n_frames * wmd::kStatDoubles * sizeof(double));
+// Gradient from the forward's records; per-frame weights as float (gf) or
+// double with a stride (gd), or all 1.
+static int backward_common(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                           const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, const double* stats,
+                           const float* gf, const double* gd, int64_t gstride, float* grad, cudaStream_t s) {
+  if (!sel && wmd::vg_usable(coords, grad, n_frames, n_atoms, stride, ctx->sm_count)) {
+    wmd::VgLaunch V = vg_launch(ctx, ref, coords, n_frames, n_atoms);
+    V.stats = const_cast<double*>(stats);
+    V.w = gd ? static_cast<const void*>(gd) : static_cast<const void*>(gf);
+    V.w_f64 = gd != nullptr;
+    V.w_stride = gd ? gstride : 1;
+    V.grad = grad;
+    CU(wmd::launch_vg(wmd::kVgBwd, V, ctx->sm_count, s), "rmsd backward launch");
+    return WMD_OK;
+  }
+  int rc = ensure(ctx, ctx->rot, (size_t)n_frames * wmd::kStatDoubles * sizeof(double));
   if (rc) return rc;
   wmd::FrameLaunch L = base_launch(ctx, ref, n_atoms, stride, sel);
   L.coords = coords;
@@ -1251,8 +1272,95 @@ WMD_EXPORT int wmd_rmsd_backward(wmd_ctx* ctx, const float* coords, int64_t n_fr
   L.gather = sel != nullptr || (reinterpret_cast<uintptr_t>(coords) & 15u) != 0;
   L.grad = grad;
   L.grid = wmd::frame_grid(L, ctx->sm_count, true);
-  CU(wmd::launch_rmsd_backward(L, stats, grad_rmsd, static_cast<double*>(ctx->rot.ptr), s), "rmsd backward launch");
+  CU(wmd::launch_rmsd_backward(L, stats, gf, gd, gstride, static_cast<double*>(ctx->rot.ptr), s),
+     "rmsd backward launch");
   return WMD_OK;
+}
+
+static int backward_checks(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                           const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, const double* stats,
+                           const void* weights, float* grad) {
+  int rc = check_common(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, ref);
+  if (rc) return rc;
+  if (n_frames > 0 && n_sel > 0 && (!stats || !grad))
+    return set_err(ctx, WMD_ERR_INVALID_ARG, "stats and grad are required");
+  if ((rc = require_device(ctx, coords, "coords")) || (rc = require_device(ctx, sel, "sel")) ||
+      (rc = require_device(ctx, stats, "stats")) || (rc = require_device(ctx, weights, "grad_rmsd")) ||
+      (rc = require_device(ctx, grad, "grad")))
+    return rc;
+  return WMD_OK;
+}
+
+WMD_EXPORT int wmd_rmsd_backward(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,
+                                 const uint32_t* sel, int64_t n_sel, const wmd_ref* ref, const double* stats,
+                                 const float* grad_rmsd, float* grad, void* stream) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  DeviceGuard g(ctx->device);
+  int rc = check_status(ctx);
+  if (rc) return rc;
+  if ((rc = backward_checks(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, ref, stats, grad_rmsd, grad)))
+    return rc;
+  if (n_frames == 0 || n_sel == 0) return WMD_OK;
+  return backward_common(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, ref, stats, grad_rmsd, nullptr, 0, grad,
+                         static_cast<cudaStream_t>(stream));
+}
+
+WMD_EXPORT int wmd_rmsd_backward_f64(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms,
+                                     int stride, const uint32_t* sel, int64_t n_sel, const wmd_ref* ref,
+                                     const double* stats, const double* grad_rmsd, int64_t grad_stride, float* grad,
+                                     void* stream) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  if (grad_stride < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "grad_stride must be >= 0");
+  DeviceGuard g(ctx->device);
+  int rc = check_status(ctx);
+  if (rc) return rc;
+  if ((rc = backward_checks(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, ref, stats, grad_rmsd, grad)))
+    return rc;
+  if (n_frames == 0 || n_sel == 0) return WMD_OK;
+  return backward_common(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, ref, stats, nullptr, grad_rmsd,
+                         grad_stride, grad, static_cast<cudaStream_t>(stream));
+}
+
+WMD_EXPORT int wmd_rmsd_value_and_grad(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms,
+                                       int stride, const uint32_t* sel, int64_t n_sel, const wmd_ref* ref,
+                                       const double* weights, int64_t weight_stride, double* rmsd, float* grad,
+                                       void* stream) {
+  if (!ctx) return WMD_ERR_INVALID_ARG;
+  if (weight_stride < 0) return set_err(ctx, WMD_ERR_INVALID_ARG, "weight_stride must be >= 0");
+  int rc = check_common(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, ref);
+  if (rc) return rc;
+  DeviceGuard g(ctx->device);
+  if ((rc = check_status(ctx))) return rc;
+  if (n_frames == 0) return WMD_OK;
+  if (!grad) return set_err(ctx, WMD_ERR_INVALID_ARG, "grad is required");
+  if ((rc = require_device(ctx, coords, "coords")) || (rc = require_device(ctx, sel, "sel")) ||
+      (rc = require_device(ctx, weights, "weights")) || (rc = require_device(ctx, rmsd, "rmsd")) ||
+      (rc = require_device(ctx, grad, "grad")))
+    return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (n_sel == 0) {
+    if (rmsd) CU(cudaMemsetAsync(rmsd, 0, (size_t)n_frames * 8, s), "memset");
+    return WMD_OK;
+  }
+  if (!sel && wmd::vg_usable(coords, grad, n_frames, n_atoms, stride, ctx->sm_count)) {
+    wmd::VgLaunch V = vg_launch(ctx, ref, coords, n_frames, n_atoms);
+    V.rmsd = rmsd;
+    V.w = weights;
+    V.w_f64 = 1;
+    V.w_stride = weight_stride;
+    V.grad = grad;
+    CU(wmd::launch_vg(wmd::kVgBoth, V, ctx->sm_count, s), "rmsd value and gradient launch");
+    return WMD_OK;
+  }
+  // any other shape: the forward into context scratch, then the backward
+  if ((rc = ensure(ctx, ctx->vg_stats, (size_t)n_frames * wmd::kStatDoubles * sizeof(double)))) return rc;
+  double* st = static_cast<double*>(ctx->vg_stats.ptr);
+  wmd::FrameOutputs o;
+  o.rmsd = rmsd;
+  o.stats = st;
+  if ((rc = forward_device(ctx, coords, n_frames, n_atoms, stride, sel, ref, 1, o, s))) return rc;
+  return backward_common(ctx, coords, n_frames, n_atoms, stride, sel, n_sel, ref, st, nullptr, weights,
+                         weights ? weight_stride : 0, grad, s);
 }
 
 static int pairwise_common(wmd_ctx* ctx, const float* coords, int64_t n_frames, int64_t n_atoms, int stride,

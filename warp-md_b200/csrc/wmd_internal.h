@@ -101,9 +101,33 @@ cudaError_t launch_rmsd_stream(const FrameLaunch& L, cudaStream_t s);
 // Only the streaming kernel, weighted statistics: per tile sum w x (3),
 // sum w x_a^2 (3) and sum x (w y_c)^T (9) into L.partial (needs L.ref.w).
 cudaError_t launch_rmsd_stream_weighted(const FrameLaunch& L, cudaStream_t s);
+// Per-frame dL/drmsd: grad_f64[f * grad_stride] when grad_f64 is set, else
+// grad_rmsd[f], else 1.
 cudaError_t launch_rmsd_backward(const FrameLaunch& L, const double* stats, const float* grad_rmsd,
-                                 double* rot_scratch, cudaStream_t s);
+                                 const double* grad_f64, int64_t grad_stride, double* rot_scratch, cudaStream_t s);
 // occupancy-derived persistent grid for a launch
 int frame_grid(const FrameLaunch& L, int sm_count, bool backward);
+
+// Whole-frame kernels for many frames of up to kVgMaxAtoms atoms
+// (rmsd_vg.cu): forward (rmsd and the 16-double records of
+// wmd_rmsd_forward), backward (gradient from those records) and both in one
+// launch.  Dense selections of packed xyz only.
+constexpr int64_t kVgMaxAtoms = 16384;
+enum VgMode : int { kVgFwd = 0, kVgBwd = 1, kVgBoth = 2 };
+struct VgLaunch {
+  const float* coords = nullptr;  // device [n_frames][n_atoms][3], 16-byte aligned
+  int64_t n_frames = 0, n_atoms = 0;
+  RefInfo ref;                    // dense reference (n_sel == n_atoms)
+  double* rmsd = nullptr;         // [n_frames] or null
+  double* stats = nullptr;        // [n_frames][16]: written (forward), read (backward), or null (both)
+  const void* w = nullptr;        // per-frame dL/drmsd (backward, both), null = 1
+  int w_f64 = 0;                  // w holds doubles (else floats)
+  int64_t w_stride = 1;           // elements between frames' weights (0: one shared weight)
+  float* grad = nullptr;          // [n_frames][n_atoms][3], 16-byte aligned (backward, both)
+  int* status = nullptr;
+  WaitCfg wait;
+};
+bool vg_usable(const float* coords, const float* grad, int64_t n_frames, int64_t n_atoms, int stride, int sm_count);
+cudaError_t launch_vg(int mode, const VgLaunch& V, int sm_count, cudaStream_t s);
 
 }  // namespace wmd

@@ -42,7 +42,7 @@ EXPORTED = (
     "wmd_create", "wmd_destroy", "wmd_last_error", "wmd_version", "wmd_reference_upload", "wmd_reference_free",
     "wmd_rmsd_frames", "wmd_rmsd_forward", "wmd_rmsd_backward", "wmd_rmsd_covariance", "wmd_pairwise_rmsd", "wmd_pairwise_dme",
     "wmd_batched_prepare", "wmd_batched_rmsd", "wmd_batched_layout", "wmd_rmsd_frames_noalloc", "wmd_set_wait_test",
-    "wmd_pairwise_rmsd_part",
+    "wmd_pairwise_rmsd_part", "wmd_rmsd_backward_f64", "wmd_rmsd_value_and_grad",
     "wmd_reference_upload_weighted", "wmd_superpose_transforms", "wmd_superpose", "wmd_rmsf", "wmd_rmsd_per_group",
     "wmd_group_ref_upload", "wmd_group_ref_free", "wmd_cluster_dbscan", "wmd_cluster_kmeans", "wmd_dcd_open",
     "wmd_dcd_close", "wmd_dcd_info", "wmd_dcd_read", "wmd_dcd_rmsd",
@@ -96,6 +96,8 @@ def load() -> ctypes.CDLL:
         L.wmd_rmsd_frames.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, i32, vp, vp]
         L.wmd_rmsd_forward.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, vp, vp]
         L.wmd_rmsd_backward.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, vp, vp, vp]
+        L.wmd_rmsd_backward_f64.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, vp, i64, vp, vp]
+        L.wmd_rmsd_value_and_grad.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, i64, vp, vp, vp]
         L.wmd_rmsd_covariance.argtypes = [vp, vp, i64, i64, i32, vp, i64, vp, vp, vp, vp, vp]
         L.wmd_pairwise_rmsd.argtypes = [vp, vp, i64, i64, i32, vp, i64, i32, i32, vp, vp]
         L.wmd_pairwise_rmsd_part.argtypes = [vp, vp, i64, i64, i32, vp, i64, i32, i32, i32, i32, vp, vp]

@@ -74,20 +74,57 @@ class RmsdFunction(torch.autograd.Function):
         ref = ctx_.ref
         ctx = N.context(x.device.index or 0)
         F, n_atoms = x.shape[0], x.shape[1]
-        g = grad_out.to(torch.float32).contiguous()
+        # dL/drmsd goes to the kernel as it is (float64, any stride: the
+        # broadcast ones of rmsd.sum() have stride 0), without a copy
+        g = grad_out
+        if g.dtype != torch.float64 or g.device != x.device or g.dim() != 1:
+            g = g.to(device=x.device, dtype=torch.float64).reshape(-1)
         # the kernel writes every selected atom of every frame; only atoms
         # outside the selection need zeros
         covers_all = not ctx_.has_sel and ref.n_sel == n_atoms
         grad = torch.empty_like(x) if covers_all else torch.zeros_like(x)
-        ctx.check(ctx.lib.wmd_rmsd_backward(ctx.handle, x.data_ptr(), F, n_atoms, 3,
-                                            sel.data_ptr() if ctx_.has_sel else None, ref.n_sel, ref.handle,
-                                            stats.data_ptr(), g.data_ptr(), grad.data_ptr(), _stream()))
+        ctx.check(ctx.lib.wmd_rmsd_backward_f64(ctx.handle, x.data_ptr(), F, n_atoms, 3,
+                                                sel.data_ptr() if ctx_.has_sel else None, ref.n_sel, ref.handle,
+                                                stats.data_ptr(), g.data_ptr(), g.stride(0), grad.data_ptr(),
+                                                _stream()))
         return grad, None, None
 
 
 def rmsd(coords: torch.Tensor, reference: torch.Tensor, selection: Optional[torch.Tensor] = None) -> torch.Tensor:
     """Per-frame aligned RMSD (float64), differentiable w.r.t. ``coords``."""
     return RmsdFunction.apply(coords, reference, selection)
+
+
+def rmsd_value_and_grad(coords: torch.Tensor, reference: torch.Tensor, weights: Optional[torch.Tensor] = None,
+                        selection: Optional[torch.Tensor] = None):
+    """Per-frame aligned RMSD (float64) and the gradient of
+    sum_f weights[f] * rmsd[f] w.r.t. ``coords`` (float32, shaped like it;
+    weights default to 1) in one call, outside autograd.  For dense packed
+    frames this is one kernel that reads each frame from DRAM once."""
+    if not coords.is_cuda or coords.dtype != torch.float32 or coords.dim() != 3 or coords.shape[2] != 3:
+        raise N.WarpMdError(N.WMD_ERR_INVALID_ARG, "coords must be a CUDA float32 tensor (frames, atoms, 3)")
+    x = coords.detach().contiguous()
+    ctx = N.context(x.device.index or 0)
+    ref = _cache.get(ctx, reference.to(x.device))
+    F, n_atoms = x.shape[0], x.shape[1]
+    sel = None
+    if selection is not None:
+        sel = selection.to(device=x.device, dtype=torch.int32).contiguous()
+        if sel.numel() != ref.n_sel:
+            raise N.WarpMdError(N.WMD_ERR_MISMATCH, "selection and reference lengths differ")
+    w = None
+    if weights is not None:
+        w = weights.to(device=x.device, dtype=torch.float64)
+        if w.dim() != 1 or w.shape[0] != F:
+            raise N.WarpMdError(N.WMD_ERR_MISMATCH, "weights must have one entry per frame")
+    out = torch.empty(F, dtype=torch.float64, device=x.device)
+    covers_all = sel is None and ref.n_sel == n_atoms
+    grad = torch.empty_like(x) if covers_all else torch.zeros_like(x)
+    ctx.check(ctx.lib.wmd_rmsd_value_and_grad(ctx.handle, x.data_ptr(), F, n_atoms, 3,
+                                              None if sel is None else sel.data_ptr(), ref.n_sel, ref.handle,
+                                              None if w is None else w.data_ptr(), 0 if w is None else w.stride(0),
+                                              out.data_ptr(), grad.data_ptr(), _stream()))
+    return out, grad
 
 
 def pairwise(coords: torch.Tensor, metric: str = "rms", mode: str = "i8x3") -> torch.Tensor:
