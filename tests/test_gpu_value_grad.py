@@ -138,3 +138,34 @@ def test_value_and_grad_is_reproducible():
     v1, g1 = rmsd_value_and_grad(x, y)
     v2, g2 = rmsd_value_and_grad(x, y)
     assert torch.equal(v1, v2) and torch.equal(g1, g2)
+
+
+def test_whole_frame_kernels_from_a_fresh_thread():
+    """The whole-frame kernels encode their tensor maps through the driver
+    API, which needs the device's context current on the calling thread; a
+    thread that made no CUDA call yet (the autograd engine's workers, a user's
+    thread) must work as the main thread does."""
+    import threading
+
+    from warp_md.torch_ops import rmsd_value_and_grad
+
+    fr, ref = _traj(2400, 400, 51)
+    x = torch.from_numpy(fr).cuda()
+    y = torch.from_numpy(ref).cuda()
+    main_v, main_g = rmsd_value_and_grad(x, y)
+    torch.cuda.synchronize()
+    box = {}
+
+    def work():
+        try:
+            v, g = rmsd_value_and_grad(x, y)
+            torch.cuda.synchronize()
+            box["v"], box["g"] = v.cpu(), g.cpu()
+        except Exception as exc:  # reported below
+            box["err"] = exc
+
+    t = threading.Thread(target=work)
+    t.start()
+    t.join(timeout=120)
+    assert "err" not in box, box.get("err")
+    assert torch.equal(box["v"], main_v.cpu()) and torch.equal(box["g"], main_g.cpu())

@@ -34,6 +34,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 
@@ -53,6 +54,7 @@ constexpr int kVgXBytes = 3 * kVgBoxBytes;            // 32 atoms of packed xyz 
 constexpr int kVgYBytes = kVgAtoms * 3 * 8;           // the stage's reference atoms, FP64
 constexpr int kVgStageBytes = (kVgXBytes + kVgYBytes + 1023) / 1024 * 1024;
 constexpr int kVgRingBytes = kVgWarps * 2 * kVgStageBytes;
+constexpr double kVgKeepBytes = 100e6;              // frames held in L2 up to this size (126 MB L2)
 constexpr int kDumpStride = 17;                       // doubles per lane in the combine (bank spread)
 constexpr int kVgFrmOffset = kVgRingBytes;            // [32][16] doubles: per-frame R, x_bar, scale, flag
 constexpr int kVgResOffset = kVgFrmOffset + 32 * 16 * 8;  // [8 warps][32] residual sums
@@ -78,22 +80,44 @@ struct VgArgs {
   int64_t w_stride = 1;        // elements between frames' weights (0: one shared weight)
   int* status = nullptr;
   WaitCfg wait;
+  int keep = 0;                // the frames fit L2: hold them for the next pass or kernel
 };
 
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+// L2 eviction priorities (cache hints only): the frames a later pass of the
+// group reads again are loaded evict_last, the last reads and the gradient
+// stores evict_first, so that the gradient does not push the frames out of
+// L2 between the passes.
+__device__ __forceinline__ uint64_t policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_normal() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar,
+                                            uint64_t policy) {
   asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
-          "r"(smem_addr(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1, {%2, %3}], [%4], %5;" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar)), "l"(policy)
       : "memory");
 }
 
 // 2-D TMA store of a box from shared memory (bulk-group completion); elements
 // outside the tensor are not written.
-__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int x, int y, const void* src) {
-  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
-                   reinterpret_cast<uint64_t>(map)),
-               "r"(x), "r"(y), "r"(smem_addr(src))
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int x, int y, const void* src, uint64_t policy) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group.L2::cache_hint [%0, {%1, %2}], [%3], %4;" ::
+                   "l"(reinterpret_cast<uint64_t>(map)),
+               "r"(x), "r"(y), "r"(smem_addr(src)), "l"(policy)
                : "memory");
 }
 
@@ -143,6 +167,12 @@ __global__ void __launch_bounds__(kVgThreads, 1) rmsd_vg_kernel(const __grid_con
   const bool withheld = A.wait.withhold && blockIdx.x == 0 && warp == 0;
   uint32_t n_iss = 0, n_don = 0;
 
+  // pass 1 loads: held in L2 for pass 2 (both), or for the backward kernel
+  // when the frames fit (forward); every other load is the last read
+  const uint64_t pol_first = policy_evict_first();
+  const uint64_t pol_hold = A.keep ? policy_evict_last() : policy_evict_normal();
+  uint64_t pol_load = MODE == kVgBwd ? pol_first : pol_hold;
+
   auto issue = [&](int64_t s, int64_t f0) {  // lane 0: stage s of the group at frame f0
     const int slot = (int)(n_iss & 1u);
     unsigned char* dst = ring + slot * kVgStageBytes;
@@ -153,7 +183,7 @@ __global__ void __launch_bounds__(kVgThreads, 1) rmsd_vg_kernel(const __grid_con
       mbar_arrive_expect_tx(&full[slot], 3u * 128u * (uint32_t)A.G + (uint32_t)kVgYBytes);
 #pragma unroll
       for (int b = 0; b < 3; ++b)
-        tma_load_2d(dst + b * kVgBoxBytes, &mx, (int)(s * 96 + 32 * b), (int)f0, &full[slot]);
+        tma_load_2d(dst + b * kVgBoxBytes, &mx, (int)(s * 96 + 32 * b), (int)f0, &full[slot], pol_load);
       bulk_copy_g2s(dst + kVgXBytes, A.yc + s * kVgAtoms * 3, kVgYBytes, &full[slot]);
     }
     ++n_iss;
@@ -161,18 +191,23 @@ __global__ void __launch_bounds__(kVgThreads, 1) rmsd_vg_kernel(const __grid_con
 
   // One pass of this warp over its stages; `pre` of them were issued already.
   // body(stage, stage index) runs on every lane.  Returns false when a wait
-  // ran out (all lanes of the warp agree).
-  auto run_pass = [&](int64_t f0, int pre, auto&& body) -> bool {
+  // ran out (all lanes of the warp agree).  A slot is refilled as soon as the
+  // warp is done with it, except in a pass that stores from its stages
+  // (late): there stage k + 1 is loaded into the slot of stage k - 1 once
+  // stage k has arrived, so that stage k - 1's store had that wait to finish
+  // reading the slot.
+  auto run_pass = [&](int64_t f0, int pre, bool late, auto&& body) -> bool {
     if (lane == 0)
       for (int64_t k = pre; k < (len < 2 ? len : (int64_t)2); ++k) issue(s0 + k, f0);
     for (int64_t k = 0; k < len; ++k) {
       bool ok = mbar_wait(&full[n_don & 1u], (n_don >> 1) & 1u, A.status, kStatusTimeoutFull, abort_flag,
                           A.wait.limit_ns);
       if (!__all_sync(0xffffffffu, ok)) return false;
+      if (late && lane == 0 && k >= 1 && k + 1 < len) issue(s0 + k + 1, f0);
       body(ring + (n_don & 1u) * kVgStageBytes, s0 + k);
       ++n_don;
       __syncwarp();
-      if (lane == 0 && k + 2 < len) issue(s0 + k + 2, f0);
+      if (!late && lane == 0 && k + 2 < len) issue(s0 + k + 2, f0);
     }
     return true;
   };
@@ -180,6 +215,7 @@ __global__ void __launch_bounds__(kVgThreads, 1) rmsd_vg_kernel(const __grid_con
   for (int64_t g = blockIdx.x; g < A.n_groups; g += gridDim.x) {
     const int64_t f0 = g * A.G;
     const int rows = (int)(A.F - f0 < (int64_t)A.G ? A.F - f0 : (int64_t)A.G);
+    if (MODE != kVgBwd) pol_load = pol_hold;
     const bool mine = lane < rows;  // this lane's frame exists
     const int64_t f = f0 + lane;
     int pre = 0;  // stages of the next pass already issued
@@ -189,7 +225,7 @@ __global__ void __launch_bounds__(kVgThreads, 1) rmsd_vg_kernel(const __grid_con
       double acc[15];
 #pragma unroll
       for (int e = 0; e < 15; ++e) acc[e] = 0.0;
-      const bool ok = run_pass(f0, 0, [&](unsigned char* st, int64_t) {
+      const bool ok = run_pass(f0, 0, false, [&](unsigned char* st, int64_t) {
         const double2* yb = reinterpret_cast<const double2*>(st + kVgXBytes);
         auto add = [&](float fx, float fy, float fz, double y0, double y1, double y2) {
           const double x0 = fx, x1 = fy, x2 = fz;
@@ -201,10 +237,13 @@ __global__ void __launch_bounds__(kVgThreads, 1) rmsd_vg_kernel(const __grid_con
         };
         // atoms past the frame's end arrive as zeros against zero reference
         // rows, so they add nothing
-#pragma unroll 2
+        // the row's 24 chunks first: independent loads, then the arithmetic
+        float4 v[24];
+#pragma unroll
+        for (int q = 0; q < 24; ++q) v[q] = *stage_chunk(st, lane, q);
+#pragma unroll
         for (int m = 0; m < kVgAtoms / 4; ++m) {
-          const float4 a = *stage_chunk(st, lane, 3 * m), b = *stage_chunk(st, lane, 3 * m + 1),
-                       c = *stage_chunk(st, lane, 3 * m + 2);
+          const float4 a = v[3 * m], b = v[3 * m + 1], c = v[3 * m + 2];
           const double2 y01 = yb[6 * m + 0], y23 = yb[6 * m + 1], y45 = yb[6 * m + 2];
           const double2 y67 = yb[6 * m + 3], y89 = yb[6 * m + 4], yab = yb[6 * m + 5];
           add(a.x, a.y, a.z, y01.x, y01.y, y23.x);
@@ -214,7 +253,8 @@ __global__ void __launch_bounds__(kVgThreads, 1) rmsd_vg_kernel(const __grid_con
         }
       });
       // both: prefetch the first stage of the next pass (every later pass of
-      // the group streams the same stages in the same order)
+      // the group streams the same stages in the same order), its last read
+      pol_load = pol_first;
       if (MODE == kVgBoth && ok && len > 0) {
         if (lane == 0) issue(s0, f0);
         pre = 1;
@@ -300,7 +340,7 @@ __global__ void __launch_bounds__(kVgThreads, 1) rmsd_vg_kernel(const __grid_con
       const bool flag = fr[kFrmFlag] != 0.0;
       const double my0 = A.sum_c[0] * inv_n, my1 = A.sum_c[1] * inv_n, my2 = A.sum_c[2] * inv_n;
       double ra = 0.0;
-      run_pass(f0, pre, [&](unsigned char* st, int64_t s) {
+      run_pass(f0, pre, false, [&](unsigned char* st, int64_t s) {
         const double2* yb = reinterpret_cast<const double2*>(st + kVgXBytes);
         const int valid = (int)(A.n_atoms - s * kVgAtoms < kVgAtoms ? A.n_atoms - s * kVgAtoms : (int64_t)kVgAtoms);
         auto add = [&](float fx, float fy, float fz, double y0, double y1, double y2, int k) {
@@ -345,30 +385,45 @@ __global__ void __launch_bounds__(kVgThreads, 1) rmsd_vg_kernel(const __grid_con
       for (int e = 0; e < 9; ++e) R[e] = fr[kFrmR + e];
       c[0] = fr[kFrmC]; c[1] = fr[kFrmC + 1]; c[2] = fr[kFrmC + 2];
       const double scale = fr[kFrmScale];
-      run_pass(f0, pre, [&](unsigned char* st, int64_t s) {
+      // grad_a = scale x_a + t_a with t_a = -scale c_a - sum_b scale R_ba y_b:
+      // 12 FP64 operations per atom (FP64 rounding differs from
+      // scale (x - c - R^T y) by ~1e-14 relative, far below float32)
+      double mt[9], d[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        d[a] = -scale * c[a];
+#pragma unroll
+        for (int b = 0; b < 3; ++b) mt[a * 3 + b] = -scale * R[b * 3 + a];
+      }
+      run_pass(f0, pre, true, [&](unsigned char* st, int64_t s) {
         const double2* yb = reinterpret_cast<const double2*>(st + kVgXBytes);
         auto grad3 = [&](float& fx, float& fy, float& fz, double y0, double y1, double y2) {
-          const double ty0 = R[0] * y0 + R[3] * y1 + R[6] * y2;
-          const double ty1 = R[1] * y0 + R[4] * y1 + R[7] * y2;
-          const double ty2 = R[2] * y0 + R[5] * y1 + R[8] * y2;
-          fx = (float)(scale * (((double)fx - c[0]) - ty0));
-          fy = (float)(scale * (((double)fy - c[1]) - ty1));
-          fz = (float)(scale * (((double)fz - c[2]) - ty2));
+          const double t0 = fma(mt[2], y2, fma(mt[1], y1, fma(mt[0], y0, d[0])));
+          const double t1 = fma(mt[5], y2, fma(mt[4], y1, fma(mt[3], y0, d[1])));
+          const double t2 = fma(mt[8], y2, fma(mt[7], y1, fma(mt[6], y0, d[2])));
+          fx = (float)fma(scale, (double)fx, t0);
+          fy = (float)fma(scale, (double)fy, t1);
+          fz = (float)fma(scale, (double)fz, t2);
         };
-#pragma unroll 2
+        // all loads of the row, then the arithmetic, then all stores back in
+        // place: no load waits behind a store it might alias
+        float4 v[24];
+#pragma unroll
+        for (int q = 0; q < 24; ++q) v[q] = *stage_chunk(st, lane, q);
+#pragma unroll
         for (int m = 0; m < kVgAtoms / 4; ++m) {
-          float4* pa = stage_chunk(st, lane, 3 * m);
-          float4* pb = stage_chunk(st, lane, 3 * m + 1);
-          float4* pc = stage_chunk(st, lane, 3 * m + 2);
-          float4 a = *pa, b = *pb, cc = *pc;
           const double2 y01 = yb[6 * m + 0], y23 = yb[6 * m + 1], y45 = yb[6 * m + 2];
           const double2 y67 = yb[6 * m + 3], y89 = yb[6 * m + 4], yab = yb[6 * m + 5];
+          float4& a = v[3 * m];
+          float4& b = v[3 * m + 1];
+          float4& cc = v[3 * m + 2];
           grad3(a.x, a.y, a.z, y01.x, y01.y, y23.x);
           grad3(a.w, b.x, b.y, y23.y, y45.x, y45.y);
           grad3(b.z, b.w, cc.x, y67.x, y67.y, y89.x);
           grad3(cc.y, cc.z, cc.w, y89.y, yab.x, yab.y);
-          *pa = a; *pb = b; *pc = cc;
         }
+#pragma unroll
+        for (int q = 0; q < 24; ++q) *stage_chunk(st, lane, q) = v[q];
         // the gradient of the stage leaves by TMA store (rows past the last
         // frame and atoms past the frame's end are outside the tensor)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -377,7 +432,7 @@ __global__ void __launch_bounds__(kVgThreads, 1) rmsd_vg_kernel(const __grid_con
 #pragma unroll
           for (int b = 0; b < 3; ++b)  // a box that starts past the frame's end has nothing to store
             if (s * 96 + 32 * b < A.n_atoms * 3)
-              tma_store_2d(&mg, (int)(s * 96 + 32 * b), (int)f0, st + b * kVgBoxBytes);
+              tma_store_2d(&mg, (int)(s * 96 + 32 * b), (int)f0, st + b * kVgBoxBytes, pol_first);
           bulk_commit();
         }
       });
@@ -414,17 +469,29 @@ EncodeTiled vg_encode_fn() {
   return fn;
 }
 
-// [F rows][n_atoms * 3 floats] with a [G rows][32 floats] box, 128-byte swizzle
-bool encode_frames(CUtensorMap* map, const float* base, int64_t F, int64_t n_atoms, int G) {
+// [F rows][n_atoms * 3 floats] with a [G rows][32 floats] box, 128-byte swizzle.
+// On failure *why describes the call.
+bool encode_frames(CUtensorMap* map, const float* base, int64_t F, int64_t n_atoms, int G, const char* what,
+                   const char** why) {
+  static thread_local char msg[256];
   EncodeTiled enc = vg_encode_fn();
-  if (!enc) return false;
+  if (!enc) {
+    if (why) *why = "cuTensorMapEncodeTiled unavailable";
+    return false;
+  }
   const cuuint64_t dims[2] = {(cuuint64_t)(n_atoms * 3), (cuuint64_t)F};
   const cuuint64_t strides[1] = {(cuuint64_t)(n_atoms * 12)};
   const cuuint32_t box[2] = {32, (cuuint32_t)G};
   const cuuint32_t estr[2] = {1, 1};
-  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, estr,
-             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS && why) {
+    snprintf(msg, sizeof(msg), "tensor map of the %s (CUresult %d, base %p, %lld x %lld floats, row %lld B, box 32 x %d)",
+             what, (int)r, (const void*)base, (long long)(n_atoms * 3), (long long)F, (long long)(n_atoms * 12), G);
+    *why = msg;
+  }
+  return r == CUDA_SUCCESS;
 }
 
 template <int MODE>
@@ -459,7 +526,7 @@ bool vg_usable(const float* coords, const float* grad, int64_t n_frames, int64_t
   return true;
 }
 
-cudaError_t launch_vg(int mode, const VgLaunch& V, int sm_count, cudaStream_t s) {
+cudaError_t launch_vg(int mode, const VgLaunch& V, int sm_count, cudaStream_t s, const char** why) {
   if (V.n_frames == 0) return cudaSuccess;
   // G frames per group: the fewest equal rounds of at most 32-frame groups
   // over one CTA per SM
@@ -481,13 +548,17 @@ cudaError_t launch_vg(int mode, const VgLaunch& V, int sm_count, cudaStream_t s)
   A.w_stride = V.w_stride;
   A.status = V.status;
   A.wait = V.wait;
+  // frames that fit comfortably in L2 are held there for the next pass (both)
+  // or for the backward kernel that usually follows the forward
+  A.keep = (double)V.n_frames * (double)V.n_atoms * 12.0 <= kVgKeepBytes;
   CUtensorMap mx, mg;
-  if (!encode_frames(&mx, V.coords, V.n_frames, V.n_atoms, G)) return cudaErrorInvalidValue;
+  if (!encode_frames(&mx, V.coords, V.n_frames, V.n_atoms, G, "frames", why)) return cudaErrorInvalidValue;
   if (mode != kVgFwd) {
-    if (!encode_frames(&mg, V.grad, V.n_frames, V.n_atoms, G)) return cudaErrorInvalidValue;
+    if (!encode_frames(&mg, V.grad, V.n_frames, V.n_atoms, G, "gradient", why)) return cudaErrorInvalidValue;
   } else {
     mg = mx;
   }
+  if (why) *why = "kernel launch";
   const int grid = (int)std::min<int64_t>(A.n_groups, sms);
   if (mode == kVgFwd) return launch_mode<kVgFwd>(mx, mg, A, grid, s);
   if (mode == kVgBwd) return launch_mode<kVgBwd>(mx, mg, A, grid, s);

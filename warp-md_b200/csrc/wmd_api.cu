@@ -147,11 +147,16 @@ int cuda_err(wmd_ctx* ctx, cudaError_t e, const char* what) {
   } while (0)
 
 // Keeps the caller's current device across a call.
+// Makes `dev` current for the call and restores the caller's device.  The
+// device is set even when it already is the thread's device: cudaSetDevice
+// also makes its primary context current on this thread, which driver-API
+// calls (the tensor-map encodes) need on threads where no runtime call has
+// bound it yet, such as the autograd engine's worker threads.
 struct DeviceGuard {
   int prev = -1;
   explicit DeviceGuard(int dev) {
     if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-    if (prev != dev) cudaSetDevice(dev);
+    cudaSetDevice(dev);
   }
   ~DeviceGuard() {
     int cur = -1;
@@ -1240,7 +1245,11 @@ WMD_EXPORT int wmd_rmsd_forward(wmd_ctx* ctx, const float* coords, int64_t n_fra
     wmd::VgLaunch V = vg_launch(ctx, ref, coords, n_frames, n_atoms);
     V.rmsd = out;
     V.stats = stats;
-    CU(wmd::launch_vg(wmd::kVgFwd, V, ctx->sm_count, s), "rmsd forward launch");
+    {
+      const char* why = "";
+      const cudaError_t e = wmd::launch_vg(wmd::kVgFwd, V, ctx->sm_count, s, &why);
+      if (e != cudaSuccess) return set_err(ctx, WMD_ERR_CUDA, "cuda driver error: rmsd forward (%s): %s", why, cudaGetErrorString(e));
+    }
     return WMD_OK;
   }
   wmd::FrameOutputs o;
@@ -1261,7 +1270,11 @@ static int backward_common(wmd_ctx* ctx, const float* coords, int64_t n_frames, 
     V.w_f64 = gd != nullptr;
     V.w_stride = gd ? gstride : 1;
     V.grad = grad;
-    CU(wmd::launch_vg(wmd::kVgBwd, V, ctx->sm_count, s), "rmsd backward launch");
+    {
+      const char* why = "";
+      const cudaError_t e = wmd::launch_vg(wmd::kVgBwd, V, ctx->sm_count, s, &why);
+      if (e != cudaSuccess) return set_err(ctx, WMD_ERR_CUDA, "cuda driver error: rmsd backward (%s): %s", why, cudaGetErrorString(e));
+    }
     return WMD_OK;
   }
   int rc = ensure(ctx, ctx->rot, (size_t)n_frames * wmd::kStatDoubles * sizeof(double));
@@ -1349,7 +1362,11 @@ WMD_EXPORT int wmd_rmsd_value_and_grad(wmd_ctx* ctx, const float* coords, int64_
     V.w_f64 = 1;
     V.w_stride = weight_stride;
     V.grad = grad;
-    CU(wmd::launch_vg(wmd::kVgBoth, V, ctx->sm_count, s), "rmsd value and gradient launch");
+    {
+      const char* why = "";
+      const cudaError_t e = wmd::launch_vg(wmd::kVgBoth, V, ctx->sm_count, s, &why);
+      if (e != cudaSuccess) return set_err(ctx, WMD_ERR_CUDA, "cuda driver error: rmsd value and gradient (%s): %s", why, cudaGetErrorString(e));
+    }
     return WMD_OK;
   }
   // any other shape: the forward into context scratch, then the backward

@@ -128,6 +128,7 @@ struct VgLaunch {
   WaitCfg wait;
 };
 bool vg_usable(const float* coords, const float* grad, int64_t n_frames, int64_t n_atoms, int stride, int sm_count);
-cudaError_t launch_vg(int mode, const VgLaunch& V, int sm_count, cudaStream_t s);
+// On failure *why (when given) names the step: a tensor map or the launch.
+cudaError_t launch_vg(int mode, const VgLaunch& V, int sm_count, cudaStream_t s, const char** why = nullptr);
 
 }  // namespace wmd

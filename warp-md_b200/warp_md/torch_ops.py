@@ -96,11 +96,14 @@ def rmsd(coords: torch.Tensor, reference: torch.Tensor, selection: Optional[torc
 
 
 def rmsd_value_and_grad(coords: torch.Tensor, reference: torch.Tensor, weights: Optional[torch.Tensor] = None,
-                        selection: Optional[torch.Tensor] = None):
+                        selection: Optional[torch.Tensor] = None, out: Optional[torch.Tensor] = None,
+                        grad: Optional[torch.Tensor] = None):
     """Per-frame aligned RMSD (float64) and the gradient of
     sum_f weights[f] * rmsd[f] w.r.t. ``coords`` (float32, shaped like it;
     weights default to 1) in one call, outside autograd.  For dense packed
-    frames this is one kernel that reads each frame from DRAM once."""
+    frames this is one kernel that reads each frame from DRAM once.  ``out``
+    and ``grad`` may be given (contiguous, right shape and dtype) to be
+    filled in place, e.g. inside a captured CUDA graph."""
     if not coords.is_cuda or coords.dtype != torch.float32 or coords.dim() != 3 or coords.shape[2] != 3:
         raise N.WarpMdError(N.WMD_ERR_INVALID_ARG, "coords must be a CUDA float32 tensor (frames, atoms, 3)")
     x = coords.detach().contiguous()
@@ -117,9 +120,17 @@ def rmsd_value_and_grad(coords: torch.Tensor, reference: torch.Tensor, weights: 
         w = weights.to(device=x.device, dtype=torch.float64)
         if w.dim() != 1 or w.shape[0] != F:
             raise N.WarpMdError(N.WMD_ERR_MISMATCH, "weights must have one entry per frame")
-    out = torch.empty(F, dtype=torch.float64, device=x.device)
+    if out is None:
+        out = torch.empty(F, dtype=torch.float64, device=x.device)
+    elif out.shape != (F,) or out.dtype != torch.float64 or not out.is_contiguous() or out.device != x.device:
+        raise N.WarpMdError(N.WMD_ERR_MISMATCH, "out must be a contiguous float64 vector of one entry per frame")
     covers_all = sel is None and ref.n_sel == n_atoms
-    grad = torch.empty_like(x) if covers_all else torch.zeros_like(x)
+    if grad is None:
+        grad = torch.empty_like(x) if covers_all else torch.zeros_like(x)
+    elif grad.shape != x.shape or grad.dtype != torch.float32 or not grad.is_contiguous() or grad.device != x.device:
+        raise N.WarpMdError(N.WMD_ERR_MISMATCH, "grad must be a contiguous float32 tensor shaped like coords")
+    elif not covers_all:
+        grad.zero_()  # rows of atoms outside the selection are not written
     ctx.check(ctx.lib.wmd_rmsd_value_and_grad(ctx.handle, x.data_ptr(), F, n_atoms, 3,
                                               None if sel is None else sel.data_ptr(), ref.n_sel, ref.handle,
                                               None if w is None else w.data_ptr(), 0 if w is None else w.stride(0),
