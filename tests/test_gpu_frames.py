@@ -274,3 +274,25 @@ def test_streaming_workload_sampled_parity(gpu_ctx):
     r.close()
     del coords
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("n_atoms,n_frames", [(4001, 2403), (1002, 9602), (99999, 66)])
+def test_frames_across_lanes_quad_rows(gpu_ctx, n_atoms, n_frames):
+    """Packed xyz frames whose stride is not a multiple of 16 bytes, enough of
+    them for the frames-across-lanes kernel: it reads quad rows of 4 frames
+    (odd n_atoms; n_atoms % 4 == 2) and leaves the last n_frames mod 4 frames
+    (3, 2, 2 here) to the gathered kernel.  Aligned and no-fit RMSD and a
+    dense prefix against the oracle (plan.rs:1093-1248) within 1e-5 A."""
+    fr, ref = synth.make_trajectory(n_atoms, n_frames, (0.05, 3.0), seed=n_atoms + n_frames)
+    fr[n_frames - 1] = ref  # in the gathered tail: the residual pass
+    got = gpu_rmsd(gpu_ctx, fr, ref, device_io=True)
+    _, exp = oracle.rmsd_frames(fr, ref)
+    np.testing.assert_allclose(got, exp, rtol=0, atol=TOL)
+    assert got[-1] < 1e-9
+    raw = gpu_rmsd(gpu_ctx, fr, ref, align=False, device_io=True)
+    _, expr = oracle.rmsd_frames(fr, ref, align=False)
+    np.testing.assert_allclose(raw, expr, rtol=0, atol=TOL)
+    k = n_atoms - 37
+    got = gpu_rmsd(gpu_ctx, fr, ref[:k], device_io=True)
+    _, exp = oracle.rmsd_frames(fr, ref[:k], selection=np.arange(k))
+    np.testing.assert_allclose(got, exp, rtol=0, atol=TOL)

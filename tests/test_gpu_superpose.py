@@ -228,3 +228,17 @@ def test_superpose_large_frames_host_chunks():
     oxf, _ = oracle.superpose(host[sample], ref.cpu().numpy())
     _check_xf(xf[sample], oxf)
     _check_coords(out[sample], _oracle_moved(oxf, host[sample]))
+
+
+def test_superpose_weighted_quad_rows_odd_atoms():
+    """Mass-weighted transforms over every atom of 2,001-atom packed frames
+    (stride not a multiple of 16 bytes): the frames-across-lanes kernel on
+    quad rows plus the gathered tail, against the oracle's weighted Kabsch."""
+    n, F = 2001, 4801
+    fr, ref = synth.make_trajectory(n, F, 0.4, 77)
+    w = np.random.default_rng(7).uniform(1.0, 16.0, n).astype(np.float32)
+    xf, out = _superpose(fr, ref, weights=w, device_io=True)
+    pick = np.r_[0:40, F - 40:F]
+    oxf, _ = oracle.superpose(fr[pick], ref, weights=w)
+    _check_xf(xf[pick], oxf)
+    _check_coords(out[pick], _oracle_moved(oxf, fr[pick]))

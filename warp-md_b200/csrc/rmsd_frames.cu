@@ -699,6 +699,21 @@ cudaError_t launch_rmsd_forward(const FrameLaunch& L, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+cudaError_t launch_gather_partials(const FrameLaunch& L, bool raw, int sm_count, cudaStream_t s) {
+  if (L.n_frames == 0) return cudaSuccess;
+  FrameLaunch B = L;
+  B.lanes = false;
+  B.gather = true;
+  B.grid = frame_grid(B, sm_count, false);
+  const int mode = raw ? kFwdRaw : (L.ref.w ? kFwdW : kFwdFit);
+  if (L.stride == 4) {
+    if (mode == kFwdRaw) return launch_gather<4, kFwdRaw>(B, s);
+    return mode == kFwdW ? launch_gather<4, kFwdW>(B, s) : launch_gather<4, kFwdFit>(B, s);
+  }
+  if (mode == kFwdRaw) return launch_gather<3, kFwdRaw>(B, s);
+  return mode == kFwdW ? launch_gather<3, kFwdW>(B, s) : launch_gather<3, kFwdFit>(B, s);
+}
+
 cudaError_t launch_rmsd_stream(const FrameLaunch& L, cudaStream_t s) {
   if (L.n_frames == 0) return cudaSuccess;
   return L.lanes ? launch_lanes_forward(L, false, s) : dispatch<kFwdFit>(L, s);

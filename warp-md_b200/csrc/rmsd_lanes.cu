@@ -20,6 +20,18 @@
 //     warp gets the same number of whole units, so results do not depend on
 //     the launch shape and are bitwise reproducible.
 //
+// Frames whose stride is not a multiple of 16 bytes (packed xyz with
+// n_atoms % 4 != 0) cannot be rows of a tensor map; four consecutive frames
+// can (48 n_atoms bytes).  Such launches (dense selections) read "quad rows":
+// a stage is four boxes of [8 quad rows x 100 floats], box j holding frames
+// 32g + 4i + j (i = 0..7).  Box j starts at the 16-byte boundary at or below
+// frame position j's first atom of the stage, so lane 4i + j reads its 96
+// floats at a fixed offset of (3 j n_atoms) mod 4 floats with 32-bit loads:
+// rows of 400 bytes put the 32 lanes in distinct banks for odd n_atoms (two
+// lanes per bank otherwise).  Atoms past the tile come from the next frame of
+// the quad row and are masked.  The last n_frames mod 4 frames are left to the
+// gathered kernel, with the same tiles and partial layout.
+//
 // Atoms streamed: a dense selection (the first n_sel atoms), or the span
 // [lane_atom0, lane_atom0 + lane_atoms) of a sorted selection with the
 // reference expanded onto it and per-atom weights (1 for selected atoms, 0
@@ -58,6 +70,28 @@ struct LaneGeo {
   static constexpr int kBarOffset = kLaneWarps * kLaneStages * kStageBytes;
   static constexpr int kAbortOffset = kBarOffset + kLaneWarps * kLaneStages * 8;
   static constexpr int kSmemBytes = kAbortOffset + 16 + 1024;  // + slack to align the base to 1024
+};
+
+// quad rows (packed xyz, n_atoms % 4 != 0): 4 boxes of [8 quad rows x 100 floats], no swizzle
+struct QuadGeo {
+  static constexpr int kBoxRowBytes = 100 * 4;
+  static constexpr int kBoxBytes = 8 * kBoxRowBytes;
+  static constexpr int kXBytes = 4 * kBoxBytes;
+  static constexpr int kYBytes = kLaneAtoms * 3 * 8;
+  static constexpr int kWBytes = kLaneAtoms * 4;
+  static constexpr int kStageBytes = (kXBytes + kYBytes + kWBytes + 127) / 128 * 128;
+  static constexpr int kBarOffset = kLaneWarps * kLaneStages * kStageBytes;
+  static constexpr int kAbortOffset = kBarOffset + kLaneWarps * kLaneStages * 8;
+  static constexpr int kSmemBytes = kAbortOffset + 16 + 1024;
+};
+
+template <bool QUAD, int STRIDE>
+struct PickGeo {
+  using type = LaneGeo<STRIDE>;
+};
+template <int STRIDE>
+struct PickGeo<true, STRIDE> {
+  using type = QuadGeo;
 };
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
@@ -130,10 +164,49 @@ __device__ __forceinline__ void stage_sums(double (&acc)[15], const unsigned cha
   }
 }
 
-template <int STRIDE, bool RAW, bool W>
+// The quad-row form of stage_sums: lane 4i + j reads frame position j's box,
+// row i, from float offset off; atoms at or past `valid` are masked.
+template <bool RAW, bool W>
+__device__ __forceinline__ void stage_sums_quad(double (&acc)[15], const unsigned char* st, int lane, int off,
+                                                int valid, const FrameLaunch& L) {
+  const float* wb = reinterpret_cast<const float*>(st + QuadGeo::kXBytes + QuadGeo::kYBytes);
+  const float* row =
+      reinterpret_cast<const float*>(st + (lane & 3) * QuadGeo::kBoxBytes + (lane >> 2) * QuadGeo::kBoxRowBytes) + off;
+  const double* yb = reinterpret_cast<const double*>(st + QuadGeo::kXBytes);
+#pragma unroll 4
+  for (int k = 0; k < kLaneAtoms; ++k) {
+    if (k >= valid) break;
+    const double x0 = row[3 * k], x1 = row[3 * k + 1], x2 = row[3 * k + 2];
+    const double y0 = yb[3 * k], y1 = yb[3 * k + 1], y2 = yb[3 * k + 2];
+    if (RAW) {
+      const bool in = !W || wb[k] != 0.0f;
+      const double d0 = x0 - (y0 + L.ref.mean[0]);
+      const double d1 = x1 - (y1 + L.ref.mean[1]);
+      const double d2 = x2 - (y2 + L.ref.mean[2]);
+      acc[0] = fma(d0, in ? d0 : 0.0, acc[0]);
+      acc[1] = fma(d1, in ? d1 : 0.0, acc[1]);
+      acc[2] = fma(d2, in ? d2 : 0.0, acc[2]);
+    } else {
+      if (W) {
+        const double w = wb[k];
+        const double u0 = w * x0, u1 = w * x1, u2 = w * x2;
+        acc[0] += u0; acc[1] += u1; acc[2] += u2;
+        acc[3] = fma(u0, x0, acc[3]); acc[4] = fma(u1, x1, acc[4]); acc[5] = fma(u2, x2, acc[5]);
+      } else {
+        acc[0] += x0; acc[1] += x1; acc[2] += x2;
+        acc[3] = fma(x0, x0, acc[3]); acc[4] = fma(x1, x1, acc[4]); acc[5] = fma(x2, x2, acc[5]);
+      }
+      acc[6] = fma(x0, y0, acc[6]);  acc[7] = fma(x0, y1, acc[7]);  acc[8] = fma(x0, y2, acc[8]);
+      acc[9] = fma(x1, y0, acc[9]);  acc[10] = fma(x1, y1, acc[10]); acc[11] = fma(x1, y2, acc[11]);
+      acc[12] = fma(x2, y0, acc[12]); acc[13] = fma(x2, y1, acc[13]); acc[14] = fma(x2, y2, acc[14]);
+    }
+  }
+}
+
+template <int STRIDE, bool RAW, bool W, bool QUAD = false>
 __global__ void __launch_bounds__(kLaneWarps * 32) rmsd_lanes_kernel(const __grid_constant__ CUtensorMap map,
                                                                      const FrameLaunch L) {
-  using G = LaneGeo<STRIDE>;
+  using G = typename PickGeo<QUAD, STRIDE>::type;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -179,9 +252,18 @@ __global__ void __launch_bounds__(kLaneWarps * 32) rmsd_lanes_kernel(const __gri
       // the warp's earlier generic reads of this slot before the async writes
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive_expect_tx(&full[slot], G::kXBytes + G::kYBytes + (W ? G::kWBytes : 0));
+      if (QUAD) {
+        // frame position j of the quad rows 8g .. 8g + 7: its atoms a0 .. a0 + 31
 #pragma unroll
-      for (int b = 0; b < G::kBoxes; ++b)
-        tma_load_2d(dst + b * 4096, &map, (int)(a0 * STRIDE + 32 * b), (int)(g * 32), &full[slot]);
+        for (int j = 0; j < 4; ++j) {
+          const int64_t e = (int64_t)j * 3 * L.n_atoms + 3 * a0;
+          tma_load_2d(dst + j * QuadGeo::kBoxBytes, &map, (int)(e & ~int64_t(3)), (int)(g * 8), &full[slot]);
+        }
+      } else {
+#pragma unroll
+        for (int b = 0; b < LaneGeo<STRIDE>::kBoxes; ++b)
+          tma_load_2d(dst + b * 4096, &map, (int)(a0 * STRIDE + 32 * b), (int)(g * 32), &full[slot]);
+      }
       bulk_copy_g2s(dst + G::kXBytes, L.lane_y + a0 * 3, G::kYBytes, &full[slot]);
       if (W) bulk_copy_g2s(dst + G::kXBytes + G::kYBytes, L.lane_w + a0, G::kWBytes, &full[slot]);
     }
@@ -194,6 +276,9 @@ __global__ void __launch_bounds__(kLaneWarps * 32) rmsd_lanes_kernel(const __gri
   if (lane == 0)
     while (n_issued < kLaneStages && pu < u1) issue_next();
 
+  // quad rows: this lane's float offset into its box row (stages start at
+  // multiples of 32 atoms, so only the frame position matters)
+  const int quad_off = QUAD ? (int)(((int64_t)(lane & 3) * 3 * L.n_atoms) & 3) : 0;
   int64_t n_done = 0;
   bool aborted = false;
   for (int64_t u = u0; u < u1 && !aborted; ++u) {
@@ -211,7 +296,10 @@ __global__ void __launch_bounds__(kLaneWarps * 32) rmsd_lanes_kernel(const __gri
       }
       const int64_t a0 = t * tile + (int64_t)k * kLaneAtoms;
       const int valid = (int)min((int64_t)kLaneAtoms, n_sel - a0);
-      stage_sums<STRIDE, RAW, W>(acc, ring + slot * G::kStageBytes, lane, valid, L);
+      if (QUAD)
+        stage_sums_quad<RAW, W>(acc, ring + slot * G::kStageBytes, lane, quad_off, valid, L);
+      else
+        stage_sums<STRIDE, RAW, W>(acc, ring + slot * G::kStageBytes, lane, valid, L);
       ++n_done;
       __syncwarp();
       if (lane == 0 && pu < u1) issue_next();
@@ -260,43 +348,62 @@ int64_t lane_units(const FrameLaunch& L, int64_t tile) {
   return ((L.n_frames + 31) / 32) * ((L.lane_atoms + tile - 1) / tile);
 }
 
-template <int STRIDE, bool RAW>
+template <int STRIDE, bool RAW, bool QUAD = false>
 int lanes_occupancy() {
-  auto kern = rmsd_lanes_kernel<STRIDE, RAW, false>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, LaneGeo<STRIDE>::kSmemBytes);
+  using G = typename PickGeo<QUAD, STRIDE>::type;
+  auto kern = rmsd_lanes_kernel<STRIDE, RAW, false, QUAD>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::kSmemBytes);
   int b = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kLaneWarps * 32, LaneGeo<STRIDE>::kSmemBytes) !=
-      cudaSuccess)
-    b = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kLaneWarps * 32, G::kSmemBytes) != cudaSuccess) b = 1;
   return std::max(b, 1);
 }
 
-template <int STRIDE, bool RAW, bool W>
+// QUAD: L.n_frames is a multiple of 4 and the rows of the tensor map are
+// quad rows of 4 frames (packed xyz, dense selection).
+template <int STRIDE, bool RAW, bool W, bool QUAD = false>
 cudaError_t launch_lanes(const FrameLaunch& L, cudaStream_t s) {
+  using G = typename PickGeo<QUAD, STRIDE>::type;
   EncodeTiled enc = encode_fn();
   if (!enc) return cudaErrorNotSupported;
   CUtensorMap map;
-  const cuuint64_t dims[2] = {(cuuint64_t)(L.lane_atoms * STRIDE), (cuuint64_t)L.n_frames};
-  const cuuint64_t strides[1] = {(cuuint64_t)(L.n_atoms * STRIDE * 4)};
-  const cuuint32_t box[2] = {32, 32};
-  const cuuint32_t estr[2] = {1, 1};
-  float* base = const_cast<float*>(L.coords) + L.lane_atom0 * STRIDE;
-  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr,
-          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-    return cudaErrorInvalidValue;
-  auto kern = rmsd_lanes_kernel<STRIDE, RAW, W>;
+  CUresult r;
+  if (QUAD) {
+    const cuuint64_t dims[2] = {(cuuint64_t)(L.n_atoms * 12), (cuuint64_t)(L.n_frames / 4)};
+    const cuuint64_t strides[1] = {(cuuint64_t)(L.n_atoms * 48)};
+    const cuuint32_t box[2] = {100, 8};
+    const cuuint32_t estr[2] = {1, 1};
+    r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(L.coords), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  } else {
+    const cuuint64_t dims[2] = {(cuuint64_t)(L.lane_atoms * STRIDE), (cuuint64_t)L.n_frames};
+    const cuuint64_t strides[1] = {(cuuint64_t)(L.n_atoms * STRIDE * 4)};
+    const cuuint32_t box[2] = {32, 32};
+    const cuuint32_t estr[2] = {1, 1};
+    float* base = const_cast<float*>(L.coords) + L.lane_atom0 * STRIDE;
+    r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  }
+  if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+  auto kern = rmsd_lanes_kernel<STRIDE, RAW, W, QUAD>;
   static bool attr_done[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   if (!attr_done[dev]) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, LaneGeo<STRIDE>::kSmemBytes);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::kSmemBytes);
     if (e != cudaSuccess) return e;
     attr_done[dev] = true;
   }
-  kern<<<L.grid, kLaneWarps * 32, LaneGeo<STRIDE>::kSmemBytes, s>>>(map, L);
+  kern<<<L.grid, kLaneWarps * 32, G::kSmemBytes, s>>>(map, L);
   return cudaGetLastError();
+}
+
+// Packed xyz frames whose stride is not a multiple of 16 bytes, streamed as
+// quad rows: a dense selection only (the tensor map covers whole frames).
+bool lanes_quad(const FrameLaunch& L) {
+  return L.stride == 3 && (L.n_atoms & 3) != 0 && L.sel == nullptr && L.lane_atom0 == 0 &&
+         L.lane_atoms == L.ref.n_sel && L.lane_y == L.ref.yc && L.lane_w == L.ref.w;
 }
 
 // y_exp[(sel[i] - a0)][c] = yc[i][c], w_exp[sel[i] - a0] = w ? w[i] : 1 (the
@@ -326,21 +433,30 @@ cudaError_t launch_lanes_expand(const uint32_t* sel, int64_t n_sel, int64_t a0, 
 bool lanes_eligible(const FrameLaunch& L) {
   static int mode = -1;
   if (mode < 0) {
+    // WMD_FRAMES_KERNEL=atoms: always the atom-major kernel; =noquad: not for
+    // packed frames whose stride is not a multiple of 16 bytes
     const char* e = std::getenv("WMD_FRAMES_KERNEL");
-    mode = (e && std::strcmp(e, "atoms") == 0) ? 0 : 1;
+    mode = (e && std::strcmp(e, "atoms") == 0) ? 0 : (e && std::strcmp(e, "noquad") == 0) ? 2 : 1;
   }
   if (!mode || L.lane_atoms <= 0 || L.n_frames <= 0) return false;
-  if (L.stride != 4 && (L.n_atoms & 3) != 0) return false;
   if ((reinterpret_cast<uintptr_t>(L.coords + L.lane_atom0 * L.stride) & 15u) != 0) return false;
+  if (L.stride != 4 && (L.n_atoms & 3) != 0) {
+    // quad rows of 4 frames: whole frames of a dense selection, and enough
+    // frames that the gathered tail (n_frames mod 4) stays small
+    if (mode == 2 || !lanes_quad(L) || L.n_frames < 32) return false;
+    return L.n_atoms * 12 < (int64_t(1) << 31) && L.n_frames < (int64_t(1) << 31);
+  }
   if ((L.lane_atom0 + L.lane_atoms) * L.stride >= (int64_t(1) << 31) || L.n_frames >= (int64_t(1) << 31))
     return false;
   return true;
 }
 
-static int lanes_slots(int stride, int sm_count) {
-  static int occ[2] = {0, 0};
-  int& o = occ[stride == 4 ? 1 : 0];
-  if (o == 0) o = stride == 4 ? lanes_occupancy<4, false>() : lanes_occupancy<3, false>();
+static int lanes_slots(const FrameLaunch& L, int sm_count) {
+  static int occ[3] = {0, 0, 0};
+  const int which = L.stride == 4 ? 1 : lanes_quad(L) ? 2 : 0;
+  int& o = occ[which];
+  if (o == 0) o = which == 1 ? lanes_occupancy<4, false>() : which == 2 ? lanes_occupancy<3, false, true>()
+                                                                        : lanes_occupancy<3, false>();
   return sm_count * o * kLaneWarps;
 }
 
@@ -363,7 +479,7 @@ int lanes_tile(const FrameLaunch& L, int sm_count) {
   // bytes: (units per warp) x (tile bytes + its 128-byte partial, written
   // and read back).  Large tiles mean few records; small ones balance short
   // runs (few frames or few atoms) over all warp slots.
-  const int64_t slots = lanes_slots(L.stride, sm_count);
+  const int64_t slots = lanes_slots(L, sm_count);
   int64_t best = kLaneTile, best_cost = -1;
   for (int64_t tile = kLaneTile; tile >= 256; tile /= 2) {
     const int64_t per = (lane_units(L, tile) + slots - 1) / slots;
@@ -377,13 +493,35 @@ int lanes_tile(const FrameLaunch& L, int sm_count) {
 }
 
 int lanes_grid(const FrameLaunch& L, int sm_count) {
-  return (int)((lane_warps(L, lanes_slots(L.stride, sm_count)) + kLaneWarps - 1) / kLaneWarps);
+  return (int)((lane_warps(L, lanes_slots(L, sm_count)) + kLaneWarps - 1) / kLaneWarps);
 }
 
 cudaError_t launch_lanes_forward(const FrameLaunch& L, bool raw, cudaStream_t s) {
   FrameLaunch K = L;
-  K.lane_warps = (int)lane_warps(L, (int64_t)L.grid * kLaneWarps);
   const bool w = L.lane_w != nullptr;
+  if (lanes_quad(L)) {
+    // whole quad rows here; the last n_frames mod 4 frames by the gathered
+    // kernel into the same partial layout
+    const int64_t main = L.n_frames & ~int64_t(3);
+    if (main > 0) {  // a batch of fewer than 4 frames has no quad row
+      K.n_frames = main;
+      K.lane_warps = (int)lane_warps(K, (int64_t)L.grid * kLaneWarps);
+      cudaError_t e = w ? (raw ? launch_lanes<3, true, true, true>(K, s) : launch_lanes<3, false, true, true>(K, s))
+                        : (raw ? launch_lanes<3, true, false, true>(K, s) : launch_lanes<3, false, false, true>(K, s));
+      if (e != cudaSuccess || main == L.n_frames) return e;
+    }
+    FrameLaunch T = L;
+    T.coords = L.coords + (size_t)main * L.n_atoms * 3;
+    T.n_frames = L.n_frames - main;
+    T.partial = L.partial + (size_t)main * frame_tiles(L) * kStatDoubles;
+    static int sms[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!sms[dev]) cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+    return launch_gather_partials(T, raw, sms[dev], s);
+  }
+  K.lane_warps = (int)lane_warps(L, (int64_t)L.grid * kLaneWarps);
   if (L.stride == 4) {
     if (w) return raw ? launch_lanes<4, true, true>(K, s) : launch_lanes<4, false, true>(K, s);
     return raw ? launch_lanes<4, true, false>(K, s) : launch_lanes<4, false, false>(K, s);

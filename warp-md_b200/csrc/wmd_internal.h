@@ -107,6 +107,10 @@ cudaError_t launch_rmsd_backward(const FrameLaunch& L, const double* stats, cons
                                  const double* grad_f64, int64_t grad_stride, double* rot_scratch, cudaStream_t s);
 // occupancy-derived persistent grid for a launch
 int frame_grid(const FrameLaunch& L, int sm_count, bool backward);
+// The gathered kernel's (tile, frame) partials for L's frames with tiles of
+// L.tile_atoms over a dense selection: the frames-across-lanes kernel's layout,
+// for frames it leaves to others (raw: the no-fit record).
+cudaError_t launch_gather_partials(const FrameLaunch& L, bool raw, int sm_count, cudaStream_t s);
 
 // Whole-frame kernels for many frames of up to kVgMaxAtoms atoms
 // (rmsd_vg.cu): forward (rmsd and the 16-double records of
