@@ -1147,6 +1147,75 @@ def run_ours(args):
     return 0
 
 
+def run_profile_case(name):
+    """Small cases of single kernels for ncu captures (``--profile-case``); they
+    print no bench line.
+
+    vg:   4,096 frames x 2,000 atoms through wmd_rmsd_forward,
+          wmd_rmsd_backward_f64 and wmd_rmsd_value_and_grad, twice, with a
+          256 MB write (larger than L2) before the forward and the fused call.
+    quad: 99,999-atom frames (a 12-byte frame stride that is not a multiple of
+          16 bytes: quad rows) x 400 frames through wmd_rmsd_frames, 3 calls.
+    perres: per-residue RMSD of 100,000 atoms x 2,000 frames (2.4 GB), residues
+          of 10 consecutive atoms, every 10th atom superposed: 3 calls of
+          wmd_rmsd_per_group.
+    """
+    import numpy as np
+    import torch
+    from warp_md import _native as N
+    from warp_md import synth
+
+    ctx = N.context(0)
+    if name == "vg":
+        F, n = 4096, 2000
+        fr, rf = synth.make_trajectory(n, F, 0.3, seed=17)
+        x = torch.from_numpy(fr).cuda()
+        ref = torch.from_numpy(rf).cuda()
+        r = N.Reference(ctx, ref.data_ptr(), n, 3, keepalive=ref)
+        out = torch.empty(F, dtype=torch.float64, device="cuda")
+        stats = torch.empty(F, N.FRAME_STATS, dtype=torch.float64, device="cuda")
+        g = torch.empty_like(x)
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        for _ in range(2):
+            flush.fill_(1)
+            ctx.check(ctx.lib.wmd_rmsd_forward(ctx.handle, x.data_ptr(), F, n, 3, None, n, r.handle,
+                                               out.data_ptr(), stats.data_ptr(), None))
+            ctx.check(ctx.lib.wmd_rmsd_backward_f64(ctx.handle, x.data_ptr(), F, n, 3, None, n, r.handle,
+                                                    stats.data_ptr(), None, 0, g.data_ptr(), None))
+            flush.fill_(1)
+            ctx.check(ctx.lib.wmd_rmsd_value_and_grad(ctx.handle, x.data_ptr(), F, n, 3, None, n, r.handle,
+                                                      None, 0, out.data_ptr(), g.data_ptr(), None))
+    elif name == "quad":
+        n, F = 99_999, 400
+        x, ref = synth.make_trajectory_torch(n, F, SIGMA, seed=1, device="cuda")
+        r = N.Reference(ctx, ref.data_ptr(), n, 3, keepalive=ref)
+        out = torch.empty(F, dtype=torch.float64, device="cuda")
+        for _ in range(3):
+            ctx.check(ctx.lib.wmd_rmsd_frames(ctx.handle, x.data_ptr(), F, n, 3, None, n, r.handle, 1,
+                                              out.data_ptr(), None))
+    elif name == "perres":
+        n, F = 100_000, 2000
+        x, ref = synth.make_trajectory_torch(n, F, SIGMA, seed=3, device="cuda")
+        ref_h = ref.cpu().numpy()
+        sel = np.arange(0, n, 10, dtype=np.uint32)
+        goff = np.arange(0, n + 1, 10, dtype=np.uint32)
+        gref = N.GroupRef(ctx, ref_h, goff, np.arange(n, dtype=np.uint32))
+        r = N.Reference.from_numpy(ctx, ref_h[sel])
+        dsel = torch.from_numpy(sel.astype(np.int32)).cuda()
+        out = torch.empty(F, goff.size - 1, device="cuda")
+        for _ in range(3):
+            ctx.check(ctx.lib.wmd_rmsd_per_group(ctx.handle, x.data_ptr(), F, n, 3, dsel.data_ptr(), sel.size,
+                                                 r.handle, gref.handle, 1, out.data_ptr(), None))
+        torch.cuda.synchronize()
+        gref.close()
+    else:
+        raise SystemExit(f"unknown profile case {name!r}")
+    torch.cuda.synchronize()
+    r.close()
+    print(f"profile case {name}: ok", flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1184,7 +1253,10 @@ def main():
     ap.add_argument("--dcd-frames", type=int, default=2000)
     ap.add_argument("--dcd-steps", type=int, default=5)
     ap.add_argument("--dcd-cpu-frames", type=int, default=100)
+    ap.add_argument("--profile-case", choices=["vg", "quad", "perres"], help="run one small kernel case for ncu and exit")
     args = ap.parse_args()
+    if args.profile_case:
+        return run_profile_case(args.profile_case)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

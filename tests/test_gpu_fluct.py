@@ -162,9 +162,10 @@ def test_group_ref_validates_groups():
 
 
 @pytest.mark.parametrize("stride", [3, 4])
-def test_rmsd_per_group_one_pass_many_frames_and_group_shapes(stride):
-    """wmd_rmsd_per_group with superposition (the one-pass clustered kernel):
-    300 frames of 6,000 atoms, every 10th atom aligned (a device selection),
+def test_rmsd_per_group_many_frames_and_group_shapes(stride):
+    """wmd_rmsd_per_group with superposition, groups that are not one run of
+    consecutive atoms (the item kernel): 300 frames of 6,000 atoms, every
+    10th atom aligned (a device selection),
     groups covering every atom -- ten-atom runs, one group of 2,500 atoms
     (larger than a 2,048-position tile) and one scattered group -- against
     the oracle's RmsdPerResPlan restatement (rms.rs:431-686) within 1e-5 A."""
@@ -195,6 +196,57 @@ def test_rmsd_per_group_one_pass_many_frames_and_group_shapes(stride):
         got = out.cpu().numpy()
         np.testing.assert_allclose(got, want, rtol=0, atol=1e-5)
         assert np.abs(got[5]).max() < 1e-5  # the frame equal to the reference
+    finally:
+        gref.close()
+        rr.close()
+
+
+@pytest.mark.parametrize("stride", [3, 4])
+def test_rmsd_per_group_contiguous_groups_edges(stride):
+    """Groups that cover consecutive atoms (no index load per position):
+    residues of 1 to 30 atoms, empty groups, one group of 2,100 atoms (larger
+    than a 2,048-position block, walked in tiles), an odd atom count and a frame
+    base 4 bytes off 16-byte alignment, with and without superposition, against
+    the oracle within 1e-5 A + 1.2e-7 relative (one float32 ulp: values reach
+    ~260 A without superposition)."""
+    from warp_md import _native as N
+
+    ctx = N.context(0)
+    n, F = 7001, 257
+    fr, ref = synth.make_trajectory(n, F, (0.1, 2.0), 29)
+    fr[3] = ref
+    rng = np.random.default_rng(4)
+    sizes, left = [], n
+    while left > 0:
+        k = 2100 if len(sizes) == 40 else (0 if len(sizes) % 17 == 5 else int(rng.integers(1, 31)))
+        k = min(k, left)
+        sizes.append(k)
+        left -= k
+    goff = np.zeros(len(sizes) + 1, np.uint32)
+    goff[1:] = np.cumsum(sizes)
+    assert goff[-1] == n and 2100 in sizes and 0 in sizes
+    groups = [np.arange(goff[i], goff[i + 1]) for i in range(len(sizes))]
+    data = fr if stride == 3 else np.concatenate([fr, np.ones(fr.shape[:2] + (1,), np.float32)], axis=2)
+    flat = torch.zeros(data.size + 1, device="cuda")
+    flat[1:] = torch.from_numpy(np.ascontiguousarray(data)).reshape(-1).cuda()
+    x = flat[1:]
+    assert x.data_ptr() % 16 == 4
+    sel = np.arange(0, n, 7, dtype=np.uint32)
+    rr = N.Reference.from_numpy(ctx, ref[sel])
+    gref = N.GroupRef(ctx, ref, goff, np.arange(n, dtype=np.uint32))
+    dsel = torch.from_numpy(sel.astype(np.int32)).cuda()
+    try:
+        for align in (1, 0):
+            out = torch.full((F, len(sizes)), -1.0, device="cuda")
+            ctx.check(ctx.lib.wmd_rmsd_per_group(ctx.handle, x.data_ptr(), F, n, stride, dsel.data_ptr(), sel.size,
+                                                 rr.handle, gref.handle, align, out.data_ptr(), None))
+            torch.cuda.synchronize()
+            got = out.cpu().numpy()
+            want = oracle.rmsd_perres(fr, ref, groups, selection=sel, align=bool(align))
+            np.testing.assert_allclose(got, want, rtol=1.2e-7, atol=1e-5, err_msg=str(align))
+            assert np.all(got[:, np.array(sizes) == 0] == 0.0)
+            if align:
+                assert np.abs(got[3]).max() < 1e-5
     finally:
         gref.close()
         rr.close()
