@@ -237,3 +237,34 @@ def test_batched_many_uneven_trajectories():
         _check_rmsd(b, xs, ys)
         _check_grad(b, xs, ys)
         b.close()
+
+
+@pytest.mark.parametrize("tile", [512, 1024])
+def test_batched_lanes_tensor_maps_match_per_lane_copies(tile):
+    """The lanes layout's forward reads each trajectory through its tensor map:
+    frame rows when a frame is a multiple of 16 bytes, quad rows otherwise
+    (the last n_frames mod 4 frames by plain loads), per-lane bulk copies for
+    fewer than 4 frames.  Every lane adds its atoms in the same order either
+    way, so RMSDs and gradients equal those of WARPMD_BATCHED_TMA=0 bit for
+    bit, and the oracle's within the usual bars."""
+    shapes = [(1000, 37), (1001, 70), (1002, 101), (1003, 66), (999, 3), (4, 33), (3, 9), (2050, 44), (2053, 35),
+              (33, 64), (5, 4)]
+    xs, ys = _batch(shapes, 77)
+    old = os.environ.get("WARPMD_BATCHED_TMA")
+    try:
+        os.environ["WARPMD_BATCHED_TMA"] = "0"
+        plain = _run(xs, ys, with_grad=True, tile=tile, layout="lanes")
+        os.environ.pop("WARPMD_BATCHED_TMA")
+        mapped = _run(xs, ys, with_grad=True, tile=tile, layout="lanes")
+    finally:
+        if old is None:
+            os.environ.pop("WARPMD_BATCHED_TMA", None)
+        else:
+            os.environ["WARPMD_BATCHED_TMA"] = old
+    _check_rmsd(mapped, xs, ys)
+    _check_grad(mapped, xs, ys)
+    for k in range(len(shapes)):
+        assert torch.equal(mapped.rmsd[k], plain.rmsd[k]), k
+        assert torch.equal(mapped.grads[k], plain.grads[k]), k
+    plain.close()
+    mapped.close()

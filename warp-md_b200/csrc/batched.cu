@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -825,21 +826,43 @@ __global__ void __launch_bounds__(kThreads, 4) batched_frame_kernel(const BatchL
 // ---------------------------------------------------------------------------
 // Lanes layout forward: units (trajectory, atom tile, 32-frame group); lane l
 // of a warp accumulates frame 32g + l over the tile, in FP64 and in atom
-// order, and stores the item partial (tile, frame) the finisher reads.  Per
-// stage (32 atoms) every lane bulk-copies its own frame's row (the 16-byte
-// hull of 32 atoms, at most 400 bytes, any atom count) and lane 0 the 32
-// reference atoms; the barrier of a stage counts 32 arrivals.  Warps take
-// contiguous runs of units of equal estimated cost.
+// order, and stores the item partial (tile, frame) the finisher reads.  A
+// stage is 32 atoms of the group's 32 frames plus the 32 reference atoms
+// (FP64, centred; a 1-D bulk copy by lane 0), and its barrier counts 32
+// arrivals.  The frames arrive by the trajectory's 2-D tensor map
+// (batched_encode_maps), lane 0 issuing every box:
+//   frame rows (tma = 1): 3 boxes of [32 frames x 32 floats], 128-byte
+//       swizzle, so that the 32 lanes reading their own rows hit distinct
+//       bank groups -- the layout of the single-trajectory lanes kernel;
+//   quad rows (tma = 2): 4 boxes of [8 quad rows x 100 floats], box j holding
+//       frame position j of quad rows 8g .. 8g + 7 from the 16-byte boundary
+//       at or below the stage's first atom; lane 4i + j reads row i of box j
+//       at a fixed float offset.  Lanes of the last n_frames mod 4 frames
+//       (past the last whole quad row) read their atoms with plain loads.
+// Without a map (tma = 0) every lane bulk-copies its own frame's row, the
+// 16-byte hull of 32 atoms (at most 400 bytes).  Warps take contiguous runs
+// of units of equal estimated cost.
 // ---------------------------------------------------------------------------
 constexpr int kBLWarps = 4;
 constexpr int kBLStages = 2;
-constexpr int kBLRow = 400;  // bytes per frame row of a stage
-constexpr int kBLXBytes = 32 * kBLRow;
+constexpr int kBLRow = 400;                // bytes per frame row of a per-lane stage
+constexpr int kBLXBytes = 32 * kBLRow;     // 12,800: per-lane rows, or 4 quad boxes; 3 swizzled boxes take 12,288
+constexpr int kBLQuadBox = 8 * kBLRow;     // [8 quad rows x 100 floats]
+constexpr int kBLXStage = 13312;           // a frame slot, a multiple of 1024 bytes (128-byte swizzle)
 constexpr int kBLYBytes = 32 * 3 * 8;
-constexpr int kBLStageBytes = kBLXBytes + kBLYBytes;
-constexpr int kBLBarOffset = kBLWarps * kBLStages * kBLStageBytes;
+constexpr int kBLYOffset = kBLWarps * kBLStages * kBLXStage;
+constexpr int kBLBarOffset = kBLYOffset + kBLWarps * kBLStages * kBLYBytes;
 constexpr int kBLAbortOffset = kBLBarOffset + kBLWarps * kBLStages * 8;
-constexpr int kBLSmemBytes = kBLAbortOffset + 16;
+constexpr int kBLSmemBytes = kBLAbortOffset + 16 + 1024;  // + slack to align the base to 1024
+static_assert(kBLXBytes <= kBLXStage && 3 * 4096 <= kBLXStage && 4 * kBLQuadBox <= kBLXStage, "frame slot");
+
+__device__ __forceinline__ void bl_tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
 
 // last segment whose units start at or before cost c
 __device__ __forceinline__ int lane_seg_of(const BatchSeg* segs, int n, int64_t c) {
@@ -867,12 +890,14 @@ __device__ __forceinline__ void lane_skip_empty(const BatchLaunch& B, LaneCur& c
 template <int APT>
 __global__ void __launch_bounds__(kBLWarps * 32) batched_lanes_kernel(const BatchLaunch B) {
   constexpr int T = kConsumerThreads * APT;
-  extern __shared__ __align__(128) unsigned char smem[];
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem = smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kBLBarOffset);
   uint64_t* full = bars + warp * kBLStages;
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + kBLAbortOffset);
-  unsigned char* ring = smem + warp * kBLStages * kBLStageBytes;
+  unsigned char* ring = smem + warp * kBLStages * kBLXStage;
+  unsigned char* yring = smem + kBLYOffset + warp * kBLStages * kBLYBytes;
   if (threadIdx.x == 0) {
     for (int i = 0; i < kBLWarps * kBLStages; ++i) mbar_init(&bars[i], 32);
     *abort_flag = 0;
@@ -913,32 +938,53 @@ __global__ void __launch_bounds__(kBLWarps * 32) batched_lanes_kernel(const Batc
     const int64_t a0 = t * T + (int64_t)pj * 32;
     const int nv = (int)min((int64_t)32, S.n_atoms - a0);
     const int slot = (int)(n_issued % kBLStages);
-    unsigned char* st = ring + slot * kBLStageBytes;
+    unsigned char* st = ring + slot * kBLXStage;
+    unsigned char* ys = yring + slot * kBLYBytes;
     unsigned char* dst = st + lane * kBLRow;
     const int64_t f = g * 32 + lane;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    uint32_t bytes = 0;
-    uint64_t c0 = 0;
-    const unsigned char* base = reinterpret_cast<const unsigned char*>(S.coords);
-    if (f < S.n_frames) {
-      const uint64_t total_al = ((uint64_t)S.n_frames * (uint64_t)S.n_atoms * 12ull) & ~15ull;
-      const uint64_t b0 = (uint64_t)(f * S.n_atoms + a0) * 12ull;
-      const uint64_t b1 = b0 + (uint64_t)nv * 12ull;
-      c0 = b0 & ~15ull;
-      uint64_t c1 = (b1 + 15ull) & ~15ull;
-      if (c1 > total_al) {  // the array's unaligned tail: plain loads
-        const uint64_t tail0 = total_al > c0 ? total_al : c0;
-        for (uint64_t bb = tail0; bb < b1; bb += 4)
-          *reinterpret_cast<float*>(dst + (bb - c0)) = __ldg(reinterpret_cast<const float*>(base + bb));
-        c1 = tail0;
+    if (S.tma) {
+      if (lane == 0) {
+        const CUtensorMap* map = B.maps + pc.seg;
+        mbar_arrive_expect_tx(&full[slot], (S.tma == 1 ? 3 * 4096 : 4 * kBLQuadBox) + kBLYBytes);
+        if (S.tma == 1) {
+#pragma unroll
+          for (int b = 0; b < 3; ++b) bl_tma_load_2d(st + b * 4096, map, (int)(a0 * 3 + 32 * b), (int)(g * 32), &full[slot]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int64_t e = (int64_t)j * 3 * S.n_atoms + 3 * a0;
+            bl_tma_load_2d(st + j * kBLQuadBox, map, (int)(e & ~int64_t(3)), (int)(g * 8), &full[slot]);
+          }
+        }
+        bulk_copy_g2s(ys, S.yc + a0 * 3, kBLYBytes, &full[slot]);
+      } else {
+        mbar_arrive(&full[slot]);
       }
-      bytes = (uint32_t)(c1 - c0);
+    } else {
+      uint32_t bytes = 0;
+      uint64_t c0 = 0;
+      const unsigned char* base = reinterpret_cast<const unsigned char*>(S.coords);
+      if (f < S.n_frames) {
+        const uint64_t total_al = ((uint64_t)S.n_frames * (uint64_t)S.n_atoms * 12ull) & ~15ull;
+        const uint64_t b0 = (uint64_t)(f * S.n_atoms + a0) * 12ull;
+        const uint64_t b1 = b0 + (uint64_t)nv * 12ull;
+        c0 = b0 & ~15ull;
+        uint64_t c1 = (b1 + 15ull) & ~15ull;
+        if (c1 > total_al) {  // the array's unaligned tail: plain loads
+          const uint64_t tail0 = total_al > c0 ? total_al : c0;
+          for (uint64_t bb = tail0; bb < b1; bb += 4)
+            *reinterpret_cast<float*>(dst + (bb - c0)) = __ldg(reinterpret_cast<const float*>(base + bb));
+          c1 = tail0;
+        }
+        bytes = (uint32_t)(c1 - c0);
+      }
+      const uint32_t tx = bytes + (lane == 0 ? (uint32_t)kBLYBytes : 0u);
+      if (tx) mbar_arrive_expect_tx(&full[slot], tx);
+      else mbar_arrive(&full[slot]);
+      if (bytes) bulk_copy_g2s(dst, base + c0, bytes, &full[slot]);
+      if (lane == 0) bulk_copy_g2s(ys, S.yc + a0 * 3, kBLYBytes, &full[slot]);
     }
-    const uint32_t tx = bytes + (lane == 0 ? (uint32_t)kBLYBytes : 0u);
-    if (tx) mbar_arrive_expect_tx(&full[slot], tx);
-    else mbar_arrive(&full[slot]);
-    if (bytes) bulk_copy_g2s(dst, base + c0, bytes, &full[slot]);
-    if (lane == 0) bulk_copy_g2s(st + kBLXBytes, S.yc + a0 * 3, kBLYBytes, &full[slot]);
     ++n_issued;
     if (++pj == p_st) {
       pj = 0;
@@ -960,6 +1006,10 @@ __global__ void __launch_bounds__(kBLWarps * 32) batched_lanes_kernel(const Batc
     const int st_n = unit_stages(cu);
     const int64_t f = g * 32 + lane;
     const bool live = f < S.n_frames;
+    // quad rows: this lane's float offset into its box row; lanes past the
+    // last whole quad row read from global memory
+    const int quad_off = (int)(((int64_t)(lane & 3) * 3 * S.n_atoms) & 3);
+    const bool quad_tail = S.tma == 2 && f >= (S.n_frames & ~int64_t(3));
     double acc[15];
 #pragma unroll
     for (int e = 0; e < 15; ++e) acc[e] = 0.0;
@@ -972,21 +1022,44 @@ __global__ void __launch_bounds__(kBLWarps * 32) batched_lanes_kernel(const Batc
       }
       const int64_t a0 = t * T + (int64_t)j * 32;
       const int nv = (int)min((int64_t)32, S.n_atoms - a0);
-      const unsigned char* st = ring + slot * kBLStageBytes;
-      const double* ys = reinterpret_cast<const double*>(st + kBLXBytes);
-      if (live) {
-        const int head = (int)(((uint64_t)(f * S.n_atoms + a0) * 12ull) & 15ull);
-        const float* xr = reinterpret_cast<const float*>(st + lane * kBLRow + head);
-#pragma unroll 4
-        for (int a = 0; a < nv; ++a) {
-          const double x0 = xr[3 * a], x1 = xr[3 * a + 1], x2 = xr[3 * a + 2];
-          const double y0 = ys[3 * a], y1 = ys[3 * a + 1], y2 = ys[3 * a + 2];
-          acc[0] += x0; acc[1] += x1; acc[2] += x2;
-          acc[3] = fma(x0, x0, acc[3]); acc[4] = fma(x1, x1, acc[4]); acc[5] = fma(x2, x2, acc[5]);
-          acc[6] = fma(x0, y0, acc[6]);  acc[7] = fma(x0, y1, acc[7]);  acc[8] = fma(x0, y2, acc[8]);
-          acc[9] = fma(x1, y0, acc[9]);  acc[10] = fma(x1, y1, acc[10]); acc[11] = fma(x1, y2, acc[11]);
-          acc[12] = fma(x2, y0, acc[12]); acc[13] = fma(x2, y1, acc[13]); acc[14] = fma(x2, y2, acc[14]);
+      const unsigned char* st = ring + slot * kBLXStage;
+      const double* ys = reinterpret_cast<const double*>(yring + slot * kBLYBytes);
+      auto add = [&](double x0, double x1, double x2, int a) {
+        const double y0 = ys[3 * a], y1 = ys[3 * a + 1], y2 = ys[3 * a + 2];
+        acc[0] += x0; acc[1] += x1; acc[2] += x2;
+        acc[3] = fma(x0, x0, acc[3]); acc[4] = fma(x1, x1, acc[4]); acc[5] = fma(x2, x2, acc[5]);
+        acc[6] = fma(x0, y0, acc[6]);  acc[7] = fma(x0, y1, acc[7]);  acc[8] = fma(x0, y2, acc[8]);
+        acc[9] = fma(x1, y0, acc[9]);  acc[10] = fma(x1, y1, acc[10]); acc[11] = fma(x1, y2, acc[11]);
+        acc[12] = fma(x2, y0, acc[12]); acc[13] = fma(x2, y1, acc[13]); acc[14] = fma(x2, y2, acc[14]);
+      };
+      if (live && S.tma == 1) {
+        // 4 atoms = 3 swizzled 16-byte chunks of this lane's 128-byte row in each box
+        const unsigned char* row = st + lane * 128;
+        const int sw = lane & 7;
+        auto chunk = [&](int c) -> float4 {
+          return *reinterpret_cast<const float4*>(row + (c >> 3) * 4096 + (((c & 7) ^ sw) << 4));
+        };
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+          if (4 * m >= nv) break;
+          const float4 p = chunk(3 * m), q = chunk(3 * m + 1), r = chunk(3 * m + 2);
+          add(p.x, p.y, p.z, 4 * m);
+          if (4 * m + 1 < nv) add(p.w, q.x, q.y, 4 * m + 1);
+          if (4 * m + 2 < nv) add(q.z, q.w, r.x, 4 * m + 2);
+          if (4 * m + 3 < nv) add(r.y, r.z, r.w, 4 * m + 3);
         }
+      } else if (live) {
+        const float* xr;
+        if (S.tma == 2 && !quad_tail) {
+          xr = reinterpret_cast<const float*>(st + (lane & 3) * kBLQuadBox + (lane >> 2) * kBLRow) + quad_off;
+        } else if (S.tma == 2) {
+          xr = S.coords + ((size_t)f * S.n_atoms + a0) * 3;
+        } else {
+          const int head = (int)(((uint64_t)(f * S.n_atoms + a0) * 12ull) & 15ull);
+          xr = reinterpret_cast<const float*>(st + lane * kBLRow + head);
+        }
+#pragma unroll 4
+        for (int a = 0; a < nv; ++a) add(xr[3 * a], xr[3 * a + 1], xr[3 * a + 2], a);
       }
       ++n_done;
       __syncwarp();
@@ -1087,6 +1160,51 @@ int occupancy_of() {
 }
 
 }  // namespace
+
+bool batched_encode_maps(std::vector<BatchSeg>& segs, CUtensorMap* maps, std::string* msg) {
+  using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static EncodeTiled enc = nullptr;
+  const char* env = std::getenv("WARPMD_BATCHED_TMA");
+  const bool off = env && std::strcmp(env, "0") == 0;
+  for (BatchSeg& g : segs) g.tma = 0;
+  if (off) return true;
+  if (!enc) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !p) {
+      cudaGetLastError();
+      *msg = "cuda driver error: cuTensorMapEncodeTiled unavailable";
+      return false;
+    }
+    enc = reinterpret_cast<EncodeTiled>(p);
+  }
+  for (size_t i = 0; i < segs.size(); ++i) {
+    BatchSeg& g = segs[i];
+    std::memset(&maps[i], 0, sizeof(CUtensorMap));
+    const int64_t n = g.n_atoms, F = g.n_frames;
+    if (n <= 0 || F < 4 || !g.coords) continue;
+    const bool rows = n % 4 == 0;
+    const cuuint64_t dims[2] = {(cuuint64_t)(rows ? 3 * n : 12 * n), (cuuint64_t)(rows ? F : F / 4)};
+    const cuuint64_t stride[1] = {(cuuint64_t)(rows ? 12 * n : 48 * n)};
+    const cuuint32_t box[2] = {rows ? 32u : 100u, rows ? 32u : 8u};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = enc(&maps[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(g.coords), dims, stride, box,
+                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           rows ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+      *msg = "cuda driver error: tensor map of batched trajectory " + std::to_string(i) + " (CUresult " +
+             std::to_string((int)r) + ", " + std::to_string((long long)n) + " atoms, " + std::to_string((long long)F) +
+             " frames)";
+      return false;
+    }
+    g.tma = rows ? 1 : 2;
+  }
+  return true;
+}
 
 int batched_tile_atoms(int apt) { return kConsumerThreads * apt; }
 

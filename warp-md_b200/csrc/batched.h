@@ -1,9 +1,12 @@
 // batched.h -- batched per-frame RMSD over many trajectories (internal).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <string>
+#include <vector>
 
 namespace wmd {
 
@@ -27,6 +30,7 @@ struct BatchSeg {
   int64_t lane_cost0;      //   estimated cost of all units before this trajectory's
   int n_tiles;
   int m_group;          //   frames per group
+  int tma;              // lanes layout forward: 0 per-lane bulk copies, 1 frame rows, 2 quad rows (tensor map)
   double sum_c[3];      // sum of y_c, written on the device each call
   double gy;            // G_y, written on the device each call
   double mean_y[3];     // mean of the reference, written on the device each call
@@ -34,6 +38,7 @@ struct BatchSeg {
 
 struct BatchLaunch {
   const BatchSeg* segs = nullptr;
+  const CUtensorMap* maps = nullptr;  // [n_segs] lanes layout: each trajectory's frames as a 2-D tensor map
   int n_segs = 0;
   int64_t total_items = 0;
   int64_t total_frames = 0;
@@ -76,6 +81,16 @@ constexpr int kGroupFrames = 16;
 constexpr int kGroupBytes = 64 * 1024;
 constexpr int64_t kCostItem = 4;
 constexpr int64_t kCostFinish = 24;
+
+// Tensor maps of the lanes layout's forward pass, one per trajectory (64-byte
+// aligned host array): frame rows [n_frames][3 n_atoms] floats in 32-row x
+// 32-float boxes with 128-byte swizzle when a frame is a multiple of 16 bytes
+// (tma = 1), else quad rows [n_frames / 4][12 n_atoms] in 8-row x 100-float
+// boxes (tma = 2; the last n_frames mod 4 frames are read with plain loads).
+// Trajectories with fewer than 4 frames, no atoms, or with
+// WARPMD_BATCHED_TMA=0, keep per-lane bulk copies (tma = 0).  Returns false
+// with *msg set when the driver's encoder is unavailable or refuses a map.
+bool batched_encode_maps(std::vector<BatchSeg>& segs, CUtensorMap* maps, std::string* msg);
 
 int batched_tile_atoms(int apt);
 int batched_grid(int apt, bool backward, int sm_count, int64_t items);

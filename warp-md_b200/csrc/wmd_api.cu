@@ -114,7 +114,7 @@ struct wmd_ctx {
   std::string err;
   wmd::PairwiseWorkspace pw;
   // batched launch prepared by wmd_batched_prepare
-  DevBuf b_segs, b_yc, b_partial, b_rot, b_refine, b_count;
+  DevBuf b_segs, b_yc, b_partial, b_rot, b_refine, b_count, b_maps;
   std::vector<wmd_batch_desc> b_descs;
   bool b_grad = false;
   bool b_ready = false;
@@ -520,7 +520,7 @@ WMD_EXPORT int wmd_destroy(wmd_ctx* ctx) {
   cudaDeviceSynchronize();
   for (DevBuf* b : {&ctx->partial, &ctx->refine, &ctx->refine_count, &ctx->rot, &ctx->chunk[0], &ctx->chunk[1], &ctx->out_tmp,
                     &ctx->sel_buf, &ctx->aux, &ctx->out_chunk, &ctx->fl_part, &ctx->fl_acc, &ctx->fl_shift, &ctx->cl_mat, &ctx->cl_scratch,
-                    &ctx->cl_out, &ctx->km_feat, &ctx->km_xf, &ctx->km_work, &ctx->lane_exp, &ctx->vg_stats, &ctx->b_segs, &ctx->b_yc, &ctx->b_partial, &ctx->b_rot,
+                    &ctx->cl_out, &ctx->km_feat, &ctx->km_xf, &ctx->km_work, &ctx->lane_exp, &ctx->vg_stats, &ctx->b_segs, &ctx->b_maps, &ctx->b_yc, &ctx->b_partial, &ctx->b_rot,
                     &ctx->b_refine, &ctx->b_count})
     if (b->ptr) cudaFree(b->ptr);
   for (HostBuf* b : {&ctx->stage[0], &ctx->stage[1]})
@@ -1806,6 +1806,16 @@ WMD_EXPORT int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, in
   const int64_t items8 = build_segs(d, 8, yc, with_grad != 0, s8, &frames8, &groups8, &cost8, &lcost8);
   const int64_t frames = frames4;
   const size_t rec = wmd::kStatDoubles * sizeof(double);
+  // the lanes layout's tensor maps (one per trajectory; the same for both tile shapes)
+  {
+    std::vector<CUtensorMap> maps((size_t)std::max(n_traj, 1));
+    std::string msg;
+    if (!wmd::batched_encode_maps(s8, maps.data(), &msg)) return set_err(ctx, WMD_ERR_CUDA, "%s", msg.c_str());
+    for (size_t i = 0; i < s4.size(); ++i) s4[i].tma = s8[i].tma;
+    if ((rc = ensure(ctx, ctx->b_maps, maps.size() * sizeof(CUtensorMap)))) return rc;
+    CU(cudaMemcpy(ctx->b_maps.ptr, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice),
+       "upload tensor maps");
+  }
   if ((rc = ensure(ctx, ctx->b_segs, std::max<size_t>(1, (size_t)n_traj) * sizeof(wmd::BatchSeg))) ||
       (rc = ensure(ctx, ctx->b_partial, (size_t)std::max<int64_t>(1, std::max(items4, items8)) * rec)) ||
       (rc = ensure(ctx, ctx->b_refine, (size_t)std::max<int64_t>(1, frames) * rec)) ||
@@ -1816,6 +1826,7 @@ WMD_EXPORT int wmd_batched_prepare(wmd_ctx* ctx, const wmd_batch_desc* descs, in
   P.n_segs = n_traj;
   P.segs_dev = static_cast<wmd::BatchSeg*>(ctx->b_segs.ptr);
   P.launch.segs = P.segs_dev;
+  P.launch.maps = static_cast<const CUtensorMap*>(ctx->b_maps.ptr);
   P.launch.n_segs = n_traj;
   P.launch.total_frames = frames;
   P.launch.partial = static_cast<double*>(ctx->b_partial.ptr);
