@@ -1159,6 +1159,9 @@ def run_profile_case(name):
     perres: per-residue RMSD of 100,000 atoms x 2,000 frames (2.4 GB), residues
           of 10 consecutive atoms, every 10th atom superposed: 3 calls of
           wmd_rmsd_per_group.
+    batched: 24 trajectories drawn like the batched workload's (atoms
+          log-uniform 50-20,000, frames uniform 50-2,500), lanes layout with
+          1,024-atom tiles, forward + gradients, 3 runs.
     """
     import numpy as np
     import torch
@@ -1208,10 +1211,32 @@ def run_profile_case(name):
                                                  r.handle, gref.handle, 1, out.data_ptr(), None))
         torch.cuda.synchronize()
         gref.close()
+    elif name == "batched":
+        from warp_md.batched import BatchedRmsd
+
+        os.environ["WARPMD_BATCHED_LAYOUT"] = "lanes"
+        os.environ["WARPMD_BATCHED_TILE_ATOMS"] = "1024"
+        rng = np.random.default_rng(2024)
+        T = 24
+        atoms = np.exp(rng.uniform(np.log(50), np.log(20000), T)).astype(np.int64)
+        frames = np.maximum(1, rng.integers(100, 5001, T) // 2).astype(np.int64)
+        xs, ys = [], []
+        for k in range(T):
+            x, y = synth.make_trajectory_torch(int(atoms[k]), int(frames[k]), 0.5, seed=100_000 + k, device="cuda",
+                                               chunk=max(1, (64 << 20) // (24 * int(atoms[k]))))
+            xs.append(x)
+            ys.append(y)
+        b = BatchedRmsd(xs, ys, with_grad=True)
+        for _ in range(3):
+            b.run()
+        torch.cuda.synchronize()
+        b.close()
+        r = None
     else:
         raise SystemExit(f"unknown profile case {name!r}")
     torch.cuda.synchronize()
-    r.close()
+    if r is not None:
+        r.close()
     print(f"profile case {name}: ok", flush=True)
     return 0
 
@@ -1253,7 +1278,7 @@ def main():
     ap.add_argument("--dcd-frames", type=int, default=2000)
     ap.add_argument("--dcd-steps", type=int, default=5)
     ap.add_argument("--dcd-cpu-frames", type=int, default=100)
-    ap.add_argument("--profile-case", choices=["vg", "quad", "perres"], help="run one small kernel case for ncu and exit")
+    ap.add_argument("--profile-case", choices=["vg", "quad", "perres", "batched"], help="run one small kernel case for ncu and exit")
     args = ap.parse_args()
     if args.profile_case:
         return run_profile_case(args.profile_case)

@@ -880,6 +880,37 @@ struct LaneCur {
   int64_t k;  // unit within the segment
 };
 
+// The fields of a trajectory the lanes kernel reads per stage and per unit,
+// held in registers while a cursor stays in that trajectory.
+struct LaneSeg {
+  const float* coords;
+  const double* yc;
+  int64_t n_atoms, n_frames, groups, item0;
+  int64_t cost0, full_units, unit_cost, last_cost;
+  int tma;
+};
+
+__device__ __forceinline__ LaneSeg lane_seg(const BatchSeg& S) {
+  LaneSeg v;
+  v.coords = S.coords;
+  v.yc = S.yc;
+  v.n_atoms = S.n_atoms;
+  v.n_frames = S.n_frames;
+  v.groups = (S.n_frames + 31) / 32;
+  v.item0 = S.item0;
+  v.cost0 = S.lane_cost0;
+  v.full_units = S.lane_full_units;
+  v.unit_cost = S.lane_unit_cost;
+  v.last_cost = S.lane_last_cost;
+  v.tma = S.tma;
+  return v;
+}
+
+// a unit's starting cost: whole-tile units first, then the last tile's
+__device__ __forceinline__ int64_t lane_unit_start(const LaneSeg& v, int64_t k) {
+  return v.cost0 + (k <= v.full_units ? k * v.unit_cost : v.full_units * v.unit_cost + (k - v.full_units) * v.last_cost);
+}
+
 __device__ __forceinline__ void lane_skip_empty(const BatchLaunch& B, LaneCur& c) {
   while (c.seg < B.n_segs && c.k >= B.segs[c.seg].lane_units) {
     ++c.seg;
@@ -913,61 +944,71 @@ __global__ void __launch_bounds__(kBLWarps * 32) batched_lanes_kernel(const Batc
   {
     const BatchSeg& S = B.segs[first.seg];
     const int64_t off = C0 - S.lane_cost0;
-    first.k = S.lane_units > 0 ? (off + S.lane_unit_cost - 1) / S.lane_unit_cost : 0;
+    const int64_t full = S.lane_full_units * S.lane_unit_cost;
+    if (S.lane_units <= 0) first.k = 0;
+    else if (off <= full) first.k = (off + S.lane_unit_cost - 1) / S.lane_unit_cost;
+    else first.k = S.lane_full_units + (off - full + S.lane_last_cost - 1) / S.lane_last_cost;
   }
   lane_skip_empty(B, first);
-  auto starts_before_end = [&](const LaneCur& c) {
-    return c.seg < B.n_segs && B.segs[c.seg].lane_cost0 + c.k * B.segs[c.seg].lane_unit_cost < C1;
+  // a cursor's trajectory view, reloaded when the cursor enters another trajectory
+  auto view = [&](const LaneCur& c, int& vseg, LaneSeg& v) {
+    if (c.seg < B.n_segs && c.seg != vseg) {
+      v = lane_seg(B.segs[c.seg]);
+      vseg = c.seg;
+    }
   };
-  auto unit_stages = [&](const LaneCur& c) {
-    const BatchSeg& S = B.segs[c.seg];
-    const int64_t groups = (S.n_frames + 31) / 32;
-    const int64_t t = c.k / groups;
-    return (int)((min((int64_t)T, S.n_atoms - t * T) + 31) / 32);
+  auto starts_before_end = [&](const LaneCur& c, const LaneSeg& v) {
+    return c.seg < B.n_segs && lane_unit_start(v, c.k) < C1;
   };
-  // producer cursor: unit pc, stage pj; every lane runs it (warp-uniform)
+  auto unit_stages = [&](const LaneCur& c, const LaneSeg& v) {
+    const int64_t t = c.k / v.groups;
+    return (int)((min((int64_t)T, v.n_atoms - t * T) + 31) / 32);
+  };
+  // producer cursor: unit pc (tile pt, frame group pg), stage pj; every lane runs it (warp-uniform)
   LaneCur pc = first;
+  int pv_seg = -1;
+  LaneSeg pv;
+  view(pc, pv_seg, pv);
   int pj = 0;
-  bool p_live = starts_before_end(pc);
-  int p_st = p_live ? unit_stages(pc) : 0;
+  bool p_live = starts_before_end(pc, pv);
+  int p_st = p_live ? unit_stages(pc, pv) : 0;
+  int64_t pt = p_live ? pc.k / pv.groups : 0, pg = p_live ? pc.k - pt * pv.groups : 0;
   int64_t n_issued = 0;
   auto issue_next = [&]() {
-    const BatchSeg& S = B.segs[pc.seg];
-    const int64_t groups = (S.n_frames + 31) / 32;
-    const int64_t t = pc.k / groups, g = pc.k - t * groups;
+    const int64_t t = pt, g = pg;
     const int64_t a0 = t * T + (int64_t)pj * 32;
-    const int nv = (int)min((int64_t)32, S.n_atoms - a0);
+    const int nv = (int)min((int64_t)32, pv.n_atoms - a0);
     const int slot = (int)(n_issued % kBLStages);
     unsigned char* st = ring + slot * kBLXStage;
     unsigned char* ys = yring + slot * kBLYBytes;
     unsigned char* dst = st + lane * kBLRow;
     const int64_t f = g * 32 + lane;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    if (S.tma) {
+    if (pv.tma) {
       if (lane == 0) {
         const CUtensorMap* map = B.maps + pc.seg;
-        mbar_arrive_expect_tx(&full[slot], (S.tma == 1 ? 3 * 4096 : 4 * kBLQuadBox) + kBLYBytes);
-        if (S.tma == 1) {
+        mbar_arrive_expect_tx(&full[slot], (pv.tma == 1 ? 3 * 4096 : 4 * kBLQuadBox) + kBLYBytes);
+        if (pv.tma == 1) {
 #pragma unroll
           for (int b = 0; b < 3; ++b) bl_tma_load_2d(st + b * 4096, map, (int)(a0 * 3 + 32 * b), (int)(g * 32), &full[slot]);
         } else {
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
-            const int64_t e = (int64_t)j * 3 * S.n_atoms + 3 * a0;
+            const int64_t e = (int64_t)j * 3 * pv.n_atoms + 3 * a0;
             bl_tma_load_2d(st + j * kBLQuadBox, map, (int)(e & ~int64_t(3)), (int)(g * 8), &full[slot]);
           }
         }
-        bulk_copy_g2s(ys, S.yc + a0 * 3, kBLYBytes, &full[slot]);
+        bulk_copy_g2s(ys, pv.yc + a0 * 3, kBLYBytes, &full[slot]);
       } else {
         mbar_arrive(&full[slot]);
       }
     } else {
       uint32_t bytes = 0;
       uint64_t c0 = 0;
-      const unsigned char* base = reinterpret_cast<const unsigned char*>(S.coords);
-      if (f < S.n_frames) {
-        const uint64_t total_al = ((uint64_t)S.n_frames * (uint64_t)S.n_atoms * 12ull) & ~15ull;
-        const uint64_t b0 = (uint64_t)(f * S.n_atoms + a0) * 12ull;
+      const unsigned char* base = reinterpret_cast<const unsigned char*>(pv.coords);
+      if (f < pv.n_frames) {
+        const uint64_t total_al = ((uint64_t)pv.n_frames * (uint64_t)pv.n_atoms * 12ull) & ~15ull;
+        const uint64_t b0 = (uint64_t)(f * pv.n_atoms + a0) * 12ull;
         const uint64_t b1 = b0 + (uint64_t)nv * 12ull;
         c0 = b0 & ~15ull;
         uint64_t c1 = (b1 + 15ull) & ~15ull;
@@ -983,15 +1024,22 @@ __global__ void __launch_bounds__(kBLWarps * 32) batched_lanes_kernel(const Batc
       if (tx) mbar_arrive_expect_tx(&full[slot], tx);
       else mbar_arrive(&full[slot]);
       if (bytes) bulk_copy_g2s(dst, base + c0, bytes, &full[slot]);
-      if (lane == 0) bulk_copy_g2s(ys, S.yc + a0 * 3, kBLYBytes, &full[slot]);
+      if (lane == 0) bulk_copy_g2s(ys, pv.yc + a0 * 3, kBLYBytes, &full[slot]);
     }
     ++n_issued;
     if (++pj == p_st) {
       pj = 0;
       ++pc.k;
       lane_skip_empty(B, pc);
-      p_live = starts_before_end(pc);
-      p_st = p_live ? unit_stages(pc) : 0;
+      view(pc, pv_seg, pv);
+      p_live = starts_before_end(pc, pv);
+      if (p_live) {
+        p_st = unit_stages(pc, pv);
+        pt = pc.k / pv.groups;
+        pg = pc.k - pt * pv.groups;
+      } else {
+        p_st = 0;
+      }
     }
   };
   while (p_live && n_issued < kBLStages) issue_next();
@@ -999,11 +1047,14 @@ __global__ void __launch_bounds__(kBLWarps * 32) batched_lanes_kernel(const Batc
   int64_t n_done = 0;
   bool aborted = false;
   LaneCur cu = first;
-  while (starts_before_end(cu) && !aborted) {
-    const BatchSeg& S = B.segs[cu.seg];
-    const int64_t groups = (S.n_frames + 31) / 32;
+  int cv_seg = -1;
+  LaneSeg cv;
+  view(cu, cv_seg, cv);
+  while (starts_before_end(cu, cv) && !aborted) {
+    const LaneSeg& S = cv;
+    const int64_t groups = S.groups;
     const int64_t t = cu.k / groups, g = cu.k - t * groups;
-    const int st_n = unit_stages(cu);
+    const int st_n = unit_stages(cu, cv);
     const int64_t f = g * 32 + lane;
     const bool live = f < S.n_frames;
     // quad rows: this lane's float offset into its box row; lanes past the
@@ -1074,6 +1125,7 @@ __global__ void __launch_bounds__(kBLWarps * 32) batched_lanes_kernel(const Batc
     }
     ++cu.k;
     lane_skip_empty(B, cu);
+    view(cu, cv_seg, cv);
   }
   // after an abort, copies this warp issued may still be landing
   if (aborted) {

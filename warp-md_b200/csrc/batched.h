@@ -25,7 +25,9 @@ struct BatchSeg {
   int64_t n_groups;     //   groups of this trajectory (m_group frames each, the last may be short)
   int64_t cost0;        //   estimated cost of all groups before this trajectory's
   int64_t group_cost;   //   estimated cost of one full group
-  int64_t lane_unit_cost;  // lanes layout: estimated cost of one (tile, 32-frame group) unit
+  int64_t lane_unit_cost;  // lanes layout: estimated cost of a (tile, 32-frame group) unit of a whole tile
+  int64_t lane_last_cost;  //   ... and of a unit of the last tile (the only one when n_atoms <= tile)
+  int64_t lane_full_units; //   units of the whole tiles, (n_tiles - 1) x ceil(n_frames / 32); tile-major
   int64_t lane_units;      //   units of this trajectory (n_tiles x ceil(n_frames / 32))
   int64_t lane_cost0;      //   estimated cost of all units before this trajectory's
   int n_tiles;

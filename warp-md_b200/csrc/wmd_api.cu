@@ -1723,18 +1723,23 @@ static int64_t build_segs(const std::vector<wmd_batch_desc>& d, int apt, double*
     g.n_tiles = (int)((d[i].n_atoms + tile - 1) / tile);
     g.yc = yc_base + yoff;
     yoff += batch_yc_doubles(d[i].n_atoms);
-    // lanes layout: (tile, 32-frame group) units; cost ~ atom-frames plus a
-    // per-stage overhead of about 8 atoms' work
+    // lanes layout: (tile, 32-frame group) units, tile-major; cost ~ the
+    // tile's atom-frames plus a per-stage overhead of about 8 atoms' work and a
+    // per-unit one of about a stage (the partial records); the last tile holds
+    // the remainder of the atoms
     g.lane_cost0 = lane_cost;
+    auto unit_cost = [](int64_t at) { return 32 * (at + 8 * ((at + 31) / 32) + 32); };
     if (g.n_atoms > 0 && g.n_frames > 0) {
-      g.lane_units = (int64_t)g.n_tiles * ((g.n_frames + 31) / 32);
-      const int64_t at = std::min<int64_t>(tile, g.n_atoms);
-      g.lane_unit_cost = 32 * (at + 8 * ((at + 31) / 32));
+      const int64_t groups_f = (g.n_frames + 31) / 32;
+      g.lane_units = (int64_t)g.n_tiles * groups_f;
+      g.lane_full_units = (int64_t)(g.n_tiles - 1) * groups_f;
+      g.lane_unit_cost = unit_cost(tile);
+      g.lane_last_cost = unit_cost(g.n_atoms - (int64_t)(g.n_tiles - 1) * tile);
     } else {
-      g.lane_units = 0;
-      g.lane_unit_cost = 1;
+      g.lane_units = g.lane_full_units = 0;
+      g.lane_unit_cost = g.lane_last_cost = 1;
     }
-    lane_cost += g.lane_units * g.lane_unit_cost;
+    lane_cost += g.lane_full_units * g.lane_unit_cost + (g.lane_units - g.lane_full_units) * g.lane_last_cost;
     g.item0 = items;
     g.frame0 = frames;
     items += (int64_t)g.n_tiles * g.n_frames;
