@@ -41,7 +41,9 @@ enum BMode : int { kBFwd = 0, kBBwd = 1 };
 template <int APT>
 struct BGeo {
   static constexpr int kTile = kConsumerThreads * APT;
-  static constexpr int kStageBytes = ((kTile * 3 * 4 + 32) + 127) / 128 * 128;
+  // the tile's 16-byte hull, then (gradient pass) the frame's 16-double rotation record
+  static constexpr int kRecOffset = ((kTile * 3 * 4 + 32) + 127) / 128 * 128;
+  static constexpr int kStageBytes = kRecOffset + kStatDoubles * 8;
   static constexpr int kStagesRaw = 51200 / kStageBytes;
   static constexpr int kStages = kStagesRaw < 3 ? 3 : (kStagesRaw > 8 ? 8 : kStagesRaw);
   static constexpr int kBarOffset = kStages * kStageBytes;
@@ -91,8 +93,11 @@ __device__ __forceinline__ void cursor_next(const BatchLaunch& B, Cursor& c) {
   }
 }
 
+// Copies item (t, f)'s coordinates into dst; with rot (the gradient pass) the
+// frame's rotation record too, to dst + kRecOffset.
 template <int APT>
-__device__ __forceinline__ void batched_issue(const BatchSeg& s, int t, int64_t f, unsigned char* dst, uint64_t* bar) {
+__device__ __forceinline__ void batched_issue(const BatchSeg& s, int t, int64_t f, unsigned char* dst, uint64_t* bar,
+                                              const double* rot) {
   constexpr int T = BGeo<APT>::kTile;
   const int64_t a0 = (int64_t)t * T;
   const int64_t a1 = min(s.n_atoms, a0 + T);
@@ -110,8 +115,9 @@ __device__ __forceinline__ void batched_issue(const BatchSeg& s, int t, int64_t 
   }
   const uint32_t core = (uint32_t)(c1 - c0);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  mbar_arrive_expect_tx(bar, core);
+  mbar_arrive_expect_tx(bar, core + (rot ? (uint32_t)(kStatDoubles * 8) : 0u));
   if (core) bulk_copy_g2s(dst, base + c0, core, bar);
+  if (rot) bulk_copy_g2s(dst + BGeo<APT>::kRecOffset, rot + (s.frame0 + f) * kStatDoubles, kStatDoubles * 8, bar);
 }
 
 template <int APT, int MODE>
@@ -137,10 +143,12 @@ __global__ void __launch_bounds__(kThreads, 4) batched_stream_kernel(const Batch
 
   Cursor pc;  // producer cursor (thread 0)
   int64_t issued = 0;
+  // the gradient pass stages each frame's rotation record with its coordinates
+  const double* rec_src = MODE == kBBwd ? B.rot : nullptr;
   if (tid == 0) {
     cursor_init(B, w0, pc);
     for (; issued < S - 1 && issued < n_items; ++issued) {
-      batched_issue<APT>(B.segs[pc.seg], pc.t, pc.f, smem + (issued % S) * G::kStageBytes, &full[issued % S]);
+      batched_issue<APT>(B.segs[pc.seg], pc.t, pc.f, smem + (issued % S) * G::kStageBytes, &full[issued % S], rec_src);
       cursor_next(B, pc);
     }
   }
@@ -155,7 +163,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_stream_kernel(const Batch
     // stage's gradient store has been issued (see below)
     if (MODE == kBFwd && tid == 0 && issued < n_items) {
       const int sp = (int)(issued % S);
-      batched_issue<APT>(B.segs[pc.seg], pc.t, pc.f, smem + sp * G::kStageBytes, &full[sp]);
+      batched_issue<APT>(B.segs[pc.seg], pc.t, pc.f, smem + sp * G::kStageBytes, &full[sp], rec_src);
       ++issued;
       cursor_next(B, pc);
     }
@@ -187,7 +195,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_stream_kernel(const Batch
       float* gs = const_cast<float*>(xs);
       const bool has_grad = sg.grad != nullptr;
       if (ok && has_grad) {
-        const double* rt = B.rot + (sg.frame0 + c.f) * kStatDoubles;
+        const double* rt = reinterpret_cast<const double*>(smem + s * G::kStageBytes + G::kRecOffset);
         double R[9], cc[3];
 #pragma unroll
         for (int e = 0; e < 9; ++e) R[e] = rt[e];
@@ -225,7 +233,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_stream_kernel(const Batch
         bulk_wait_read<1>();
         if (issued < n_items) {
           const int sp = (int)(issued % S);
-          batched_issue<APT>(B.segs[pc.seg], pc.t, pc.f, smem + sp * G::kStageBytes, &full[sp]);
+          batched_issue<APT>(B.segs[pc.seg], pc.t, pc.f, smem + sp * G::kStageBytes, &full[sp], rec_src);
           ++issued;
           cursor_next(B, pc);
         }
@@ -601,7 +609,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_frame_kernel(const BatchL
   auto issue = [&]() {
     const int sp = (int)(issued % S);
     const BatchSeg& ps = B.segs[pc.seg];
-    batched_issue<APT>(ps, pc.t, pc.gi * ps.m_group + pc.j, smem + sp * G::kStageBytes, &full[sp]);
+    batched_issue<APT>(ps, pc.t, pc.gi * ps.m_group + pc.j, smem + sp * G::kStageBytes, &full[sp], nullptr);
     ++issued;
     group_next_item<T, GRAD>(B, pc);
   };
