@@ -49,7 +49,9 @@ enum Mode : int { kFwdFit = 0, kFwdRaw = 1, kBwd = 2, kFwdW = 3 };
 template <int STRIDE, int APT>
 struct Geo {
   static constexpr int kTile = kConsumerThreads * APT;
-  static constexpr int kStageBytes = ((kTile * STRIDE * 4 + 32) + 127) / 128 * 128;
+  // the tile's 16-byte hull, then (gradient pass) the frame's 16-double rotation record
+  static constexpr int kRecOffset = ((kTile * STRIDE * 4 + 32) + 127) / 128 * 128;
+  static constexpr int kStageBytes = kRecOffset + kStatDoubles * 8;
   static constexpr int kStagesRaw = 51200 / kStageBytes;
   static constexpr int kStages = kStagesRaw < 3 ? 3 : (kStagesRaw > 8 ? 8 : kStagesRaw);
   static constexpr int kRedBytes = 2 * kConsumerWarps * 16 * 8;
@@ -141,10 +143,12 @@ __global__ void __launch_bounds__(256) rmsd_finalize_kernel(const FrameLaunch L,
 
 // Byte range of item (t, f) and its bulk copy into a stage.  The 16-byte
 // aligned hull [c0, c1) is copied; a range that runs into the unaligned tail
-// of the array gets its last floats by plain loads.  Called by one thread.
+// of the array gets its last floats by plain loads.  With rec_offset > 0 (the
+// gradient pass) frame f's rotation record follows at dst + rec_offset.
+// Called by one thread.
 template <int STRIDE, int T>
 __device__ __forceinline__ void issue_item(const FrameLaunch& L, int t, int64_t f, unsigned char* dst, uint64_t* bar,
-                                           uint64_t total_al) {
+                                           uint64_t total_al, int rec_offset = 0) {
   const int64_t a0 = (int64_t)t * T;
   const int64_t a1 = min(L.ref.n_sel, a0 + T);
   const unsigned char* base = reinterpret_cast<const unsigned char*>(L.coords);
@@ -162,8 +166,9 @@ __device__ __forceinline__ void issue_item(const FrameLaunch& L, int t, int64_t 
   // order this CTA's earlier generic-proxy reads of the stage before the
   // async-proxy write into it
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  mbar_arrive_expect_tx(bar, core);
+  mbar_arrive_expect_tx(bar, core + (rec_offset ? (uint32_t)(kStatDoubles * 8) : 0u));
   if (core) bulk_copy_g2s(dst, base + c0, core, bar);
+  if (rec_offset) bulk_copy_g2s(dst + rec_offset, L.rot + f * kStatDoubles, kStatDoubles * 8, bar);
 }
 
 // Streaming kernel.  Items (tile t, frame f) are enumerated tile-major; each
@@ -207,7 +212,8 @@ __global__ void __launch_bounds__(kThreads, 3) rmsd_frames_kernel(const FrameLau
   if (!GATHER && tid == 0) {
     for (; issued < S - 1 && issued < n_items; ++issued) {
       if (!(withheld && issued == 0))
-        issue_item<STRIDE, T>(L, tp, fp, smem + (issued % S) * G::kStageBytes, &full[issued % S], total_al);
+        issue_item<STRIDE, T>(L, tp, fp, smem + (issued % S) * G::kStageBytes, &full[issued % S], total_al,
+                              MODE == kBwd ? G::kRecOffset : 0);
       if (++fp == F) { fp = 0; ++tp; }
     }
   }
@@ -223,7 +229,9 @@ __global__ void __launch_bounds__(kThreads, 3) rmsd_frames_kernel(const FrameLau
   for (int64_t i = 0; i < n_items; ++i) {
     if (!GATHER && tid == 0 && issued < n_items) {
       const int sp = (int)(issued % S);
-      if (!(withheld && issued == 0)) issue_item<STRIDE, T>(L, tp, fp, smem + sp * G::kStageBytes, &full[sp], total_al);
+      if (!(withheld && issued == 0))
+        issue_item<STRIDE, T>(L, tp, fp, smem + sp * G::kStageBytes, &full[sp], total_al,
+                              MODE == kBwd ? G::kRecOffset : 0);
       ++issued;
       if (++fp == F) { fp = 0; ++tp; }
     }
@@ -297,12 +305,14 @@ __global__ void __launch_bounds__(kThreads, 3) rmsd_frames_kernel(const FrameLau
 
     if (MODE == kBwd) {
       if (ok) {
-        const double* rt = L.rot + f * kStatDoubles;
+        // the staged copy of the frame's rotation record, or (gathered) the record itself
+        const double* rt = GATHER ? L.rot + f * kStatDoubles
+                                  : reinterpret_cast<const double*>(smem + s * G::kStageBytes + G::kRecOffset);
         double R[9], c[3];
 #pragma unroll
-        for (int e = 0; e < 9; ++e) R[e] = __ldg(rt + e);
-        c[0] = __ldg(rt + 9); c[1] = __ldg(rt + 10); c[2] = __ldg(rt + 11);
-        const double scale = __ldg(rt + 12);
+        for (int e = 0; e < 9; ++e) R[e] = rt[e];
+        c[0] = rt[9]; c[1] = rt[10]; c[2] = rt[11];
+        const double scale = rt[12];
         float* gframe = L.grad + (size_t)f * L.n_atoms * 3;
 #pragma unroll
         for (int j = 0; j < APT; ++j) {
