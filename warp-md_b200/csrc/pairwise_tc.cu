@@ -6,34 +6,44 @@
 // int8 limbs q = sum_p a_p 2^(8p) (balanced digits in [-128, 127]).  The
 // covariance of a frame pair is then
 //     H_ij = s^2 sum_{p,r} 2^(8(p+r)) sum_k a_p(i,k) a_r(j,k),
-// i.e. 2*LIMBS - 1 "shift groups" g = p + r of int8 x int8 GEMMs whose int32
-// accumulation is exact (checked: 3 n 128^2 < 2^31 for n < 43,690 atoms).  The
-// tensor cores thus produce the exact Gram matrix of the quantised frames; the
-// only approximation is the quantisation (<= s/2 per coordinate, s ~ 1e-5 A for
-// 24-bit at 100 A extent), and the FP64 epilogue combines the groups and runs
-// QCP per pair.  Split-BF16 with FP32 accumulation cannot do this: dropping or
-// rounding the lo*lo products biases n*MSD by ~n |lo|^2, which at 1,000 atoms
-// is ~1e-2 A in RMSD for adjacent frames.
+// i.e. "shift groups" g = p + r of int8 x int8 GEMMs whose int32 accumulation
+// is exact (3 n 128^2 < 2^31 for n < 43,690 atoms), combined exactly in int64
+// by the FP64 epilogue, which runs QCP per pair.  Split-BF16 with FP32
+// accumulation cannot reach this: dropping or rounding the lo*lo products
+// biases n*MSD by ~n |lo|^2, which at 1,000 atoms is ~1e-2 A in RMSD for
+// adjacent frames.
+//   2 limbs (16-bit): all four products, 3 groups -- the exact Gram matrix of
+//       the quantised frames.
+//   3 limbs (24-bit): the eight products other than lo x lo, 4 groups (1..4).
+//       The frame self-sums G use the same truncated product, so a frame
+//       against itself still gives exactly 0, and the truncation lowers n*MSD
+//       by sum_k |lo_i - R lo_j|^2 s^2 (lo: the low limb, |lo| s < 7.7e-4 A at
+//       100 A extent), about 1.2e-6 A^2 per atom: < 6e-5 A of RMSD above
+//       0.01 A.  Pairs below 0.01 A are recomputed exactly in FP64 from the
+//       coordinates (pair_refine_kernel), so every entry stays within 1e-4 A.
 //
 // Layout.  Rows of the GEMM are (frame, component); 10 frames occupy 32 rows
 // (30 used), so a 128-row tile holds 40 frames and a frame's three rows sit in
 // one warp's TMEM lane quarter.  The limb array is L[limb][row][k] (k = atom,
 // padded to 64) and serves as both A (tile of 128 rows = 40 frames) and B
-// (96 rows = 30 frames); D = A B^T, both operands K-major.
+// (128 rows = 40 frames); D = A B^T, both operands K-major, M = N = 128 (an
+// N of 128 or more runs the MMA at the full int8 rate with both operands in
+// shared memory; N = 96 measured 86 % of it).
 //
 // Kernel.  Persistent, one CTA per SM, warp-specialised:
 //   warp 0     TMA producer: per 64-atom K chunk one 3-D box per operand
-//              (all limbs at once), SWIZZLE_64B, 3-4 stage mbarrier ring;
+//              (all limbs at once), SWIZZLE_64B, 2-3 stage mbarrier ring;
 //   warp 1     allocates 512 TMEM columns; lane 0 issues tcgen05.mma
-//              kind::i8 (M=128, N=96, K=32) for every limb pair into the
-//              pair's shift-group accumulator (5 x 96 columns for 3 limbs),
-//              commits stages back to the producer and tiles to the epilogue;
-//   warps 2-13 drain: tcgen05.ld of its 32 lanes x 32 columns per group,
+//              kind::i8 (M=128, N=128, K=32) for every limb pair into the
+//              pair's shift-group accumulator (4 x 128 columns for 3 limbs,
+//              3 x 128 for 2), commits stages back to the producer and tiles
+//              to the epilogue;
+//   warps 2-17 drain: tcgen05.ld of its 32 lanes x 32 columns per group,
 //              exact combination of the groups in int64, the 9 entries of H
 //              of its 10 x 10 frame pairs staged pair-major in shared memory,
 //              release of TMEM (the next tile's MMAs start);
-//   warps 14-21 stage the tile's per-frame terms (G, centroids);
-//   warps 2-21 then run the FP64 pair epilogue (QCP) for the tile's 1,200
+//   warps 18-21 stage the tile's per-frame terms (G, centroids);
+//   warps 2-21 then run the FP64 pair epilogue (QCP) for the tile's 1,600
 //              pairs, one pair per lane per round, and the symmetric store.
 // Every wait is bounded; a wait that runs out raises the CTA's abort flag and
 // all roles leave, after the MMAs in flight are drained and TMEM is freed.
@@ -56,13 +66,13 @@ namespace {
 constexpr int kFramesPerQuarter = 10;  // frames per 32 TMEM lanes
 constexpr int kTileM = 128;            // GEMM rows per tile (40 frames)
 constexpr int kTileFramesM = 40;
-constexpr int kTileN = 96;             // GEMM columns per tile (30 frames)
-constexpr int kTileFramesN = 30;
+constexpr int kTileN = 128;            // GEMM columns per tile (40 frames)
+constexpr int kTileFramesN = 40;
 constexpr int kSliceCols = 32;         // epilogue columns per warp: one 32-row group of B
 constexpr int kSliceFrames = kFramesPerQuarter;  // 10 frames (30 columns + 2 pad)
-constexpr int kSlices = kTileN / kSliceCols;  // 3
-constexpr int kEpiWarps = 4 * kSlices; // 12 drain warps: every (lane quarter, slice)
-constexpr int kHelpWarps = 8;          // extra warps for the per-pair FP64 epilogue
+constexpr int kSlices = kTileN / kSliceCols;  // 4
+constexpr int kEpiWarps = 4 * kSlices; // 16 drain warps: every (lane quarter, slice)
+constexpr int kHelpWarps = 4;          // extra warps for the per-pair FP64 epilogue
 constexpr int kQcpWarps = kEpiWarps + kHelpWarps;
 constexpr int kTcThreads = 64 + 32 * kQcpWarps;
 constexpr int kKChunk = 64;            // atoms (= bytes per operand row) per stage
@@ -74,10 +84,12 @@ constexpr int kEpiWarpBytes = 9 * kBlockPairs * 8;
 
 template <int LIMBS>
 struct TcGeo {
-  static constexpr int kGroups = 2 * LIMBS - 1;
-  static constexpr int kStages = LIMBS == 3 ? 3 : 4;  // fits 227 KB with the H staging
+  // accumulators: shift groups kShift .. 2 LIMBS - 2 (3 limbs leave out lo x lo, group 0)
+  static constexpr int kShift = LIMBS == 3 ? 1 : 0;
+  static constexpr int kGroups = 2 * LIMBS - 1 - kShift;
+  static constexpr int kStages = LIMBS == 3 ? 2 : 3;  // fits 227 KB with the H staging
   static constexpr int kALimbBytes = kTileM * kKChunk;  // 8 KB
-  static constexpr int kBLimbBytes = kTileN * kKChunk;  // 6 KB
+  static constexpr int kBLimbBytes = kTileN * kKChunk;  // 8 KB
   static constexpr int kABytes = LIMBS * kALimbBytes;
   static constexpr int kBBytes = LIMBS * kBLimbBytes;
   static constexpr int kStageBytes = kABytes + kBBytes;
@@ -87,7 +99,11 @@ struct TcGeo {
   // full[8], empty[8], tmem_full, tmem_empty, drain, tmem address, abort flag
   static constexpr int kSmemBytes = kBarOffset + 24 * 8 + 64;
   static constexpr int kQmax = LIMBS == 3 ? (1 << 23) - (1 << 16) : (1 << 15) - (1 << 8);
+  static_assert(kSmemBytes <= 227 * 1024, "shared memory");
 };
+
+// Pairs whose truncated 3-limb RMSD falls below this are recomputed exactly.
+constexpr float kRefineRmsd = 0.01f;
 
 // ------------------------------------------------------------------ PTX --
 
@@ -181,6 +197,9 @@ struct TcArgs {
   float* out;          // [F][F]
   int* status;
   WaitCfg wait;
+  uint2* flagged;      // 3 limbs: pairs (i, j) below kRefineRmsd for pair_refine_kernel
+  unsigned* n_flagged; //   their count (may exceed cap: the refine pass then scans the matrix)
+  unsigned cap;
 };
 
 // -------------------------------------------------------------- kernel --
@@ -272,6 +291,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
             for (int r = 0; r < LIMBS; ++r) {
               const int g = p + r;
+              if (g < G::kShift) continue;  // 3 limbs: lo x lo is left out
               // the first MMA of a group in a tile overwrites, the rest add
               const bool first_pair = (p == (g < LIMBS ? 0 : g - LIMBS + 1));
 #pragma unroll
@@ -279,7 +299,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 const uint64_t da = desc_sw64(st + p * G::kALimbBytes + ks * 32);
                 const uint64_t db = desc_sw64(st + G::kABytes + r * G::kBLimbBytes + ks * 32);
                 const uint32_t acc = (kc > 0 || !first_pair || ks > 0) ? 1u : 0u;
-                mma_i8(tmem_base + (uint32_t)(g * kTileN), da, db, kIdesc, acc);
+                mma_i8(tmem_base + (uint32_t)((g - G::kShift) * kTileN), da, db, kIdesc, acc);
               }
             }
           }
@@ -336,7 +356,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
               tmem_ld8(col + 8, v + 8);
               tmem_wait_ld();
 #pragma unroll
-              for (int c = 0; c < 16; ++c) acc[c] += (long long)v[c] << (8 * g);
+              for (int c = 0; c < 16; ++c) acc[c] += (long long)v[c] << (8 * (g + G::kShift));
             }
             if (lane < 30) {
               // lane = 3 pi + a (row frame pi, component a); column 3 pj + b
@@ -397,6 +417,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         args.out[(size_t)i * args.F + j] = (float)v;
         args.out[(size_t)j * args.F + i] = (float)v;
+        if (G::kShift && v < (double)kRefineRmsd) {  // recomputed exactly by pair_refine_kernel
+          const unsigned k = atomicAdd(args.n_flagged, 1u);
+          if (k < args.cap) args.flagged[k] = make_uint2((unsigned)i, (unsigned)j);
+        }
       }
       named_barrier_sync(2, 32 * kQcpWarps);  // staging may be rewritten
     }
@@ -463,7 +487,8 @@ __global__ void __launch_bounds__(256) tc_prep_centre(const float* __restrict__ 
 }
 
 // Pass 2 (one CTA per frame): quantise with the trajectory-wide scale and
-// write the int8 limbs L[p][row(f, a)][k]; G_f = sum q^2 exactly (int64).
+// write the int8 limbs L[p][row(f, a)][k]; G_f = sum q^2 exactly (int64),
+// less sum lo^2 with 3 limbs (the products the tensor cores form).
 template <int LIMBS>
 __global__ void __launch_bounds__(256) tc_prep_limbs(const float* __restrict__ coords, int64_t n_atoms, int stride,
                                                      const uint32_t* __restrict__ sel, int64_t n_sel, int64_t n_pad,
@@ -497,6 +522,8 @@ __global__ void __launch_bounds__(256) tc_prep_limbs(const float* __restrict__ c
         // balanced base-256 digit in [-128, 127]
         int32_t d = ((rem % 256) + 256 + 128) % 256 - 128;
         if (l == LIMBS - 1) d = rem;
+        // the self-sum G leaves out lo x lo as the tensor-core products do
+        if (l == 0 && TcGeo<LIMBS>::kShift) g -= (long long)d * d;
         limbs[((size_t)l * rows + row0 + a) * n_pad + k] = (int8_t)d;
         rem = (rem - d) / 256;
       }
@@ -509,6 +536,88 @@ __global__ void __launch_bounds__(256) tc_prep_limbs(const float* __restrict__ c
     long long t = 0;
     for (int w = 0; w < 8; ++w) t += red[w];
     gsum[f] = (double)t;
+  }
+}
+
+// 3 limbs: pairs whose truncated RMSD came out below kRefineRmsd, recomputed
+// exactly in FP64 from the coordinates, a warp per pair: the centred sums H,
+// G_i, G_j and QCP (metric rms), or sum |x_i - x_j|^2 (nofit), each lane
+// taking atoms lane, lane + 32, ... and the warp adding its lanes in a fixed
+// tree.  When more pairs were flagged than the list holds, every pair (i, j),
+// i < j, of this launch's tile rows (i / 40 = part mod parts) whose entry is
+// below kRefineRmsd is found in the matrix itself.
+__global__ void __launch_bounds__(256) pair_refine_kernel(const float* __restrict__ coords, int64_t n_atoms, int stride,
+                                                          const uint32_t* __restrict__ sel, int64_t n_sel, int64_t F,
+                                                          const double* __restrict__ cen, int metric,
+                                                          const uint2* __restrict__ list,
+                                                          const unsigned* __restrict__ count, unsigned cap,
+                                                          float* __restrict__ out, int part, int parts, int* status) {
+  const int lane = threadIdx.x & 31;
+  const int64_t wg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const unsigned n_list = *count;
+  auto refine = [&](int64_t i, int64_t j) {
+    const float* xi = coords + (size_t)i * n_atoms * stride;
+    const float* xj = coords + (size_t)j * n_atoms * stride;
+    const double ci0 = cen[i * 3], ci1 = cen[i * 3 + 1], ci2 = cen[i * 3 + 2];
+    const double cj0 = cen[j * 3], cj1 = cen[j * 3 + 1], cj2 = cen[j * 3 + 2];
+    double v[12];
+#pragma unroll
+    for (int e = 0; e < 12; ++e) v[e] = 0.0;
+    for (int64_t k = lane; k < n_sel; k += 32) {
+      int64_t a = sel ? (int64_t)sel[k] : k;
+      if (a >= n_atoms) {  // bad device-side selection: report, read atom 0
+        atomicOr(status, kStatusBadIndex);
+        a = 0;
+      }
+      const float* p = xi + a * stride;
+      const float* q = xj + a * stride;
+      if (metric == WMD_PAIR_NOFIT) {
+        const double d0 = (double)p[0] - (double)q[0], d1 = (double)p[1] - (double)q[1],
+                     d2 = (double)p[2] - (double)q[2];
+        v[0] += d0 * d0 + d1 * d1 + d2 * d2;
+      } else {
+        const double u0 = (double)p[0] - ci0, u1 = (double)p[1] - ci1, u2 = (double)p[2] - ci2;
+        const double w0 = (double)q[0] - cj0, w1 = (double)q[1] - cj1, w2 = (double)q[2] - cj2;
+        v[0] += u0 * w0; v[1] += u0 * w1; v[2] += u0 * w2;
+        v[3] += u1 * w0; v[4] += u1 * w1; v[5] += u1 * w2;
+        v[6] += u2 * w0; v[7] += u2 * w1; v[8] += u2 * w2;
+        v[9] += u0 * u0 + u1 * u1 + u2 * u2;
+        v[10] += w0 * w0 + w1 * w1 + w2 * w2;
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 11; ++e)
+      for (int o = 16; o; o >>= 1) v[e] += __shfl_xor_sync(0xffffffffu, v[e], o);
+    if (lane == 0) {
+      const double nn = (double)n_sel;
+      double r;
+      if (metric == WMD_PAIR_NOFIT) {
+        r = sqrt(v[0] / nn);
+      } else {
+        const QcpOut qo = qcp_lambda(v, 0.5 * (v[9] + v[10]));
+        r = sqrt(msd_from(v[9], v[10], qo.lambda, nn));
+      }
+      out[(size_t)i * F + j] = (float)r;
+      out[(size_t)j * F + i] = (float)r;
+    }
+  };
+  if (n_list <= cap) {
+    for (int64_t p = wg; p < (int64_t)n_list; p += nw) refine(list[p].x, list[p].y);
+    return;
+  }
+  for (int64_t i = wg; i < F; i += nw) {
+    if ((int)((i / kTileFramesM) % parts) != part) continue;
+    for (int64_t j0 = i + 1; j0 < F; j0 += 32) {
+      const int64_t j = j0 + lane;
+      const bool low = j < F && out[(size_t)i * F + j] < kRefineRmsd;
+      unsigned m = __ballot_sync(0xffffffffu, low);
+      while (m) {
+        const int b = __ffs(m) - 1;
+        m &= m - 1;
+        refine(i, j0 + b);
+      }
+    }
   }
 }
 
@@ -543,8 +652,11 @@ int run_tc(PairwiseWorkspace& w, int sm_count, const float* coords, int64_t F, i
   const int64_t rows_pad = (rows + kTileM - 1) / kTileM * kTileM;  // whole 128-row tiles
   const size_t limb_bytes = (size_t)LIMBS * rows_pad * n_pad;
   const size_t small = 256 + (size_t)F * (sizeof(double) * 4);
-  // workspace: [scale, maxbits | gsum F | cen 3F][limbs]
-  const size_t need = small + limb_bytes + 1024;
+  // pairs flagged for the exact recomputation (3 limbs)
+  const unsigned cap = G::kShift ? (unsigned)std::min<int64_t>(std::max<int64_t>(F * (F - 1) / 2, 1), 1 << 20) : 0u;
+  const size_t list_bytes = (size_t)cap * sizeof(uint2);
+  // workspace: [scale, maxbits, flagged count | gsum F | cen 3F][limbs][flagged pairs]
+  const size_t need = small + limb_bytes + 1024 + list_bytes + 16;
   if (!w.extra || w.extra_bytes < need) {
     if (w.extra) cudaFree(w.extra);
     w.extra = nullptr;
@@ -562,7 +674,9 @@ int run_tc(PairwiseWorkspace& w, int sm_count, const float* coords, int64_t F, i
   unsigned* maxbits = reinterpret_cast<unsigned*>(base + 8);
   double* gsum = reinterpret_cast<double*>(base + 256);
   double* cen = gsum + F;
+  unsigned* n_flagged = reinterpret_cast<unsigned*>(base + 16);
   int8_t* limbs = reinterpret_cast<int8_t*>(base + ((small + 1023) & ~size_t(1023)));
+  uint2* flagged = reinterpret_cast<uint2*>(base + (((small + 1023) & ~size_t(1023)) + limb_bytes + 15) / 16 * 16);
 
   cudaError_t e = cudaMemsetAsync(base, 0, 256, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(limbs, 0, limb_bytes, s);
@@ -609,6 +723,9 @@ int run_tc(PairwiseWorkspace& w, int sm_count, const float* coords, int64_t F, i
   a.out = out;
   a.status = status;
   a.wait = wait;
+  a.flagged = flagged;
+  a.n_flagged = n_flagged;
+  a.cap = cap;
   TileList tl;
   tl.ni = (int)((F + kTileFramesM - 1) / kTileFramesM);
   tl.nj = (int)((F + kTileFramesN - 1) / kTileFramesN);
@@ -626,6 +743,14 @@ int run_tc(PairwiseWorkspace& w, int sm_count, const float* coords, int64_t F, i
   if ((e = cudaGetLastError()) != cudaSuccess) {
     *msg = std::string("cuda driver error: pairwise tensor-core launch: ") + cudaGetErrorString(e);
     return WMD_ERR_CUDA;
+  }
+  if (G::kShift) {
+    pair_refine_kernel<<<(unsigned)(2 * sm_count), 256, 0, s>>>(coords, n_atoms, stride, sel, n_sel, F, cen, metric,
+                                                                 flagged, n_flagged, cap, out, w.part, w.parts, status);
+    if ((e = cudaGetLastError()) != cudaSuccess) {
+      *msg = std::string("cuda driver error: pairwise refine launch: ") + cudaGetErrorString(e);
+      return WMD_ERR_CUDA;
+    }
   }
   return 0;
 }
