@@ -5,7 +5,8 @@ Tolerances (max abs error vs the FP64 oracle; outputs are float32 like the
 reference's, so a relative 1e-7 for the float32 rounding of large values is
 added to each):
   fp64 : 1e-5 A   (FP64 covariance tiles, exact up to the float32 output)
-  i8x3 : 1e-4 A   (24-bit fixed point, exact int32 accumulation)
+  i8x3 : 1e-4 A   (24-bit fixed point, the eight limb products other than lo x lo in exact
+                   int32 accumulation; pairs below 0.01 A recomputed exactly in FP64)
   i8x2 : 5e-4 A   (16-bit fixed point)
   fp32 : 2e-2 A   (plain FP32 accumulation; measured error is reported by bench.py)
 """
@@ -282,3 +283,59 @@ def test_parts_are_disjoint_and_sum_to_the_full_matrix(mode):
     bad = ctx.lib.wmd_pairwise_rmsd_part(ctx.handle, x.data_ptr(), F, 120, 3, None, 120, N.PAIR_RMS,
                                          _PAIR_MODES[mode], 3, 3, full.data_ptr(), None)
     assert bad == N.WMD_ERR_INVALID_ARG
+
+
+def _near_identical(F, n, step, seed):
+    """Frames that differ by ~step A per coordinate from frame 0, each under a
+    random rigid motion: every pair is below the 0.01 A refine threshold."""
+    rng = np.random.default_rng(seed)
+    base = synth.make_trajectory(n, 1, 0.0, seed)[1]
+    out = np.empty((F, n, 3), np.float32)
+    for f in range(F):
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        w, x, y, z = q
+        R = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                      [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                      [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+        noisy = base + rng.normal(0, step, base.shape)
+        out[f] = (noisy @ R.T + rng.normal(0, 10, 3)).astype(np.float32)
+    return out
+
+
+@pytest.mark.parametrize("metric", ["rms", "nofit"])
+def test_i8x3_pairs_below_refine_threshold_are_exact(metric):
+    """3 limbs leave the lo x lo limb product out of the tensor-core sums; the
+    pairs whose RMSD then comes out below 0.01 A are recomputed in FP64 from
+    the coordinates.  Frames within ~1e-3 A of each other (a duplicate
+    included): every off-diagonal pair is refined and agrees with the oracle
+    to 2e-6 A (FP64 against FP64, float32 output), the duplicate pair to 0."""
+    ctx = N.context(0)
+    if not _supported(ctx, "i8x3"):
+        pytest.skip("tensor-core form not supported on this device")
+    fr = _near_identical(96, 700, 6e-4, seed=5)
+    fr[17] = fr[3]
+    if metric == "nofit":  # no superposition: identical placement, small displacements
+        fr = np.repeat(fr[:1], 96, axis=0) + np.random.default_rng(6).normal(0, 6e-4, fr.shape).astype(np.float32)
+        fr[17] = fr[3]
+    got = gpu_pairwise(ctx, fr, metric, "i8x3", device_io=True)
+    _, exp = oracle.pairwise(fr, metric)
+    off = ~np.eye(96, dtype=bool)
+    assert exp[off].max() < 0.01
+    np.testing.assert_allclose(got, exp, rtol=1e-6, atol=2e-6)
+    assert got[3, 17] < 2e-6 and got[17, 3] < 2e-6
+
+
+def test_i8x3_refine_list_overflow_scans_the_matrix():
+    """More flagged pairs than the list holds (1,600 near-identical frames:
+    1,279,200 pairs against a list of 2^20): the refine pass then finds them
+    in the matrix itself; the result equals the oracle on a 300-frame block."""
+    ctx = N.context(0)
+    if not _supported(ctx, "i8x3"):
+        pytest.skip("tensor-core form not supported on this device")
+    F = 1600
+    fr = _near_identical(F, 200, 5e-4, seed=9)
+    got = gpu_pairwise(ctx, fr, "rms", "i8x3", device_io=True)
+    idx = np.r_[np.arange(150), np.arange(F - 150, F)]
+    _, exp = oracle.pairwise(fr[idx], "rms")
+    np.testing.assert_allclose(got[np.ix_(idx, idx)], exp, rtol=1e-6, atol=2e-6)
