@@ -412,8 +412,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           const double ssq = gi + gj - 2.0 * (h[0] + h[4] + h[8]) + args.n * (d0 * d0 + d1 * d1 + d2 * d2);
           v = ssq > 0.0 ? sqrt(ssq / args.n) : 0.0;
         } else {
-          const QcpOut q = qcp_lambda(h, 0.5 * (gi + gj));
-          v = sqrt(msd_from(gi, gj, q.lambda, args.n));
+          double msd;
+          if (!qcp_msd_shifted(h, gi, gj, args.n, &msd)) {  // a root that is not simple: the FP64 route
+            const QcpOut q = qcp_lambda(h, 0.5 * (gi + gj));
+            msd = msd_from(gi, gj, q.lambda, args.n);
+          }
+          v = sqrt(msd);
         }
         args.out[(size_t)i * args.F + j] = (float)v;
         args.out[(size_t)j * args.F + i] = (float)v;
