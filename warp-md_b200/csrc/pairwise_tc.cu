@@ -31,8 +31,9 @@
 // shared memory; N = 96 measured 86 % of it).
 //
 // Kernel.  Persistent, one CTA per SM, warp-specialised:
-//   warp 0     TMA producer: per 64-atom K chunk one 3-D box per operand
-//              (all limbs at once), SWIZZLE_64B, 2-3 stage mbarrier ring;
+//   warp 0     TMA producer: per K chunk (32 atoms with 3 limbs, 64 with 2)
+//              one 3-D box per operand (all limbs at once), SWIZZLE_32B or
+//              SWIZZLE_64B, 4- or 3-stage mbarrier ring;
 //   warp 1     allocates 512 TMEM columns; lane 0 issues tcgen05.mma
 //              kind::i8 (M=128, N=128, K=32) for every limb pair into the
 //              pair's shift-group accumulator (4 x 128 columns for 3 limbs,
@@ -75,7 +76,7 @@ constexpr int kEpiWarps = 4 * kSlices; // 16 drain warps: every (lane quarter, s
 constexpr int kHelpWarps = 4;          // extra warps for the per-pair FP64 epilogue
 constexpr int kQcpWarps = kEpiWarps + kHelpWarps;
 constexpr int kTcThreads = 64 + 32 * kQcpWarps;
-constexpr int kKChunk = 64;            // atoms (= bytes per operand row) per stage
+constexpr int kKPad = 64;              // atoms are padded to a multiple of this
 constexpr int kTmemCols = 512;
 constexpr int kBlockPairs = kFramesPerQuarter * kSliceFrames;  // 100 frame pairs per drain warp
 // per-warp H staging, pair-major: element e = 3a + b of pair p at [e][p], so
@@ -87,9 +88,12 @@ struct TcGeo {
   // accumulators: shift groups kShift .. 2 LIMBS - 2 (3 limbs leave out lo x lo, group 0)
   static constexpr int kShift = LIMBS == 3 ? 1 : 0;
   static constexpr int kGroups = 2 * LIMBS - 1 - kShift;
-  static constexpr int kStages = LIMBS == 3 ? 2 : 3;  // fits 227 KB with the H staging
-  static constexpr int kALimbBytes = kTileM * kKChunk;  // 8 KB
-  static constexpr int kBLimbBytes = kTileN * kKChunk;  // 8 KB
+  // atoms (= bytes per operand row) per stage: 32 with 3 limbs (4 stages of 24 KB),
+  // 64 with 2 (3 stages of 32 KB); either fits 227 KB with the H staging
+  static constexpr int kKChunk = LIMBS == 3 ? 32 : 64;
+  static constexpr int kStages = LIMBS == 3 ? 4 : 3;
+  static constexpr int kALimbBytes = kTileM * kKChunk;
+  static constexpr int kBLimbBytes = kTileN * kKChunk;
   static constexpr int kABytes = LIMBS * kALimbBytes;
   static constexpr int kBBytes = LIMBS * kBLimbBytes;
   static constexpr int kStageBytes = kABytes + kBBytes;
@@ -154,11 +158,15 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
-// Shared-memory matrix descriptor, K-major, SWIZZLE_64B (rows of 64 bytes,
-// 8-row core groups 512 bytes apart), sm_100 descriptor version 1.
-__device__ __forceinline__ uint64_t desc_sw64(const void* p) {
+// Shared-memory matrix descriptor, K-major, rows of ROW bytes with the
+// matching swizzle (64: SWIZZLE_64B, layout 4; 32: SWIZZLE_32B, layout 6),
+// 8-row core groups 8 ROW bytes apart, sm_100 descriptor version 1.
+template <int ROW>
+__device__ __forceinline__ uint64_t desc_sw(const void* p) {
+  static_assert(ROW == 32 || ROW == 64, "row bytes");
   const uint64_t start = (smem_addr(p) >> 4) & 0x3FFFu;
-  return start | (uint64_t(1) << 16) | (uint64_t(512 >> 4) << 32) | (uint64_t(1) << 46) | (uint64_t(4) << 61);
+  return start | (uint64_t(1) << 16) | (uint64_t((8 * ROW) >> 4) << 32) | (uint64_t(1) << 46) |
+         (uint64_t(ROW == 64 ? 4 : 6) << 61);
 }
 
 // kind::i8 instruction descriptor: D s32, A/B s8, both K-major, M=128, N=96.
@@ -188,7 +196,7 @@ struct TileList {
 
 struct TcArgs {
   int64_t F;
-  int64_t n_pad;      // atoms padded to kKChunk
+  int64_t n_pad;      // atoms padded to kKPad
   double n;           // selected atoms
   int metric;
   const double* gsum;  // [F] sum |q|^2 (units of s^2)
@@ -221,7 +229,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + G::kBarOffset + 24 * 8 + 16);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n_k = (int)(args.n_pad / kKChunk);
+  const int n_k = (int)(args.n_pad / G::kKChunk);
   const int64_t n_tiles = (int64_t)tiles.ni * tiles.nj;
 
   if (threadIdx.x == 0) {
@@ -258,8 +266,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           if (withheld && it == 0) continue;
           unsigned char* st = smem + s * G::kStageBytes;
           mbar_arrive_expect_tx(&full[s], G::kStageBytes);
-          tma_load_3d(st, &map_a, kc * kKChunk, bi * kTileM, 0, &full[s]);
-          tma_load_3d(st + G::kABytes, &map_b, kc * kKChunk, bj * kTileN, 0, &full[s]);
+          tma_load_3d(st, &map_a, kc * G::kKChunk, bi * kTileM, 0, &full[s]);
+          tma_load_3d(st + G::kABytes, &map_b, kc * G::kKChunk, bj * kTileN, 0, &full[s]);
         }
       }
       // When the MMAs stopped early (a wait ran out), stages loaded for them
@@ -295,9 +303,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
               // the first MMA of a group in a tile overwrites, the rest add
               const bool first_pair = (p == (g < LIMBS ? 0 : g - LIMBS + 1));
 #pragma unroll
-              for (int ks = 0; ks < kKChunk / 32; ++ks) {
-                const uint64_t da = desc_sw64(st + p * G::kALimbBytes + ks * 32);
-                const uint64_t db = desc_sw64(st + G::kABytes + r * G::kBLimbBytes + ks * 32);
+              for (int ks = 0; ks < G::kKChunk / 32; ++ks) {
+                const uint64_t da = desc_sw<G::kKChunk>(st + p * G::kALimbBytes + ks * 32);
+                const uint64_t db = desc_sw<G::kKChunk>(st + G::kABytes + r * G::kBLimbBytes + ks * 32);
                 const uint32_t acc = (kc > 0 || !first_pair || ks > 0) ? 1u : 0u;
                 mma_i8(tmem_base + (uint32_t)((g - G::kShift) * kTileN), da, db, kIdesc, acc);
               }
@@ -651,7 +659,7 @@ int run_tc(PairwiseWorkspace& w, int sm_count, const float* coords, int64_t F, i
            const uint32_t* sel, int64_t n_sel, int metric, float* out, int* status, const WaitCfg& wait,
            cudaStream_t s, std::string* msg) {
   using G = TcGeo<LIMBS>;
-  const int64_t n_pad = (n_sel + kKChunk - 1) / kKChunk * kKChunk;
+  const int64_t n_pad = (n_sel + kKPad - 1) / kKPad * kKPad;
   const int64_t rows = (F + kFramesPerQuarter - 1) / kFramesPerQuarter * 32;
   const int64_t rows_pad = (rows + kTileM - 1) / kTileM * kTileM;  // whole 128-row tiles
   const size_t limb_bytes = (size_t)LIMBS * rows_pad * n_pad;
@@ -701,15 +709,16 @@ int run_tc(PairwiseWorkspace& w, int sm_count, const float* coords, int64_t F, i
   CUtensorMap map_a, map_b;
   const cuuint64_t dims[3] = {(cuuint64_t)n_pad, (cuuint64_t)rows_pad, (cuuint64_t)LIMBS};
   const cuuint64_t strides[2] = {(cuuint64_t)n_pad, (cuuint64_t)(rows_pad * n_pad)};
-  const cuuint32_t box_a[3] = {kKChunk, kTileM, LIMBS};
-  const cuuint32_t box_b[3] = {kKChunk, kTileN, LIMBS};
+  const cuuint32_t box_a[3] = {G::kKChunk, kTileM, LIMBS};
+  const cuuint32_t box_b[3] = {G::kKChunk, kTileN, LIMBS};
+  const CUtensorMapSwizzle swz = G::kKChunk == 32 ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_64B;
   const cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = enc(&map_a, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, limbs, dims, strides, box_a, estr,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r == CUDA_SUCCESS)
     r = enc(&map_b, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, limbs, dims, strides, box_b, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     *msg = "cuda driver error: cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
