@@ -180,13 +180,23 @@ __device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t parity, int* sta
   return mbar_wait(bar, parity, status, kStatusTimeoutFull, abort, limit_ns);
 }
 
+// Tiles are enumerated in groups of kRowGroup tile rows, column after column
+// inside a group, so that the ~148 tiles in flight at once share a few A rows
+// and B columns and their limbs stay in L2.  (Row after row, they would share
+// one A row but stream 148 B columns, rereading each column from DRAM for
+// every row once the limbs outgrow L2: 196 MB for 20,000 frames x 1,000 atoms.)
+constexpr int kRowGroup = 8;
+
 struct TileList {
-  int ni, nj;  // I blocks (40 frames) x J blocks (30 frames)
+  int ni, nj;  // I blocks (40 frames) x J blocks (40 frames)
   int64_t F;
   int part, parts;  // this launch computes the I blocks bi = part (mod parts)
   __device__ __forceinline__ bool valid(int64_t t, int& bi, int& bj) const {
-    bi = (int)(t / nj);
-    bj = (int)(t - (int64_t)bi * nj);
+    const int64_t gsz = (int64_t)kRowGroup * nj;
+    const int64_t g = t / gsz, r = t - g * gsz;
+    const int rows = min(kRowGroup, ni - (int)g * kRowGroup);
+    bj = (int)(r / rows);
+    bi = (int)g * kRowGroup + (int)(r - (int64_t)bj * rows);
     if (bi % parts != part) return false;
     const int64_t i0 = (int64_t)bi * kTileFramesM;
     const int64_t jmax = min((int64_t)(bj + 1) * kTileFramesN, F) - 1;
@@ -282,6 +292,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (lane == 0) {
       uint32_t it = 0, tc = 0;
       bool ok = true;
+      // descriptors differ only in their start-address field (address >> 4, 14
+      // bits, which the shared-memory window never overflows): one base, offsets
+      // added per MMA, so the issuing thread spends few instructions per MMA
+      const uint64_t dbase = desc_sw<G::kKChunk>(smem);
       for (int64_t t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
         int bi, bj;
         if (!tiles.valid(t, bi, bj)) continue;
@@ -293,7 +307,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           const uint32_t ph = (it / kStagesTc) & 1u;
           if (!tc_wait(&full[s], ph, args.status, abort_flag, args.wait.limit_ns)) { ok = false; break; }
           tc_fence_after();
-          const unsigned char* st = smem + s * G::kStageBytes;
+          const uint64_t dst = dbase + (uint64_t)((uint32_t)(s * G::kStageBytes) >> 4);
+          const uint32_t later = kc > 0 ? 1u : 0u;
 #pragma unroll
           for (int p = 0; p < LIMBS; ++p) {
 #pragma unroll
@@ -304,9 +319,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
               const bool first_pair = (p == (g < LIMBS ? 0 : g - LIMBS + 1));
 #pragma unroll
               for (int ks = 0; ks < G::kKChunk / 32; ++ks) {
-                const uint64_t da = desc_sw<G::kKChunk>(st + p * G::kALimbBytes + ks * 32);
-                const uint64_t db = desc_sw<G::kKChunk>(st + G::kABytes + r * G::kBLimbBytes + ks * 32);
-                const uint32_t acc = (kc > 0 || !first_pair || ks > 0) ? 1u : 0u;
+                const uint64_t da = dst + (uint64_t)((p * G::kALimbBytes + ks * 32) >> 4);
+                const uint64_t db = dst + (uint64_t)((G::kABytes + r * G::kBLimbBytes + ks * 32) >> 4);
+                const uint32_t acc = (!first_pair || ks > 0) ? 1u : later;
                 mma_i8(tmem_base + (uint32_t)((g - G::kShift) * kTileN), da, db, kIdesc, acc);
               }
             }
@@ -339,7 +354,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int slice = wq >> 2;     // 32-column slice (10 frames) of a drain warp
     const double s = *args.scale;
     const double s2 = s * s;
-    double* frm = reinterpret_cast<double*>(smem + G::kFrameOffset);  // [4][70]: g, cx, cy, cz
+    const float s2f = (float)s2;
+    const float nf = (float)args.n;
+    // per-frame terms [4][80]: G (units of s^2), then centroids cx, cy, cz
+    double* frm = reinterpret_cast<double*>(smem + G::kFrameOffset);
     constexpr int kTf = kTileFramesM + kTileFramesN;
     uint32_t tc = 0;
     for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
@@ -348,7 +366,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       if (drainer) {
         if (tc_wait(tmem_full, tc & 1u, args.status, abort_flag, args.wait.limit_ns)) {
           tc_fence_after();
-          double* epi = reinterpret_cast<double*>(smem + G::kEpiOffset + wq * kEpiWarpBytes);
+          long long* epi = reinterpret_cast<long long*>(smem + G::kEpiOffset + wq * kEpiWarpBytes);
 #pragma unroll
           for (int half = 0; half < 2; ++half) {
             // columns [16 half, 16 half + 16) of the slice; 30 are frame columns
@@ -369,11 +387,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (lane < 30) {
               // lane = 3 pi + a (row frame pi, component a); column 3 pj + b
               const int pi = lane / 3, a = lane - 3 * pi;
-              double* row = epi + a * 3 * kBlockPairs + pi * kSliceFrames;
+              long long* row = epi + a * 3 * kBlockPairs + pi * kSliceFrames;
 #pragma unroll
               for (int c = 0; c < 16; ++c) {
                 const int cc = 16 * half + c;
-                if (cc < 30) row[(cc % 3) * kBlockPairs + cc / 3] = (double)acc[c] * s2;
+                if (cc < 30) row[(cc % 3) * kBlockPairs + cc / 3] = acc[c];  // exact, units of s^2
               }
             }
           }
@@ -387,7 +405,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           const int64_t f = q < kTileFramesM ? (int64_t)bi * kTileFramesM + q
                                              : (int64_t)bj * kTileFramesN + (q - kTileFramesM);
           const bool in = f < args.F;
-          frm[q] = in ? args.gsum[f] * s2 : 0.0;
+          frm[q] = in ? args.gsum[f] : 0.0;
           frm[kTf + q] = in ? args.cen[f * 3 + 0] : 0.0;
           frm[2 * kTf + q] = in ? args.cen[f * 3 + 1] : 0.0;
           frm[3 * kTf + q] = in ? args.cen[f * 3 + 2] : 0.0;
@@ -407,29 +425,35 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const int64_t i = (int64_t)bi * kTileFramesM + fi - 0;
         const int64_t j = (int64_t)bj * kTileFramesN + bs * kSliceFrames + pj;
         if (!(i < j && j < args.F)) continue;
-        const double* epi = reinterpret_cast<const double*>(smem + G::kEpiOffset + blk * kEpiWarpBytes);
-        double h[9];
+        const long long* epi = reinterpret_cast<const long long*>(smem + G::kEpiOffset + blk * kEpiWarpBytes);
+        long long h[9];
 #pragma unroll
         for (int e = 0; e < 9; ++e) h[e] = epi[e * kBlockPairs + pl];
         const double gi = frm[fi], gj = frm[fj];
-        double v;
+        float v;
         if (args.metric == WMD_PAIR_NOFIT) {
-          const double d0 = frm[kTf + fi] - frm[kTf + fj];
-          const double d1 = frm[2 * kTf + fi] - frm[2 * kTf + fj];
-          const double d2 = frm[3 * kTf + fi] - frm[3 * kTf + fj];
-          const double ssq = gi + gj - 2.0 * (h[0] + h[4] + h[8]) + args.n * (d0 * d0 + d1 * d1 + d2 * d2);
-          v = ssq > 0.0 ? sqrt(ssq / args.n) : 0.0;
+          // sum |q_i - q_j|^2 = G_i + G_j - 2 tr H (exact inputs, double-float), plus n |c_i - c_j|^2
+          const double dq = gi + gj - 2.0 * ((double)h[0] + (double)h[4] + (double)h[8]);
+          const float d0 = (float)(frm[kTf + fi] - frm[kTf + fj]);
+          const float d1 = (float)(frm[2 * kTf + fi] - frm[2 * kTf + fj]);
+          const float d2 = (float)(frm[3 * kTf + fi] - frm[3 * kTf + fj]);
+          const float ssq = (float)dq * s2f + nf * (d0 * d0 + d1 * d1 + d2 * d2);
+          v = ssq > 0.0f ? sqrtf(ssq / nf) : 0.0f;
         } else {
-          double msd;
-          if (!qcp_msd_shifted(h, gi, gj, args.n, &msd)) {  // a root that is not simple: the FP64 route
-            const QcpOut q = qcp_lambda(h, 0.5 * (gi + gj));
-            msd = msd_from(gi, gj, q.lambda, args.n);
+          float msd;
+          if (!qcp_msd_mixed(h, gi, gj, nf, s2f, &msd)) {  // a root that is not simple: the FP64 route
+            double hd[9];
+#pragma unroll
+            for (int e = 0; e < 9; ++e) hd[e] = (double)h[e] * s2;
+            const double gid = gi * s2, gjd = gj * s2;
+            const QcpOut q = qcp_lambda(hd, 0.5 * (gid + gjd));
+            msd = (float)msd_from(gid, gjd, q.lambda, args.n);
           }
-          v = sqrt(msd);
+          v = sqrtf(msd);
         }
-        args.out[(size_t)i * args.F + j] = (float)v;
-        args.out[(size_t)j * args.F + i] = (float)v;
-        if (G::kShift && v < (double)kRefineRmsd) {  // recomputed exactly by pair_refine_kernel
+        args.out[(size_t)i * args.F + j] = v;
+        args.out[(size_t)j * args.F + i] = v;
+        if (G::kShift && v < kRefineRmsd) {  // recomputed exactly by pair_refine_kernel
           const unsigned k = atomicAdd(args.n_flagged, 1u);
           if (k < args.cap) args.flagged[k] = make_uint2((unsigned)i, (unsigned)j);
         }

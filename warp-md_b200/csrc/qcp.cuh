@@ -235,6 +235,75 @@ WMD_HD bool qcp_msd_shifted(const double h[9], double gx, double gy, double n, d
   return true;
 }
 
+// Mean-square deviation of a frame pair in the tensor-core epilogue, with as
+// little FP64 arithmetic as the cancellation allows (on sm_100a FP64 issue
+// stalls beside tensor-core MMAs, FP32 does not).  H (9 entries) is exact in
+// integer units of s^2; gx, gy are the self-sums in the same units.  With
+// D = G_x + G_y = 2 e0, the quartic of qcp_msd_shifted is
+// Q(u) = det(M - u I), M = I - K / e0:
+//   * its constant term det(M) is where the cancellation sits (~8 u1 from O(1)
+//     parts): M D = D I - 2K is formed from the exact inputs and its
+//     determinant taken in FP64 (no division), then scaled by 1 / D^4 with an
+//     FP32 reciprocal (a relative 1e-7 on this small term is harmless);
+//   * the other coefficients, -(4 + 2 d2 + d1) and 6 + d2, are O(1) sums
+//     without cancellation and are formed in FP32 from H / e0;
+//   * Newton from u = 0 runs in FP32 as in qcp_msd_shifted.
+// MSD = D u1 s2 / n.  Returns false, leaving *msd unset, when Newton did not
+// converge to a clearly simple root (a second eigenvalue within ~1e-2 e0:
+// collinear or nearly collinear structures); the caller then takes the FP64
+// route.
+WMD_HD bool qcp_msd_mixed(const long long hq[9], double gx, double gy, float n, float s2, float* msd) {
+  const double D = gx + gy;
+  if (!(D > 0.0)) {
+    *msd = 0.0f;
+    return true;
+  }
+  double h[9];
+  for (int i = 0; i < 9; ++i) h[i] = (double)hq[i];
+  // M D = D I - 2 K (K as key_matrix, symmetric)
+  const double m00 = D - 2.0 * (h[0] + h[4] + h[8]);
+  const double m11 = D - 2.0 * (h[0] - h[4] - h[8]);
+  const double m22 = D - 2.0 * (h[4] - h[0] - h[8]);
+  const double m33 = D - 2.0 * (h[8] - h[0] - h[4]);
+  const double m01 = -2.0 * (h[5] - h[7]), m02 = -2.0 * (h[6] - h[2]), m03 = -2.0 * (h[1] - h[3]);
+  const double m12 = -2.0 * (h[1] + h[3]), m13 = -2.0 * (h[6] + h[2]), m23 = -2.0 * (h[5] + h[7]);
+  const double m[16] = {m00, m01, m02, m03, m01, m11, m12, m13, m02, m12, m22, m23, m03, m13, m23, m33};
+  const float invd = 1.0f / (float)D;
+  const double invd2 = (double)invd * (double)invd;  // D^-4 underflows FP32
+  const float b0 = (float)(det4(m) * (invd2 * invd2));
+  // H / e0 in FP32: d2 = c2 / e0^2 = -2 sum h'^2, d1 = c1 / e0^3 = -8 det h'
+  float hf[9];
+  for (int i = 0; i < 9; ++i) hf[i] = (float)hq[i] * (2.0f * invd);
+  float ss = 0.0f;
+  for (int i = 0; i < 9; ++i) ss = fmaf(hf[i], hf[i], ss);
+  const float det3f = hf[0] * (hf[4] * hf[8] - hf[5] * hf[7]) - hf[1] * (hf[3] * hf[8] - hf[5] * hf[6]) +
+                      hf[2] * (hf[3] * hf[7] - hf[4] * hf[6]);
+  const float d2 = -2.0f * ss, d1 = -8.0f * det3f;
+  const float b1 = -(4.0f + 2.0f * d2 + d1), b2 = 6.0f + d2;
+  float u = 0.0f, dq = b1;
+  bool converged = false;
+  for (int it = 0; it < 24; ++it) {
+    const float q = (((u - 4.0f) * u + b2) * u + b1) * u + b0;
+    dq = ((4.0f * u - 12.0f) * u + 2.0f * b2) * u + b1;
+    if (!(dq != 0.0f)) break;
+    const float du = q / dq;
+    u -= du;
+    if (fabsf(du) <= 2e-7f * fabsf(u) + 1e-30f) {
+      converged = true;
+      break;
+    }
+  }
+  dq = ((4.0f * u - 12.0f) * u + 2.0f * b2) * u + b1;
+  // Near a double root (collinear or nearly collinear structures) the rounded
+  // coefficients may carry no real root at all (the pair turns complex) and
+  // Newton wanders; it only counts when it converged to a clearly simple root
+  // (the slope there is ~2.4 for a well-spread structure).
+  if (!converged || !(fabsf(dq) > 1e-2f) || !(u == u)) return false;
+  const float mm = (float)D * u / n * s2;
+  *msd = mm > 0.0f ? mm : 0.0f;
+  return true;
+}
+
 // Mean-square deviation from the QCP eigenvalue, clamped at zero as the
 // reference does (math.rs:34-37).
 WMD_HD double msd_from(double gx, double gy, double lambda, double n) {
