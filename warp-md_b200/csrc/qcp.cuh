@@ -183,75 +183,26 @@ WMD_HD QcpOut qcp_lambda(const double h[9], double e0) {
 
 
 
-// Mean-square deviation of a pair from H and the self-sums G_x, G_y, with the
-// root search in FP32.  Written in u = 1 - lambda / e0 (e0 = (G_x + G_y) / 2,
-// an upper bound of lambda_max), the characteristic polynomial divided by
-// e0^4 is
-//     Q(u) = u^4 - 4 u^3 + (6 + d2) u^2 - (4 + 2 d2 + d1) u + (1 + d2 + d1 + d0),
-// d_k = c_k / e0^(4-k), and its smallest root u1 = 1 - lambda_max / e0 gives
-// MSD = 2 e0 u1 / n.  The coefficients are formed in FP64: they carry the
-// cancellation (the constant term is ~8 u1 while its parts are O(1)).  Newton
-// from u = 0 runs on their FP32 roundings, without FP64 divisions (on sm_100a
-// FP64 arithmetic stalls beside tensor-core MMAs); rounding moves the root by
-// ~1e-7 of itself when the other roots lie near 1.3, more when one comes
-// close (planar structures), so one last Newton step evaluates the FP64
-// polynomial with the FP32 slope.  Returns false, leaving *msd unset, when the root is not
-// simple (a second eigenvalue within ~1e-4 e0: collinear or planar
-// structures); qcp_lambda then handles the pair.
-WMD_HD bool qcp_msd_shifted(const double h[9], double gx, double gy, double n, double* msd) {
-  const double e0 = 0.5 * (gx + gy);
-  if (!(e0 > 0.0)) {
-    *msd = 0.0;
-    return true;
-  }
-  double k[16];
-  key_matrix(h, k);
-  double c2 = 0.0;
-  for (int i = 0; i < 9; ++i) c2 += h[i] * h[i];
-  c2 *= -2.0;
-  const double c1 = -8.0 * det3(h);
-  const double c0 = det4(k);
-  const double inv = 1.0 / e0, inv2 = inv * inv;
-  const double d2 = c2 * inv2, d1 = c1 * inv2 * inv, d0 = c0 * inv2 * inv2;
-  const double bb0 = ((1.0 + d2) + d1) + d0, bb1 = -(4.0 + 2.0 * d2 + d1), bb2 = 6.0 + d2;
-  const float b0 = (float)bb0, b1 = (float)bb1, b2 = (float)bb2;
-  float u = 0.0f, dq = b1;
-  for (int it = 0; it < 16; ++it) {
-    const float q = (((u - 4.0f) * u + b2) * u + b1) * u + b0;
-    dq = ((4.0f * u - 12.0f) * u + 2.0f * b2) * u + b1;
-    if (!(dq != 0.0f)) break;
-    const float du = q / dq;
-    u -= du;
-    if (fabsf(du) <= 2e-7f * fabsf(u) + 1e-30f) break;
-  }
-  dq = ((4.0f * u - 12.0f) * u + 2.0f * b2) * u + b1;
-  if (!(fabsf(dq) > 1e-4f) || !(u == u)) return false;
-  // one Newton step on the FP64 polynomial with the FP32 slope: the error of
-  // the FP32 root (coefficients rounded to FP32) shrinks by ~1e-7
-  double ud = (double)u;
-  ud -= ((((ud - 4.0) * ud + bb2) * ud + bb1) * ud + bb0) * (double)(1.0f / dq);
-  const double m = 2.0 * e0 * ud / n;
-  *msd = m > 0.0 ? m : 0.0;
-  return true;
-}
-
 // Mean-square deviation of a frame pair in the tensor-core epilogue, with as
 // little FP64 arithmetic as the cancellation allows (on sm_100a FP64 issue
 // stalls beside tensor-core MMAs, FP32 does not).  H (9 entries) is exact in
-// integer units of s^2; gx, gy are the self-sums in the same units.  With
-// D = G_x + G_y = 2 e0, the quartic of qcp_msd_shifted is
-// Q(u) = det(M - u I), M = I - K / e0:
-//   * its constant term det(M) is where the cancellation sits (~8 u1 from O(1)
+// integer units of s^2; gx, gy are the self-sums in the same units.  Written in
+// u = 1 - lambda / e0 (e0 = (G_x + G_y) / 2 = D / 2, an upper bound of
+// lambda_max), the characteristic polynomial of K divided by e0^4 is
+//     Q(u) = det(M - u I) = u^4 - 4 u^3 + (6 + d2) u^2 - (4 + 2 d2 + d1) u + det(M),
+// M = I - K / e0, d_k = c_k / e0^(4-k); its smallest root u1 = 1 - lambda_max / e0
+// gives MSD = 2 e0 u1 / n.
+//   * The constant term det(M) is where the cancellation sits (~8 u1 from O(1)
 //     parts): M D = D I - 2K is formed from the exact inputs and its
 //     determinant taken in FP64 (no division), then scaled by 1 / D^4 with an
-//     FP32 reciprocal (a relative 1e-7 on this small term is harmless);
-//   * the other coefficients, -(4 + 2 d2 + d1) and 6 + d2, are O(1) sums
-//     without cancellation and are formed in FP32 from H / e0;
-//   * Newton from u = 0 runs in FP32 as in qcp_msd_shifted.
-// MSD = D u1 s2 / n.  Returns false, leaving *msd unset, when Newton did not
-// converge to a clearly simple root (a second eigenvalue within ~1e-2 e0:
-// collinear or nearly collinear structures); the caller then takes the FP64
-// route.
+//     FP32 reciprocal (a relative 1e-7 on this small term is harmless).
+//   * The other coefficients are O(1) sums without cancellation (the roots
+//     other than u1 lie near 1.3, so u1 is well conditioned) and are formed in
+//     FP32 from H / e0.
+//   * Newton from u = 0 runs in FP32, without FP64 divisions.
+// Returns false, leaving *msd unset, when Newton did not converge to a clearly
+// simple root (a second eigenvalue within ~1e-2 e0: collinear or nearly
+// collinear structures); the caller then takes the FP64 route (qcp_lambda).
 WMD_HD bool qcp_msd_mixed(const long long hq[9], double gx, double gy, float n, float s2, float* msd) {
   const double D = gx + gy;
   if (!(D > 0.0)) {
