@@ -209,28 +209,42 @@ WMD_HD bool qcp_msd_mixed(const long long hq[9], double gx, double gy, float n, 
     *msd = 0.0f;
     return true;
   }
-  double h[9];
-  for (int i = 0; i < 9; ++i) h[i] = (double)hq[i];
-  // M D = D I - 2 K (K as key_matrix, symmetric)
-  const double m00 = D - 2.0 * (h[0] + h[4] + h[8]);
-  const double m11 = D - 2.0 * (h[0] - h[4] - h[8]);
-  const double m22 = D - 2.0 * (h[4] - h[0] - h[8]);
-  const double m33 = D - 2.0 * (h[8] - h[0] - h[4]);
-  const double m01 = -2.0 * (h[5] - h[7]), m02 = -2.0 * (h[6] - h[2]), m03 = -2.0 * (h[1] - h[3]);
-  const double m12 = -2.0 * (h[1] + h[3]), m13 = -2.0 * (h[6] + h[2]), m23 = -2.0 * (h[5] + h[7]);
-  const double m[16] = {m00, m01, m02, m03, m01, m11, m12, m13, m02, m12, m22, m23, m03, m13, m23, m33};
   const float invd = 1.0f / (float)D;
+  // FP32 part first (fewer live registers): d2 = c2 / e0^2 = -2 sum h'^2,
+  // d1 = c1 / e0^3 = -8 det h', h' = H / e0
+  float b1, b2;
+  {
+    float hf[9];
+    for (int i = 0; i < 9; ++i) hf[i] = (float)hq[i] * (2.0f * invd);
+    float ss = 0.0f;
+    for (int i = 0; i < 9; ++i) ss = fmaf(hf[i], hf[i], ss);
+    const float det3f = hf[0] * (hf[4] * hf[8] - hf[5] * hf[7]) - hf[1] * (hf[3] * hf[8] - hf[5] * hf[6]) +
+                        hf[2] * (hf[3] * hf[7] - hf[4] * hf[6]);
+    const float d2 = -2.0f * ss, d1 = -8.0f * det3f;
+    b1 = -(4.0f + 2.0f * d2 + d1);
+    b2 = 6.0f + d2;
+  }
+  // M D = D I - 2 K (K as key_matrix, symmetric) from the exact inputs, in FP64
+  const double h0 = (double)hq[0], h4 = (double)hq[4], h8 = (double)hq[8];
+  const double m00 = D - 2.0 * (h0 + h4 + h8);
+  const double m11 = D - 2.0 * (h0 - h4 - h8);
+  const double m22 = D - 2.0 * (h4 - h0 - h8);
+  const double m33 = D - 2.0 * (h8 - h0 - h4);
+  const double h1 = (double)hq[1], h2 = (double)hq[2], h3 = (double)hq[3];
+  const double h5 = (double)hq[5], h6 = (double)hq[6], h7 = (double)hq[7];
+  const double m01 = -2.0 * (h5 - h7), m02 = -2.0 * (h6 - h2), m03 = -2.0 * (h1 - h3);
+  const double m12 = -2.0 * (h1 + h3), m13 = -2.0 * (h6 + h2), m23 = -2.0 * (h5 + h7);
+  // det of the symmetric M D by 2x2 minors of rows 2-3, then of rows 0-1 (as det4)
+  const double c5 = m22 * m33 - m23 * m23, c4 = m12 * m33 - m23 * m13, c3 = m12 * m23 - m22 * m13;
+  const double c2 = m02 * m33 - m23 * m03, c1 = m02 * m23 - m22 * m03, c0 = m02 * m13 - m12 * m03;
+  double det = (m00 * m11 - m01 * m01) * c5;
+  det -= (m00 * m12 - m02 * m01) * c4;
+  det += (m00 * m13 - m03 * m01) * c3;
+  det += (m01 * m12 - m02 * m11) * c2;
+  det -= (m01 * m13 - m03 * m11) * c1;
+  det += (m02 * m13 - m03 * m12) * c0;
   const double invd2 = (double)invd * (double)invd;  // D^-4 underflows FP32
-  const float b0 = (float)(det4(m) * (invd2 * invd2));
-  // H / e0 in FP32: d2 = c2 / e0^2 = -2 sum h'^2, d1 = c1 / e0^3 = -8 det h'
-  float hf[9];
-  for (int i = 0; i < 9; ++i) hf[i] = (float)hq[i] * (2.0f * invd);
-  float ss = 0.0f;
-  for (int i = 0; i < 9; ++i) ss = fmaf(hf[i], hf[i], ss);
-  const float det3f = hf[0] * (hf[4] * hf[8] - hf[5] * hf[7]) - hf[1] * (hf[3] * hf[8] - hf[5] * hf[6]) +
-                      hf[2] * (hf[3] * hf[7] - hf[4] * hf[6]);
-  const float d2 = -2.0f * ss, d1 = -8.0f * det3f;
-  const float b1 = -(4.0f + 2.0f * d2 + d1), b2 = 6.0f + d2;
+  const float b0 = (float)(det * (invd2 * invd2));
   float u = 0.0f, dq = b1;
   bool converged = false;
   for (int it = 0; it < 24; ++it) {
