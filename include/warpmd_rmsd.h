@@ -52,9 +52,12 @@ extern "C" {
 #define WMD_PAIR_DME 2   /* distance-matrix error (metric "dme")        */
 
 #define WMD_MODE_FP32 0  /* plain FP32 SIMT covariance tiles, FP64 QCP epilogue       */
-#define WMD_MODE_I8X3 1  /* tcgen05 int8 tensor cores, 3 limbs (24-bit fixed point), */
-                         /* exact int32 accumulation, FP64 QCP epilogue              */
-#define WMD_MODE_I8X2 2  /* as WMD_MODE_I8X3 with 2 limbs (16-bit fixed point)       */
+#define WMD_MODE_I8X3 1  /* tcgen05 int8 tensor cores, 3 limbs (24-bit fixed point):   */
+                         /* the 8 limb products other than lo x lo in exact int32     */
+                         /* accumulation, self-sums truncated alike; pairs below      */
+                         /* 0.01 A recomputed exactly in FP64; error <= 1e-4 A        */
+#define WMD_MODE_I8X2 2  /* 2 limbs (16-bit fixed point), all 4 products, exact Gram  */
+                         /* matrix of the quantised frames; error ~2e-4 A             */
 #define WMD_MODE_FP64 3  /* FP64 SIMT covariance tiles (accuracy reference on GPU)    */
 
 /* Per-frame statistics written by wmd_rmsd_forward and read by
