@@ -1,7 +1,9 @@
-"""The library's FP64 QCP header (warp-md_b200/csrc/qcp.cuh) compiled for the
-host and checked against the oracle's SVD route: lambda_max, the
-degenerate-root fallback, and the rotation convention (R maps frame
-coordinates onto the reference, as R = V U^T in plan.rs:1214-1221)."""
+"""The library's QCP header (warp-md_b200/csrc/qcp.cuh) compiled for the host
+and checked against the oracle's SVD route: lambda_max, the degenerate-root
+fallback, and the rotation convention (R maps frame coordinates onto the
+reference, as R = V U^T in plan.rs:1214-1221).  The mixed-precision MSD of the
+tensor-core pairwise epilogue is checked against the FP64 route on the same
+exact integer sums."""
 import ctypes
 import os
 import subprocess
@@ -28,6 +30,10 @@ def qlib(tmp_path_factory):
     L.t_lambda_svd.restype = ctypes.c_double
     L.t_rotation_qcp.argtypes = [dp, ctypes.c_double, dp]
     L.t_rotation_svd.argtypes = [dp, dp]
+    ip = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+    L.t_qcp_msd_mixed.argtypes = [ip, ctypes.c_double, ctypes.c_double, ctypes.c_float, ctypes.c_float,
+                                  ctypes.POINTER(ctypes.c_float)]
+    L.t_qcp_msd_mixed.restype = ctypes.c_int
     return L
 
 
@@ -106,3 +112,58 @@ def test_mirror_uses_reflection_fix(qlib):
     lam, _, _ = _lam(qlib, h, 0.5 * (gx + gy))
     _, ss = oracle.kabsch_rotation(h)
     assert abs(lam - ss) < 1e-10 * ss
+
+
+def _random_rotation(rng):
+    q = rng.normal(size=4)
+    w, a, b, c = q / np.linalg.norm(q)
+    return np.array([[1 - 2 * (b * b + c * c), 2 * (a * b - c * w), 2 * (a * c + b * w)],
+                     [2 * (a * b + c * w), 1 - 2 * (a * a + c * c), 2 * (b * c - a * w)],
+                     [2 * (a * c - b * w), 2 * (b * c + a * w), 1 - 2 * (a * a + b * b)]])
+
+
+def test_mixed_precision_msd_matches_fp64_route(qlib):
+    """qcp_msd_mixed (the tensor-core epilogue's QCP: FP64 only for det(D I - 2K),
+    FP32 for the other coefficients and Newton) against qcp_lambda in FP64 on
+    the same exact integer sums.  Inputs as the i8 limb path builds them:
+    centred coordinates quantised to steps s of 6e-6 .. 4.2e-5 A, H and the
+    self-sums exact in units of s^2.  Accepted roots agree within 5e-6 A of
+    RMSD; collinear and nearly collinear structures are handed back to the
+    FP64 route."""
+    rng = np.random.default_rng(11)
+    worst = 0.0
+    handed_back = {"general": 0, "collinear": 0}
+    counts = {"general": 0, "collinear": 0}
+    for trial in range(400):
+        n = int(rng.integers(3, 1500))
+        kind = ("general", "general", "planar", "collinear")[trial % 4]
+        sig = 10 ** rng.uniform(-3.5, 0.5)
+        s = 6e-6 * (1 + trial % 7)
+        x = 15 * rng.normal(size=(n, 3))
+        if kind == "planar":
+            x[:, 2] = 0.0
+        if kind == "collinear":
+            x[:, 1] = (trial % 8 == 3) * 1e-3 * rng.normal(size=n)
+            x[:, 2] = 0.0
+        y = x @ _random_rotation(rng).T + sig * rng.normal(size=(n, 3))
+        qx = np.rint((x - x.mean(0)) / s).astype(np.int64)
+        qy = np.rint((y - y.mean(0)) / s).astype(np.int64)
+        h = np.ascontiguousarray((qx.T @ qy).reshape(9))
+        gx, gy = float((qx * qx).sum()), float((qy * qy).sum())
+        lam, _, _ = _lam(qlib, h.astype(np.float64).reshape(3, 3), 0.5 * (gx + gy))
+        ref = np.sqrt(max(gx + gy - 2 * lam, 0.0) / n * s * s)
+        m = ctypes.c_float()
+        ok = qlib.t_qcp_msd_mixed(h, gx, gy, float(n), float(s * s), ctypes.byref(m))
+        group = "collinear" if kind == "collinear" else "general"
+        counts[group] += 1
+        if not ok:
+            handed_back[group] += 1
+            continue
+        err = abs(np.sqrt(m.value) - ref)
+        worst = max(worst, err)
+        assert err <= 5e-6, (trial, kind, n, sig, np.sqrt(m.value), ref)
+    assert worst <= 5e-6
+    # general and planar structures stay on the mixed route; exactly collinear ones do not
+    assert handed_back["general"] <= counts["general"] // 50, handed_back
+    assert handed_back["collinear"] >= counts["collinear"] // 4, handed_back
+
